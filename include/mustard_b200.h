@@ -1,0 +1,176 @@
+/*
+ * mustard_b200.h -- C ABI of the B200 (sm_100a) runtime for static tiled LU / Cholesky
+ * task graphs.
+ *
+ * The reference (ParCoreLab/mustard) exposes a header-only C++ interface whose tasks are
+ * captured cuBLAS/cuSOLVER calls: TiledGraphCreator (mustard/mustard.h:132-384), a
+ * broker queue (mustard/broker_queue.h:13-147), and the device kernels kernel_scheduler,
+ * kernel_dep_update and kernel_populate_queue (mustard/mustard.h:70-129).  Here a task is
+ * structured data (operation, tile written, tiles read) and a single persistent kernel
+ * pops ready work, runs hand-written FP64 tile kernels and resolves dependencies on the
+ * device.  Every entry point returns an mtd_status; nothing here exits the process.
+ *
+ * Conventions
+ *   - Matrices are FP64, column-major, leading dimension lda >= n.  Tile (i, j) covers
+ *     rows [i*tile, min((i+1)*tile, n)) and columns [j*tile, min((j+1)*tile, n)), as in
+ *     the reference's `matrix + i*B + j*B*N` (mustard/cholesky_mustard.cu:157-160).  The
+ *     last tile row/column may be ragged (the reference requires tile | n).
+ *   - The caller owns the matrix; a graph owns its device-side DAG, queues, counters and
+ *     the per-step inverse workspace.
+ *   - `stream` is a cudaStream_t passed as void* (0 = legacy default stream).
+ *   - One host thread per graph; different graphs are independent.
+ */
+#ifndef MUSTARD_B200_H
+#define MUSTARD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MTD_ABI_VERSION 1
+
+typedef enum mtd_status {
+    MTD_OK = 0,
+    MTD_ERR_INVALID_ARG = 1,     /* bad argument (size, tile, op, pointer)              */
+    MTD_ERR_STATE = 2,           /* call out of order (e.g. add_task after finalize)    */
+    MTD_ERR_CUDA = 3,            /* a CUDA runtime call failed                          */
+    MTD_ERR_TIMEOUT = 4,         /* a device-side wait ran past its limit               */
+    MTD_ERR_NOT_POSITIVE_DEFINITE = 5, /* POTRF met a non-positive pivot; see info    */
+    MTD_ERR_SINGULAR = 6,        /* GETRF (no pivoting) met a zero pivot; see info      */
+    MTD_ERR_BAD_DAG = 7,         /* graph cannot be executed (see mtd_graph_finalize)   */
+    MTD_ERR_NO_DEVICE = 8,       /* no CUDA device / not an sm_100 device               */
+    MTD_ERR_OUT_OF_MEMORY = 9,   /* device allocation failed                            */
+    MTD_ERR_QUEUE = 10           /* ready-queue overflow (internal invariant broken)    */
+} mtd_status;
+
+typedef enum mtd_kind {
+    MTD_KIND_LU = 0,             /* no-pivot LU, reference lu_mustard                   */
+    MTD_KIND_CHOLESKY = 1,       /* lower Cholesky, reference cholesky_mustard          */
+    MTD_KIND_CUSTOM = 2          /* tasks supplied one by one with mtd_graph_add_task   */
+} mtd_kind;
+
+/* Tile operations.  Each replaces one captured library call of the reference. */
+typedef enum mtd_op {
+    MTD_OP_POTRF = 0,     /* A(k,k) = chol(A(k,k)), lower         cholesky_mustard.cu:238   */
+    MTD_OP_TRSM_RLT = 1,  /* A(i,k) = A(i,k) L(k,k)^-T            cholesky_mustard.cu:281   */
+    MTD_OP_SYRK_LN = 2,   /* A(i,i) -= A(i,k) A(i,k)^T, lower     cholesky_mustard.cu:327   */
+    MTD_OP_GEMM_NT = 3,   /* A(j,i) -= A(j,k) A(i,k)^T            cholesky_mustard.cu:376   */
+    MTD_OP_GETRF = 4,     /* A(k,k) = L U, no pivoting            lu_mustard.cu:361         */
+    MTD_OP_TRSM_LLNU = 5, /* A(k,i) = L(k,k)^-1 A(k,i), unit L    lu_mustard.cu:413         */
+    MTD_OP_TRSM_RUN = 6,  /* A(i,k) = A(i,k) U(k,k)^-1            lu_mustard.cu:459         */
+    MTD_OP_GEMM_NN = 7    /* A(i,j) -= A(i,k) A(k,j)              lu_mustard.cu:511         */
+} mtd_op;
+
+typedef enum mtd_generator {
+    MTD_GEN_UNIFORM_DIAG = 0,    /* U[-1,1) entries + n on the diagonal (LU input)      */
+    MTD_GEN_SPD = 1              /* B B^T / n + alpha I, B = U[-1,1) (Cholesky input)   */
+} mtd_generator;
+
+typedef struct mtd_graph mtd_graph;
+
+/* Per-run statistics, filled by mtd_graph_last_stats after a run completed. */
+typedef struct mtd_run_stats {
+    int64_t tasks;               /* tasks executed                                      */
+    int64_t items;               /* work items executed                                 */
+    int64_t ctas;                /* persistent CTAs launched                            */
+    double busy_fraction;        /* sum of item durations / (ctas * kernel span); only  */
+                                 /* valid when tracing was enabled, else -1             */
+    double span_ms;              /* first item start to last item end (tracing), or -1  */
+} mtd_run_stats;
+
+/* ---- graph construction: replaces TiledGraphCreator (mustard/mustard.h:132-384) ---- */
+
+/* Create an empty graph over an n x n matrix cut into tile x tile tiles.
+ * Replaces the TiledGraphCreator constructor (mustard/mustard.h:139-146). */
+int mtd_graph_create(mtd_graph **out, int kind, int64_t n, int64_t tile);
+
+/* Record one task: operation `op` writing tile (wi, wj) and reading `nreads` tiles given
+ * as (row, col) pairs in `reads` -- the arguments of the reference's
+ * beginCaptureOperation(tileToWrite, {tilesToRead}) (mustard/mustard.h:148-167); the
+ * operation replaces the library call captured between begin and endCaptureOperation.
+ * Predecessors are inferred as in getSubgraphDependencies (mustard/mustard.h:279-296):
+ * the last writer of every tile in reads + {write}, sorted and de-duplicated; a writer
+ * additionally waits for earlier readers of the tile it overwrites.  Returns the task
+ * index (>= 0) or a negative mtd_status. */
+int mtd_graph_add_task(mtd_graph *g, int op, int wi, int wj, const int *reads, int nreads);
+
+/* Emit the reference's whole task list for the graph's kind, in its loop order
+ * (cholesky_mustard.cu:224-395 or lu_mustard.cu:345-533). */
+int mtd_graph_build_tiled(mtd_graph *g);
+
+/* Number of tasks recorded so far. */
+int mtd_graph_num_tasks(const mtd_graph *g);
+
+/* Copy task `task`'s predecessor list (the reference's subgraphDependencies[task],
+ * mustard/mustard.h:137) into out[0..cap); returns the full count or a negative status. */
+int mtd_graph_get_deps(const mtd_graph *g, int task, int *out, int cap);
+
+/* Number of device work items task `task` is split into (0 before finalize). */
+int mtd_graph_task_items(const mtd_graph *g, int task);
+
+/* Validate and upload the DAG: predecessor counts (the reference's h_dependencies,
+ * cholesky_mustard.cu:422-425), successor lists (what insertDependencyKernel wires,
+ * mustard/mustard.h:197-211), work items, priorities, queues and workspace.  Replaces
+ * the per-task graph instantiation and queue set-up of cholesky_mustard.cu:408-466. */
+int mtd_graph_finalize(mtd_graph *g);
+
+/* Enable (1) or disable (0) the per-item device trace used for busy-fraction stats. */
+int mtd_graph_set_trace(mtd_graph *g, int enable);
+
+/* Upper bound (seconds) on any single device-side wait; default 10 s. */
+int mtd_graph_set_timeout(mtd_graph *g, double seconds);
+
+/* Run the graph on the device matrix dA (column-major, leading dimension lda).
+ * Replaces the timed cudaGraphLaunch(schedulerExec, s) of cholesky_mustard.cu:474 /
+ * lu_mustard.cu:609, plus the counter/queue reset of :479-485.  Stream-ordered.  If
+ * info_out is non-NULL the call synchronises the stream and returns the run's status
+ * with LAPACK-style info (1-based column of the first bad pivot, else 0); if NULL it
+ * returns after enqueueing and mtd_graph_status reports the outcome later. */
+int mtd_run(mtd_graph *g, double *dA, int64_t lda, void *stream, int *info_out);
+
+/* Synchronise with the last run and return its status (and info). */
+int mtd_graph_status(mtd_graph *g, int *info_out);
+
+/* Statistics of the last completed run. */
+int mtd_graph_last_stats(mtd_graph *g, mtd_run_stats *out);
+
+/* Raw per-item trace of the last run (tracing enabled): 4 words per work item -- start
+ * and end %globaltimer ns, SM id, task << 32 | item.  Returns the number of records
+ * copied into out (at most cap_records), or a negative status. */
+long long mtd_graph_copy_trace(mtd_graph *g, unsigned long long *out, long long cap_records);
+
+/* Release everything the graph owns (replaces queue.free_mem(), broker_queue.h:36-43). */
+int mtd_graph_destroy(mtd_graph *g);
+
+/* ---- one-call drivers: replace tiledCholesky / tiledLU (cholesky_mustard.cu:135,
+ *      lu_mustard.cu:256) for a caller that owns the device matrix ---- */
+int mtd_tiled_cholesky(double *dA, int64_t n, int64_t lda, int64_t tile, void *stream,
+                       int *info_out);
+int mtd_tiled_lu(double *dA, int64_t n, int64_t lda, int64_t tile, void *stream,
+                 int *info_out);
+
+/* ---- inputs: device generators (the reference builds its input on the host,
+ *      include/gen.h:23-38; these make the seeded inputs of the benchmark shapes) ---- */
+int mtd_generate(double *dA, int64_t n, int64_t lda, int which, uint64_t seed, double alpha,
+                 void *stream);
+
+/* Host generator identical to the reference's include/gen.h:23-38 (glibc srand(420),
+ * rand()/RAND_MAX upper triangle, mirrored, +n diagonal); writes n*n doubles. */
+int mtd_generate_reference_host(double *hA, int64_t n);
+
+/* ---- measurement ---- */
+
+/* Measure the device's FP64 tensor-core (DMMA) rate with a register-only loop; writes
+ * TFLOP/s.  Used as the roofline denominator next to the datasheet figure. */
+int mtd_probe_fp64_peak(double *tflops_out);
+
+const char *mtd_strerror(int status);
+int mtd_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MUSTARD_B200_H */

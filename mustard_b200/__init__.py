@@ -1,0 +1,246 @@
+"""mustard_b200: B200 (sm_100a) runtime for static tiled LU / Cholesky task graphs.
+
+Python view of the C ABI in include/mustard_b200.h (loaded with ctypes from the in-tree
+``mustard_b200/lib/libmustard_b200.so``).  The reference's host interface is the C++
+``mustard::TiledGraphCreator`` (mustard/mustard.h:132-384); ``TiledGraphCreator`` below
+keeps its names -- ``beginCaptureOperation`` / ``endCaptureOperation`` /
+``subgraphDependencies`` -- with the captured library call replaced by the operation
+code given to ``beginCaptureOperation``.
+
+Matrices are FP64 and column-major.  A torch tensor ``a`` of shape (n, n) is passed as
+the column-major matrix ``a.T`` when ``a.T`` is contiguous (``colmajor(x)`` makes one),
+i.e. the storage order is the reference's ``matrix[i + j * N]``.
+
+There is no CPU fallback: if the shared library is missing, importing this package
+raises ``ImportError``.
+"""
+import ctypes
+import os
+
+from . import _capi
+from ._capi import (  # noqa: F401  (re-exported constants)
+    GEN_SPD, GEN_UNIFORM_DIAG, KIND_CHOLESKY, KIND_CUSTOM, KIND_LU, OP_GEMM_NN, OP_GEMM_NT,
+    OP_GETRF, OP_NAMES, OP_POTRF, OP_SYRK_LN, OP_TRSM_LLNU, OP_TRSM_RLT, OP_TRSM_RUN,
+    STATUS_NAMES, MtdError, lib, lib_path)
+
+__all__ = [
+    "TaskGraph", "TiledGraphCreator", "tiled_cholesky", "tiled_lu", "generate", "colmajor",
+    "probe_fp64_peak", "MtdError", "lib", "lib_path",
+]
+
+
+def _stream_handle(stream):
+    if stream is None:
+        import torch
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if hasattr(stream, "cuda_stream"):
+        return ctypes.c_void_p(stream.cuda_stream)
+    return ctypes.c_void_p(int(stream))
+
+
+def _matrix_ptr(a, n=None):
+    """(pointer, n, lda) of a column-major FP64 CUDA matrix given as a torch tensor whose
+    transpose is contiguous (shape (n, n), strides (1, lda)), or as an int pointer."""
+    if isinstance(a, int):
+        if n is None:
+            raise ValueError("n is required with a raw pointer")
+        return a, n, n
+    import torch
+    if a.dtype != torch.float64 or not a.is_cuda:
+        raise TypeError("expected a float64 CUDA tensor")
+    if a.dim() != 2 or a.shape[0] != a.shape[1]:
+        raise ValueError("expected a square matrix")
+    if a.stride(0) != 1 or a.stride(1) < a.shape[0]:
+        raise ValueError("expected column-major storage (use mustard_b200.colmajor)")
+    return a.data_ptr(), a.shape[0], a.stride(1)
+
+
+def colmajor(x):
+    """Column-major copy of a square torch tensor (same values, Fortran storage)."""
+    return x.t().contiguous().t()
+
+
+class TaskGraph:
+    """Owner of one ``mtd_graph``."""
+
+    def __init__(self, kind, n, tile):
+        self._lib = lib()
+        h = ctypes.c_void_p()
+        _capi.check(self._lib.mtd_graph_create(ctypes.byref(h), kind, n, tile))
+        self._h = h
+        self.kind, self.n, self.tile = kind, n, tile
+        self.tiles = (n + tile - 1) // tile
+        self.finalized = False
+
+    # -- construction ------------------------------------------------------
+    def add_task(self, op, write, reads):
+        flat = [int(v) for tile in reads for v in tile]
+        arr = (ctypes.c_int * max(len(flat), 1))(*flat)
+        rc = self._lib.mtd_graph_add_task(self._h, op, int(write[0]), int(write[1]), arr, len(reads))
+        if rc < 0:
+            raise MtdError(-rc)
+        return rc
+
+    def build_tiled(self):
+        _capi.check(self._lib.mtd_graph_build_tiled(self._h))
+        return self
+
+    def set_trace(self, enable=True):
+        _capi.check(self._lib.mtd_graph_set_trace(self._h, 1 if enable else 0))
+        return self
+
+    def set_timeout(self, seconds):
+        _capi.check(self._lib.mtd_graph_set_timeout(self._h, float(seconds)))
+        return self
+
+    def finalize(self):
+        _capi.check(self._lib.mtd_graph_finalize(self._h))
+        self.finalized = True
+        return self
+
+    # -- queries -----------------------------------------------------------
+    @property
+    def num_tasks(self):
+        return self._lib.mtd_graph_num_tasks(self._h)
+
+    def deps(self, task):
+        cnt = self._lib.mtd_graph_get_deps(self._h, task, None, 0)
+        if cnt < 0:
+            raise MtdError(-cnt)
+        buf = (ctypes.c_int * max(cnt, 1))()
+        self._lib.mtd_graph_get_deps(self._h, task, buf, cnt)
+        return list(buf[:cnt])
+
+    def items(self, task):
+        return self._lib.mtd_graph_task_items(self._h, task)
+
+    # -- execution ---------------------------------------------------------
+    def run(self, a, stream=None, sync=True, lda=None):
+        """Factor the column-major device matrix ``a`` in place.  With ``sync`` the call
+        waits and raises MtdError on failure; otherwise it returns at once and
+        ``status()`` reports later."""
+        ptr, n, ld = _matrix_ptr(a, self.n)
+        if lda is not None:
+            ld = lda
+        if n != self.n:
+            raise ValueError(f"matrix is {n}x{n}, graph expects {self.n}")
+        info = ctypes.c_int(0)
+        rc = self._lib.mtd_run(self._h, ctypes.c_void_p(ptr), ld, _stream_handle(stream),
+                               ctypes.byref(info) if sync else None)
+        _capi.check(rc, info.value)
+        return info.value
+
+    def status(self):
+        info = ctypes.c_int(0)
+        rc = self._lib.mtd_graph_status(self._h, ctypes.byref(info))
+        return rc, info.value
+
+    def stats(self):
+        s = _capi.RunStats()
+        _capi.check(self._lib.mtd_graph_last_stats(self._h, ctypes.byref(s)))
+        return {"tasks": s.tasks, "items": s.items, "ctas": s.ctas,
+                "busy_fraction": s.busy_fraction, "span_ms": s.span_ms}
+
+    def trace(self, max_records=None):
+        """Per-item records of the last traced run: list of (start_ns, end_ns, sm, task, item)."""
+        cap = max_records or 1 << 22
+        buf = (ctypes.c_ulonglong * (4 * cap))()
+        n = self._lib.mtd_graph_copy_trace(self._h, buf, cap)
+        if n < 0:
+            raise MtdError(-n)
+        return [(buf[4 * i], buf[4 * i + 1], buf[4 * i + 2], buf[4 * i + 3] >> 32, buf[4 * i + 3] & 0xFFFFFFFF)
+                for i in range(n)]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.mtd_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class TiledGraphCreator:
+    """The reference's TiledGraphCreator (mustard/mustard.h:132-384) over the C ABI.
+
+    ``beginCaptureOperation(op, tileToWrite, tilesToRead)`` records a task (the reference
+    captures the library call issued between begin and end; here the call is named by
+    ``op``), ``endCaptureOperation()`` closes it, and ``subgraphDependencies[i]`` is the
+    sorted predecessor list of task i (mustard/mustard.h:279-296)."""
+
+    def __init__(self, kind, n, tile):
+        self.graph = TaskGraph(kind, n, tile)
+        self._open = None
+
+    def beginCaptureOperation(self, op, tileToWrite, tilesToRead):
+        if self._open is not None:
+            raise MtdError(_capi.ERR_STATE)
+        self._open = (op, tuple(tileToWrite), [tuple(t) for t in tilesToRead])
+
+    def endCaptureOperation(self):
+        if self._open is None:
+            raise MtdError(_capi.ERR_STATE)
+        op, write, reads = self._open
+        self._open = None
+        return self.graph.add_task(op, write, reads)
+
+    @property
+    def subgraphDependencies(self):
+        return [self.graph.deps(t) for t in range(self.graph.num_tasks)]
+
+
+def _one_call(kind, a, tile, stream):
+    ptr, n, ld = _matrix_ptr(a)
+    info = ctypes.c_int(0)
+    fn = lib().mtd_tiled_cholesky if kind == KIND_CHOLESKY else lib().mtd_tiled_lu
+    rc = fn(ctypes.c_void_p(ptr), n, ld, tile, _stream_handle(stream), ctypes.byref(info))
+    _capi.check(rc, info.value)
+    return info.value
+
+
+def tiled_cholesky(a, tile, stream=None):
+    """In-place lower Cholesky of the column-major CUDA matrix ``a`` (tiledCholesky,
+    mustard/cholesky_mustard.cu:135)."""
+    return _one_call(KIND_CHOLESKY, a, tile, stream)
+
+
+def tiled_lu(a, tile, stream=None):
+    """In-place no-pivot LU of the column-major CUDA matrix ``a`` (tiledLU,
+    mustard/lu_mustard.cu:256)."""
+    return _one_call(KIND_LU, a, tile, stream)
+
+
+def generate(a, which, seed=0, alpha=1.0, stream=None):
+    """Fill the column-major CUDA matrix ``a`` with a seeded benchmark input."""
+    ptr, n, ld = _matrix_ptr(a)
+    _capi.check(lib().mtd_generate(ctypes.c_void_p(ptr), n, ld, which, ctypes.c_uint64(seed),
+                                   ctypes.c_double(alpha), _stream_handle(stream)))
+
+
+def generate_reference_host(n):
+    """The reference's host input (include/gen.h:23-38) as a numpy array (symmetric)."""
+    import numpy as np
+    out = np.empty((n, n), dtype=np.float64)
+    _capi.check(lib().mtd_generate_reference_host(out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n))
+    return out
+
+
+def probe_fp64_peak():
+    """Measured FP64 tensor-core (DMMA) rate of the current device, TFLOP/s."""
+    v = ctypes.c_double(0.0)
+    _capi.check(lib().mtd_probe_fp64_peak(ctypes.byref(v)))
+    return v.value
+
+
+LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
+
+lib()  # fail at import when the native library is missing: there is no fallback path

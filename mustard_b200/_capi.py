@@ -1,0 +1,91 @@
+"""ctypes declarations for include/mustard_b200.h."""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "lib", "libmustard_b200.so")
+
+OK = 0
+ERR_INVALID_ARG, ERR_STATE, ERR_CUDA, ERR_TIMEOUT = 1, 2, 3, 4
+ERR_NOT_POSITIVE_DEFINITE, ERR_SINGULAR, ERR_BAD_DAG = 5, 6, 7
+ERR_NO_DEVICE, ERR_OUT_OF_MEMORY, ERR_QUEUE = 8, 9, 10
+STATUS_NAMES = {
+    0: "MTD_OK", 1: "MTD_ERR_INVALID_ARG", 2: "MTD_ERR_STATE", 3: "MTD_ERR_CUDA",
+    4: "MTD_ERR_TIMEOUT", 5: "MTD_ERR_NOT_POSITIVE_DEFINITE", 6: "MTD_ERR_SINGULAR",
+    7: "MTD_ERR_BAD_DAG", 8: "MTD_ERR_NO_DEVICE", 9: "MTD_ERR_OUT_OF_MEMORY", 10: "MTD_ERR_QUEUE",
+}
+
+KIND_LU, KIND_CHOLESKY, KIND_CUSTOM = 0, 1, 2
+OP_POTRF, OP_TRSM_RLT, OP_SYRK_LN, OP_GEMM_NT = 0, 1, 2, 3
+OP_GETRF, OP_TRSM_LLNU, OP_TRSM_RUN, OP_GEMM_NN = 4, 5, 6, 7
+OP_NAMES = {0: "POTRF", 1: "TRSM_RLT", 2: "SYRK", 3: "GEMM_NT", 4: "GETRF", 5: "TRSM_LLNU",
+            6: "TRSM_RUN", 7: "GEMM_NN"}
+GEN_UNIFORM_DIAG, GEN_SPD = 0, 1
+
+# Every symbol the header declares, with its ctypes signature.
+_vp, _i, _i64, _d = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_double
+
+
+class RunStats(ctypes.Structure):
+    _fields_ = [("tasks", ctypes.c_int64), ("items", ctypes.c_int64), ("ctas", ctypes.c_int64),
+                ("busy_fraction", ctypes.c_double), ("span_ms", ctypes.c_double)]
+
+
+SIGNATURES = {
+    "mtd_graph_create": (_i, [ctypes.POINTER(_vp), _i, _i64, _i64]),
+    "mtd_graph_add_task": (_i, [_vp, _i, _i, _i, ctypes.POINTER(_i), _i]),
+    "mtd_graph_build_tiled": (_i, [_vp]),
+    "mtd_graph_num_tasks": (_i, [_vp]),
+    "mtd_graph_get_deps": (_i, [_vp, _i, ctypes.POINTER(_i), _i]),
+    "mtd_graph_task_items": (_i, [_vp, _i]),
+    "mtd_graph_finalize": (_i, [_vp]),
+    "mtd_graph_set_trace": (_i, [_vp, _i]),
+    "mtd_graph_set_timeout": (_i, [_vp, _d]),
+    "mtd_run": (_i, [_vp, _vp, _i64, _vp, ctypes.POINTER(_i)]),
+    "mtd_graph_status": (_i, [_vp, ctypes.POINTER(_i)]),
+    "mtd_graph_last_stats": (_i, [_vp, ctypes.POINTER(RunStats)]),
+    "mtd_graph_copy_trace": (ctypes.c_longlong, [_vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_longlong]),
+    "mtd_graph_destroy": (_i, [_vp]),
+    "mtd_tiled_cholesky": (_i, [_vp, _i64, _i64, _i64, _vp, ctypes.POINTER(_i)]),
+    "mtd_tiled_lu": (_i, [_vp, _i64, _i64, _i64, _vp, ctypes.POINTER(_i)]),
+    "mtd_generate": (_i, [_vp, _i64, _i64, _i, ctypes.c_uint64, _d, _vp]),
+    "mtd_generate_reference_host": (_i, [ctypes.POINTER(_d), _i64]),
+    "mtd_probe_fp64_peak": (_i, [ctypes.POINTER(_d)]),
+    "mtd_strerror": (ctypes.c_char_p, [_i]),
+    "mtd_abi_version": (_i, []),
+}
+
+_lib = None
+
+
+def lib_path():
+    return _LIB_PATH
+
+
+def lib():
+    """Load the runtime library (raises ImportError when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            raise ImportError(f"mustard_b200 native library missing: {_LIB_PATH} "
+                              "(build it with `python -m mustard_b200.build`)")
+        handle = ctypes.CDLL(_LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+class MtdError(RuntimeError):
+    def __init__(self, status, info=0):
+        self.status = status
+        self.info = info
+        msg = lib().mtd_strerror(status).decode() if _lib is not None else STATUS_NAMES.get(status, "?")
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}" + (f" (info={info})" if info else ""))
+
+
+def check(rc, info=0):
+    if rc != OK:
+        raise MtdError(rc, info)

@@ -1,0 +1,63 @@
+// Host-side task DAG: the data the reference keeps in TiledGraphCreator
+// (mustard/mustard.h:132-384) -- task list, last-writer map, predecessor lists -- plus what
+// the device runtime needs (successor CSR, work-item counts, priorities).
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <utility>
+#include <vector>
+
+#include "device_types.hpp"
+
+namespace mtd {
+
+using TileId = std::pair<int, int>;  // (row tile, column tile), the reference's MatrixTile
+
+struct HostTask {
+    int op = 0;
+    TileId write{0, 0};
+    std::vector<TileId> reads;  // as given by the caller (reference order)
+    TileId a{0, 0};             // first operand (triangular tile for TRSM)
+    TileId b{0, 0};             // second operand (GEMM only)
+};
+
+class Dag {
+public:
+    Dag(int kind, int64_t n, int64_t tile);
+
+    int kind() const { return kind_; }
+    int64_t n() const { return n_; }
+    int64_t tile() const { return tile_; }
+    int tiles() const { return tiles_; }
+    int64_t extent(int t) const;  // rows (or columns) of tile row t
+
+    // Returns the new task index, or a negative mtd_status.
+    int add_task(int op, int wi, int wj, const int *reads, int nreads);
+    int build_reference_order();
+
+    int num_tasks() const { return static_cast<int>(tasks_.size()); }
+    const std::vector<int> &deps(int t) const { return deps_[t]; }
+    const HostTask &task(int t) const { return tasks_[t]; }
+
+    // Fills the device task table, successor CSR and predecessor counts.
+    // Returns MTD_OK or MTD_ERR_BAD_DAG.
+    int lower(std::vector<DevTask> &tasks, std::vector<int> &succ, std::vector<int> &pred_count,
+              int64_t queue_cap[kNumQueues]) const;
+
+    int items_of(int t) const;
+
+private:
+    int kind_;
+    int64_t n_, tile_;
+    int tiles_;
+    std::vector<HostTask> tasks_;
+    std::vector<std::vector<int>> deps_;
+    std::map<TileId, int> last_writer_;                 // tileIndexByMap (mustard.h:177)
+    std::map<TileId, std::vector<int>> readers_since_;  // readers since the last write
+
+    bool valid_tile(const TileId &t) const;
+    int queue_of(int t) const;
+};
+
+}  // namespace mtd

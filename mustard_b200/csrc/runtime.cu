@@ -1,0 +1,385 @@
+// C ABI implementation: graph lifetime, device upload, runs, statistics.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/mustard_b200.h"
+#include "dag.hpp"
+#include "scheduler.cuh"
+
+using namespace mtd;
+
+struct mtd_graph {
+    Dag dag;
+    bool finalized = false;
+    int device = 0;
+    int num_sms = 0;
+    bool trace = false;
+    double timeout_s = 10.0;
+
+    DevTask *d_tasks = nullptr;
+    int *d_succ = nullptr;
+    int *d_deps_init = nullptr;
+    int *d_deps = nullptr;
+    int *d_items_left = nullptr;
+    int *d_roots = nullptr;
+    int n_roots = 0;
+    unsigned long long *d_queue[kNumQueues] = {nullptr, nullptr};
+    long long queue_cap[kNumQueues] = {0, 0};
+    QueueCtl *d_qctl = nullptr;
+    RunCtl *d_ctl = nullptr;
+    RunCtl *h_ctl = nullptr;  // pinned copy of the control block, filled at the end of a run
+    double *d_ws_lower = nullptr;
+    double *d_ws_upper = nullptr;
+    unsigned long long *d_trace = nullptr;
+    long long trace_cap = 0;
+    long long total_items = 0;
+
+    cudaStream_t last_stream = nullptr;
+    bool run_pending = false;
+    int last_grid = 0;
+
+    mtd_graph(int kind, int64_t n, int64_t tile) : dag(kind, n, tile) {}
+};
+
+namespace {
+
+template <int VEC>
+int smem_setup(int device) {
+    static bool done[64] = {false};
+    if (device < 0 || device >= 64) return MTD_ERR_INVALID_ARG;
+    if (!done[device]) {
+        if (cudaFuncSetAttribute(persistent_kernel<VEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kOpSmemBytes()) != cudaSuccess)
+            return MTD_ERR_CUDA;
+        done[device] = true;
+    }
+    return MTD_OK;
+}
+
+int check_device(int *device, int *num_sms) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return MTD_ERR_NO_DEVICE;
+    int major = 0;
+    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess)
+        return MTD_ERR_NO_DEVICE;
+    if (major != 10) return MTD_ERR_NO_DEVICE;  // built for sm_100a only
+    if (cudaDeviceGetAttribute(num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return MTD_ERR_NO_DEVICE;
+    *device = dev;
+    return MTD_OK;
+}
+
+template <typename T>
+int dev_alloc(T **p, size_t count) {
+    if (count == 0) count = 1;
+    if (cudaMalloc(reinterpret_cast<void **>(p), count * sizeof(T)) != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return MTD_ERR_OUT_OF_MEMORY;
+    }
+    return MTD_OK;
+}
+
+void release_device(mtd_graph *g) {
+    cudaFree(g->d_tasks);
+    cudaFree(g->d_succ);
+    cudaFree(g->d_deps_init);
+    cudaFree(g->d_deps);
+    cudaFree(g->d_items_left);
+    cudaFree(g->d_roots);
+    for (int q = 0; q < kNumQueues; ++q) cudaFree(g->d_queue[q]);
+    cudaFree(g->d_qctl);
+    cudaFree(g->d_ctl);
+    if (g->h_ctl) cudaFreeHost(g->h_ctl);
+    cudaFree(g->d_ws_lower);
+    cudaFree(g->d_ws_upper);
+    cudaFree(g->d_trace);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mtd_abi_version(void) { return MTD_ABI_VERSION; }
+
+const char *mtd_strerror(int status) {
+    switch (status) {
+    case MTD_OK: return "ok";
+    case MTD_ERR_INVALID_ARG: return "invalid argument";
+    case MTD_ERR_STATE: return "call out of order for this graph";
+    case MTD_ERR_CUDA: return "CUDA runtime error";
+    case MTD_ERR_TIMEOUT: return "device-side wait exceeded its time limit";
+    case MTD_ERR_NOT_POSITIVE_DEFINITE: return "matrix is not positive definite (see info)";
+    case MTD_ERR_SINGULAR: return "zero pivot in LU without pivoting (see info)";
+    case MTD_ERR_BAD_DAG: return "task graph cannot be executed";
+    case MTD_ERR_NO_DEVICE: return "no sm_100 CUDA device";
+    case MTD_ERR_OUT_OF_MEMORY: return "device allocation failed";
+    case MTD_ERR_QUEUE: return "ready-queue overflow";
+    default: return "unknown status";
+    }
+}
+
+int mtd_graph_create(mtd_graph **out, int kind, int64_t n, int64_t tile) {
+    if (!out) return MTD_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (kind < MTD_KIND_LU || kind > MTD_KIND_CUSTOM) return MTD_ERR_INVALID_ARG;
+    if (n <= 0 || tile <= 0 || tile > n) return MTD_ERR_INVALID_ARG;
+    if (n > (int64_t(1) << 31) - 1) return MTD_ERR_INVALID_ARG;
+    if ((n + tile - 1) / tile > 4096) return MTD_ERR_INVALID_ARG;
+    mtd_graph *g = new (std::nothrow) mtd_graph(kind, n, tile);
+    if (!g) return MTD_ERR_OUT_OF_MEMORY;
+    *out = g;
+    return MTD_OK;
+}
+
+int mtd_graph_add_task(mtd_graph *g, int op, int wi, int wj, const int *reads, int nreads) {
+    if (!g) return -MTD_ERR_INVALID_ARG;
+    if (g->finalized) return -MTD_ERR_STATE;
+    return g->dag.add_task(op, wi, wj, reads, nreads);
+}
+
+int mtd_graph_build_tiled(mtd_graph *g) {
+    if (!g) return MTD_ERR_INVALID_ARG;
+    if (g->finalized || g->dag.num_tasks() != 0) return MTD_ERR_STATE;
+    return g->dag.build_reference_order();
+}
+
+int mtd_graph_num_tasks(const mtd_graph *g) { return g ? g->dag.num_tasks() : -MTD_ERR_INVALID_ARG; }
+
+int mtd_graph_get_deps(const mtd_graph *g, int task, int *out, int cap) {
+    if (!g || task < 0 || task >= g->dag.num_tasks() || cap < 0 || (cap > 0 && !out)) return -MTD_ERR_INVALID_ARG;
+    const auto &d = g->dag.deps(task);
+    for (int i = 0; i < cap && i < static_cast<int>(d.size()); ++i) out[i] = d[i];
+    return static_cast<int>(d.size());
+}
+
+int mtd_graph_task_items(const mtd_graph *g, int task) {
+    if (!g || task < 0 || task >= g->dag.num_tasks()) return -MTD_ERR_INVALID_ARG;
+    return g->finalized ? g->dag.items_of(task) : 0;
+}
+
+int mtd_graph_set_trace(mtd_graph *g, int enable) {
+    if (!g) return MTD_ERR_INVALID_ARG;
+    if (g->finalized) return MTD_ERR_STATE;
+    g->trace = enable != 0;
+    return MTD_OK;
+}
+
+int mtd_graph_set_timeout(mtd_graph *g, double seconds) {
+    if (!g || !(seconds > 0.0) || seconds > 3600.0) return MTD_ERR_INVALID_ARG;
+    g->timeout_s = seconds;
+    return MTD_OK;
+}
+
+int mtd_graph_finalize(mtd_graph *g) {
+    if (!g) return MTD_ERR_INVALID_ARG;
+    if (g->finalized) return MTD_ERR_STATE;
+    if (g->dag.num_tasks() == 0) return MTD_ERR_BAD_DAG;
+    int rc = check_device(&g->device, &g->num_sms);
+    if (rc) return rc;
+
+    std::vector<DevTask> tasks;
+    std::vector<int> succ, preds;
+    int64_t cap[kNumQueues];
+    rc = g->dag.lower(tasks, succ, preds, cap);
+    if (rc) return rc;
+    std::vector<int> roots;
+    for (int t = 0; t < static_cast<int>(preds.size()); ++t)
+        if (preds[t] == 0) roots.push_back(t);
+    if (roots.empty()) return MTD_ERR_BAD_DAG;
+
+    const int nt = g->dag.num_tasks();
+    const size_t ws = size_t(g->dag.tiles()) * size_t(g->dag.tile()) * kNB;
+    g->total_items = 0;
+    for (int q = 0; q < kNumQueues; ++q) {
+        g->queue_cap[q] = cap[q];
+        g->total_items += cap[q];
+    }
+    g->trace_cap = g->trace ? g->total_items : 0;
+    bool needs_upper = false;
+    for (const auto &t : tasks)
+        if (t.op == MTD_OP_GETRF) needs_upper = true;
+
+    rc = MTD_OK;
+    rc = rc ? rc : dev_alloc(&g->d_tasks, nt);
+    rc = rc ? rc : dev_alloc(&g->d_succ, succ.size());
+    rc = rc ? rc : dev_alloc(&g->d_deps_init, nt);
+    rc = rc ? rc : dev_alloc(&g->d_deps, nt);
+    rc = rc ? rc : dev_alloc(&g->d_items_left, nt);
+    rc = rc ? rc : dev_alloc(&g->d_roots, roots.size());
+    for (int q = 0; q < kNumQueues; ++q) rc = rc ? rc : dev_alloc(&g->d_queue[q], size_t(cap[q]));
+    rc = rc ? rc : dev_alloc(&g->d_qctl, kNumQueues);
+    rc = rc ? rc : dev_alloc(&g->d_ctl, 1);
+    rc = rc ? rc : dev_alloc(&g->d_ws_lower, ws);
+    if (needs_upper) rc = rc ? rc : dev_alloc(&g->d_ws_upper, ws);
+    if (g->trace) rc = rc ? rc : dev_alloc(&g->d_trace, size_t(4 * g->trace_cap));
+    if (!rc && cudaMallocHost(reinterpret_cast<void **>(&g->h_ctl), sizeof(RunCtl)) != cudaSuccess) {
+        g->h_ctl = nullptr;
+        rc = MTD_ERR_OUT_OF_MEMORY;
+    }
+    if (!rc) {
+        bool ok = cudaMemcpy(g->d_tasks, tasks.data(), nt * sizeof(DevTask), cudaMemcpyHostToDevice) == cudaSuccess;
+        ok = ok && (succ.empty() ||
+                    cudaMemcpy(g->d_succ, succ.data(), succ.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess);
+        ok = ok && cudaMemcpy(g->d_deps_init, preds.data(), nt * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
+        ok = ok && cudaMemcpy(g->d_roots, roots.data(), roots.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
+        ok = ok && cudaMemset(g->d_ws_lower, 0, ws * sizeof(double)) == cudaSuccess;
+        if (needs_upper) ok = ok && cudaMemset(g->d_ws_upper, 0, ws * sizeof(double)) == cudaSuccess;
+        ok = ok && cudaMemset(g->d_ctl, 0, sizeof(RunCtl)) == cudaSuccess;
+        if (!ok) rc = MTD_ERR_CUDA;
+    }
+    if (!rc) rc = smem_setup<2>(g->device);
+    if (!rc) rc = smem_setup<1>(g->device);
+    if (rc) {
+        release_device(g);
+        g->d_tasks = nullptr;
+        return rc;
+    }
+    std::memset(g->h_ctl, 0, sizeof(RunCtl));
+    g->n_roots = static_cast<int>(roots.size());
+    g->finalized = true;
+    return MTD_OK;
+}
+
+int mtd_run(mtd_graph *g, double *dA, int64_t lda, void *stream, int *info_out) {
+    if (!g || !dA) return MTD_ERR_INVALID_ARG;
+    if (!g->finalized) return MTD_ERR_STATE;
+    if (lda < g->dag.n()) return MTD_ERR_INVALID_ARG;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev != g->device) return MTD_ERR_STATE;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+    RunArgs a{};
+    a.a = dA;
+    a.lda = lda;
+    a.n = g->dag.n();
+    a.tile = g->dag.tile();
+    a.tiles = g->dag.tiles();
+    a.n_tasks = g->dag.num_tasks();
+    a.tasks = g->d_tasks;
+    a.succ = g->d_succ;
+    a.deps = g->d_deps;
+    a.items_left = g->d_items_left;
+    for (int q = 0; q < kNumQueues; ++q) {
+        a.queue[q] = g->d_queue[q];
+        a.queue_cap[q] = g->queue_cap[q];
+    }
+    a.qctl = g->d_qctl;
+    a.ctl = g->d_ctl;
+    a.ws_lower = g->d_ws_lower;
+    a.ws_upper = g->d_ws_upper;
+    a.trace = g->d_trace;
+    a.trace_cap = g->trace_cap;
+    a.timeout_ns = static_cast<unsigned long long>(g->timeout_s * 1e9);
+
+    const bool vec2 = (reinterpret_cast<uintptr_t>(dA) % 16 == 0) && (lda % 2 == 0) &&
+                      (g->dag.tile() % 2 == 0) && (g->dag.n() % 2 == 0);
+    const int grid = g->num_sms;
+    g->last_grid = grid;
+    const int reset_blocks = static_cast<int>(std::min<long long>(
+        1024, std::max<long long>(1, (std::max<long long>(g->total_items, a.n_tasks) + kThreads - 1) / kThreads)));
+    reset_kernel<<<reset_blocks, kThreads, 0, s>>>(a, g->d_deps_init);
+    seed_kernel<<<1, 32, 0, s>>>(a, g->d_roots, g->n_roots);
+    if (vec2) persistent_kernel<2><<<grid, kThreads, kOpSmemBytes(), s>>>(a);
+    else persistent_kernel<1><<<grid, kThreads, kOpSmemBytes(), s>>>(a);
+    if (cudaGetLastError() != cudaSuccess) return MTD_ERR_CUDA;
+    if (cudaMemcpyAsync(g->h_ctl, g->d_ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return MTD_ERR_CUDA;
+    g->last_stream = s;
+    g->run_pending = true;
+    if (info_out) return mtd_graph_status(g, info_out);
+    return MTD_OK;
+}
+
+int mtd_graph_status(mtd_graph *g, int *info_out) {
+    if (!g) return MTD_ERR_INVALID_ARG;
+    if (info_out) *info_out = 0;
+    if (!g->run_pending) return MTD_ERR_STATE;
+    if (cudaStreamSynchronize(g->last_stream) != cudaSuccess) return MTD_ERR_CUDA;
+    const RunCtl &c = *g->h_ctl;
+    if (info_out) *info_out = (c.error != 0 && c.info != 0x7fffffff) ? c.info : 0;
+    if (c.error) return c.error;
+    if (c.tasks_done != g->dag.num_tasks()) return MTD_ERR_TIMEOUT;
+    return MTD_OK;
+}
+
+int mtd_graph_last_stats(mtd_graph *g, mtd_run_stats *out) {
+    if (!g || !out) return MTD_ERR_INVALID_ARG;
+    if (!g->run_pending) return MTD_ERR_STATE;
+    if (cudaStreamSynchronize(g->last_stream) != cudaSuccess) return MTD_ERR_CUDA;
+    out->tasks = g->h_ctl->tasks_done;
+    out->items = static_cast<int64_t>(g->h_ctl->items_done);
+    out->ctas = g->last_grid;
+    out->busy_fraction = -1.0;
+    out->span_ms = -1.0;
+    if (g->trace && g->d_trace) {
+        const long long n = std::min<long long>(static_cast<long long>(g->h_ctl->items_done), g->trace_cap);
+        std::vector<unsigned long long> rec(size_t(4 * std::max<long long>(n, 1)));
+        if (n > 0 && cudaMemcpy(rec.data(), g->d_trace, size_t(4 * n) * sizeof(unsigned long long),
+                                cudaMemcpyDeviceToHost) != cudaSuccess)
+            return MTD_ERR_CUDA;
+        if (n > 0) {
+            unsigned long long lo = ~0ull, hi = 0;
+            double busy = 0.0;
+            for (long long i = 0; i < n; ++i) {
+                lo = std::min(lo, rec[4 * i]);
+                hi = std::max(hi, rec[4 * i + 1]);
+                busy += double(rec[4 * i + 1] - rec[4 * i]);
+            }
+            const double span = double(hi - lo);
+            out->span_ms = span * 1e-6;
+            out->busy_fraction = span > 0 ? busy / (span * g->last_grid) : 0.0;
+        }
+    }
+    return MTD_OK;
+}
+
+// Raw trace of the last run: 4 words per work item (start ns, end ns, SM id,
+// task << 32 | item).  Returns the number of records copied.
+long long mtd_graph_copy_trace(mtd_graph *g, unsigned long long *out, long long cap_records) {
+    if (!g || !out || cap_records < 0) return -MTD_ERR_INVALID_ARG;
+    if (!g->trace || !g->run_pending) return -MTD_ERR_STATE;
+    if (cudaStreamSynchronize(g->last_stream) != cudaSuccess) return -MTD_ERR_CUDA;
+    const long long n = std::min(std::min<long long>(static_cast<long long>(g->h_ctl->items_done), g->trace_cap), cap_records);
+    if (n > 0 && cudaMemcpy(out, g->d_trace, size_t(4 * n) * sizeof(unsigned long long), cudaMemcpyDeviceToHost) !=
+                     cudaSuccess)
+        return -MTD_ERR_CUDA;
+    return n;
+}
+
+int mtd_graph_destroy(mtd_graph *g) {
+    if (!g) return MTD_ERR_INVALID_ARG;
+    if (g->run_pending && g->last_stream != nullptr) cudaStreamSynchronize(g->last_stream);
+    else if (g->run_pending) cudaDeviceSynchronize();
+    if (g->finalized) release_device(g);
+    delete g;
+    return MTD_OK;
+}
+
+static int tiled_driver(int kind, double *dA, int64_t n, int64_t lda, int64_t tile, void *stream, int *info_out) {
+    mtd_graph *g = nullptr;
+    int rc = mtd_graph_create(&g, kind, n, tile);
+    if (rc) return rc;
+    rc = mtd_graph_build_tiled(g);
+    if (!rc) rc = mtd_graph_finalize(g);
+    int info = 0;
+    if (!rc) rc = mtd_run(g, dA, lda, stream, &info);
+    if (info_out) *info_out = info;
+    mtd_graph_destroy(g);
+    return rc;
+}
+
+int mtd_tiled_cholesky(double *dA, int64_t n, int64_t lda, int64_t tile, void *stream, int *info_out) {
+    return tiled_driver(MTD_KIND_CHOLESKY, dA, n, lda, tile, stream, info_out);
+}
+
+int mtd_tiled_lu(double *dA, int64_t n, int64_t lda, int64_t tile, void *stream, int *info_out) {
+    return tiled_driver(MTD_KIND_LU, dA, n, lda, tile, stream, info_out);
+}
+
+}  // extern "C"

@@ -1,0 +1,191 @@
+// The persistent scheduler: one CTA per SM pops ready work items, runs the tile
+// operation, and resolves dependencies on the device.
+//
+// It replaces, for one GPU, the reference's device runtime (mustard/mustard.h:57-129,
+// mustard/broker_queue.h): the 1-thread kernel_scheduler that dequeues task ids and
+// device-launches one CUDA graph per task, the per-edge kernel_dep_update nodes that
+// decrement a successor's counter and enqueue it at zero, kernel_populate_queue, and the
+// occupancy throttle.  Differences, by design:
+//   - a task is split into independent work items (output sub-tiles / row strips) so all
+//     148 SMs can share one tile operation;
+//   - the dependency decrement is fused into the epilogue of a task's last work item;
+//   - two ready queues (critical path first) replace the single FIFO ring;
+//   - a queue is a bounded array of 64-bit slots (task << 32 | item) claimed with a CAS
+//     on `head` only while head < tail, so a consumer never claims a slot nobody has
+//     reserved; every slot is written once per run (capacity = that queue's total items);
+//   - every wait is bounded by a globaltimer deadline after which the CTA records
+//     MTD_ERR_TIMEOUT, raises the abort flag and returns.
+#pragma once
+
+#include "device_types.hpp"
+#include "tile_ops.cuh"
+
+namespace mtd {
+
+constexpr unsigned long long kEmptySlot = ~0ull;
+enum { kCmdWork = 0, kCmdExit = 1 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned long long ld_volatile(const unsigned long long *p) {
+    return *reinterpret_cast<const volatile unsigned long long *>(p);
+}
+__device__ __forceinline__ int ld_volatile(const int *p) { return *reinterpret_cast<const volatile int *>(p); }
+
+// Thread 0 of a CTA: push every work item of `task`.
+__device__ __forceinline__ void enqueue_task(const RunArgs &p, int task) {
+    const DevTask &t = p.tasks[task];
+    const int q = t.queue;
+    const unsigned long long n = static_cast<unsigned long long>(t.n_items);
+    const unsigned long long base = atomicAdd(&p.qctl[q].tail, n);
+    if (base + n > static_cast<unsigned long long>(p.queue_cap[q])) {
+        report_error(p.ctl, MTD_ERR_QUEUE, 0);
+        return;
+    }
+    volatile unsigned long long *slots = p.queue[q];
+    for (unsigned long long i = 0; i < n; ++i)
+        slots[base + i] = (static_cast<unsigned long long>(task) << 32) | i;
+}
+
+// Thread 0 of a CTA: claim one work item, waiting (bounded) while none is ready.
+__device__ __forceinline__ int pop_item(const RunArgs &p, int *task, int *item) {
+    const unsigned long long t0 = global_ns();
+    unsigned int backoff = 32;
+    while (true) {
+        if (ld_volatile(&p.ctl->abort)) return kCmdExit;
+        if (ld_volatile(&p.ctl->tasks_done) >= p.n_tasks) return kCmdExit;
+        bool retry = false;
+        for (int q = 0; q < kNumQueues; ++q) {
+            const unsigned long long h = ld_volatile(&p.qctl[q].head);
+            const unsigned long long tl = ld_volatile(&p.qctl[q].tail);
+            if (h >= tl) continue;
+            if (atomicCAS(&p.qctl[q].head, h, h + 1) != h) {
+                retry = true;  // lost the race for this slot: look again at once
+                break;
+            }
+            const unsigned long long *slot = p.queue[q] + h;
+            unsigned long long v;
+            while ((v = ld_volatile(slot)) == kEmptySlot) {
+                if (global_ns() - t0 > p.timeout_ns) {
+                    report_error(p.ctl, MTD_ERR_TIMEOUT, 0);
+                    return kCmdExit;
+                }
+                __nanosleep(20);
+            }
+            __threadfence();
+            *task = static_cast<int>(v >> 32);
+            *item = static_cast<int>(v & 0xffffffffull);
+            return kCmdWork;
+        }
+        if (retry) continue;
+        if (global_ns() - t0 > p.timeout_ns) {
+            report_error(p.ctl, MTD_ERR_TIMEOUT, 0);
+            return kCmdExit;
+        }
+        __nanosleep(backoff);
+        if (backoff < 256) backoff *= 2;
+    }
+}
+
+// Thread 0 of a CTA, after the whole CTA finished an item of `task`.
+__device__ __forceinline__ void complete_item(const RunArgs &p, int task) {
+    __threadfence();
+    if (atomicSub(&p.items_left[task], 1) != 1) return;
+    __threadfence();
+    const DevTask &t = p.tasks[task];
+    for (int s = 0; s < t.succ_count; ++s) {
+        const int succ = p.succ[t.succ_begin + s];
+        if (atomicSub(&p.deps[succ], 1) == 1) enqueue_task(p, succ);
+    }
+    __threadfence();
+    atomicAdd(&p.ctl->tasks_done, 1);
+}
+
+template <int VEC>
+__device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int item, double *smem) {
+    switch (t.op) {
+    case MTD_OP_POTRF: return op_potrf<VEC>(p, t, smem);
+    case MTD_OP_TRSM_RLT: return op_trsm_rlt<VEC>(p, t, item, smem);
+    case MTD_OP_SYRK_LN: return op_syrk_ln<VEC>(p, t, item, smem);
+    case MTD_OP_GEMM_NT: return op_gemm_nt<VEC>(p, t, item, smem);
+    case MTD_OP_GETRF: return op_getrf<VEC>(p, t, smem);
+    case MTD_OP_TRSM_LLNU: return op_trsm_llnu<VEC>(p, t, item, smem);
+    case MTD_OP_TRSM_RUN: return op_trsm_run<VEC>(p, t, item, smem);
+    case MTD_OP_GEMM_NN: return op_gemm_nn<VEC>(p, t, item, smem);
+    default:
+        if (threadIdx.x == 0) report_error(p.ctl, MTD_ERR_INVALID_ARG, 0);
+        return MTD_ERR_INVALID_ARG;
+    }
+}
+
+template <int VEC>
+__global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const RunArgs p) {
+    extern __shared__ __align__(128) double smem[];
+    __shared__ int s_cmd, s_task, s_item;
+    while (true) {
+        if (threadIdx.x == 0) {
+            int tk = 0, it = 0;
+            s_cmd = pop_item(p, &tk, &it);
+            s_task = tk;
+            s_item = it;
+        }
+        __syncthreads();
+        const int cmd = s_cmd, task = s_task, item = s_item;
+        if (cmd != kCmdWork) break;
+        const unsigned long long t_start = p.trace ? global_ns() : 0ull;
+        const DevTask t = p.tasks[task];
+        const int st = dispatch<VEC>(p, t, item, smem);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (st == 0) complete_item(p, task);
+            const long long slot = static_cast<long long>(atomicAdd(&p.ctl->items_done, 1ull));
+            if (p.trace && slot < p.trace_cap) {
+                unsigned int smid;
+                asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+                unsigned long long *rec = p.trace + 4 * slot;
+                rec[0] = t_start;
+                rec[1] = global_ns();
+                rec[2] = smid;
+                rec[3] = (static_cast<unsigned long long>(task) << 32) | static_cast<unsigned int>(item);
+            }
+        }
+    }
+}
+
+// Per-run reset: counters from their initial values, queues empty.
+__global__ void reset_kernel(const RunArgs p, const int *deps_init) {
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    const long long tid = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (long long i = tid; i < p.n_tasks; i += stride) {
+        p.deps[i] = deps_init[i];
+        p.items_left[i] = p.tasks[i].n_items;
+    }
+    for (int q = 0; q < kNumQueues; ++q)
+        for (long long i = tid; i < p.queue_cap[q]; i += stride) p.queue[q][i] = kEmptySlot;
+    if (tid == 0) {
+        for (int q = 0; q < kNumQueues; ++q) {
+            p.qctl[q].head = 0;
+            p.qctl[q].tail = 0;
+        }
+        p.ctl->tasks_done = 0;
+        p.ctl->error = 0;
+        p.ctl->info = 0x7fffffff;
+        p.ctl->abort = 0;
+        p.ctl->items_done = 0;
+    }
+}
+
+// Seed the queues with the tasks that have no predecessor (kernel_populate_queue,
+// mustard/mustard.h:87-95).
+__global__ void seed_kernel(const RunArgs p, const int *roots, int n_roots) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        for (int r = 0; r < n_roots; ++r) enqueue_task(p, roots[r]);
+        __threadfence();
+    }
+}
+
+}  // namespace mtd

@@ -1,0 +1,416 @@
+// FP64 tile operations executed by one persistent CTA per work item.
+//
+// Each operation replaces one captured cuBLAS / cuSOLVER call of the reference
+// (mustard/cholesky_mustard.cu:238-387, mustard/lu_mustard.cu:361-522).  The dense
+// updates are tensor-core DMMA block products (mma.cuh).  The diagonal factorisations
+// are left-looking blocked algorithms with kNB-wide diagonal blocks factored in shared
+// memory; while a block is in shared memory its triangular inverse is formed and left in
+// a per-step workspace, so every triangular solve of the step -- inside the diagonal
+// task and in the TRSM tasks that follow it -- becomes a block product as well.
+#pragma once
+
+#include "device_types.hpp"
+#include "mma.cuh"
+#include "../../include/mustard_b200.h"
+
+namespace mtd {
+
+constexpr int kDiagLd = kNB + 1;  // shared-memory leading dimension of a diagonal block
+
+__device__ __forceinline__ void block_fence_sync() {
+    __threadfence_block();
+    __syncthreads();
+}
+
+struct TileView {
+    double *a;
+    int64_t lda, n, tile;
+    __device__ __forceinline__ double *ptr(int i, int j) const { return a + int64_t(i) * tile + int64_t(j) * tile * lda; }
+    __device__ __forceinline__ int ext(int t) const {
+        const int64_t e = n - int64_t(t) * tile;
+        return static_cast<int>(e < tile ? e : tile);
+    }
+};
+
+__device__ __forceinline__ void report_error(RunCtl *ctl, int code, int info) {
+    if (info > 0) atomicMin(&ctl->info, info);
+    atomicCAS(&ctl->error, 0, code);
+    __threadfence();
+    atomicExch(&ctl->abort, 1);
+}
+
+// X = T^-1 for a jn x jn lower-triangular T read through tl(i, l) (i >= l); unit
+// diagonal when UNIT.  Four lanes per column, 64 columns per CTA; rows swept top-down.
+template <bool UNIT, typename TL>
+__device__ __forceinline__ void lower_inverse(int jn, TL tl, double *X) {
+    const int c = threadIdx.x >> 2;
+    const int q = threadIdx.x & 3;
+    for (int i = 0; i < jn; ++i) {
+        double part = 0.0;
+        if (c < i)
+            for (int l = c + q; l < i; l += 4) part += tl(i, l) * X[l + c * kDiagLd];
+        part += __shfl_xor_sync(0xffffffffu, part, 1);
+        part += __shfl_xor_sync(0xffffffffu, part, 2);
+        if (q == 0 && c < jn) {
+            double v;
+            if (c > i) v = 0.0;
+            else if (UNIT) v = (c == i) ? 1.0 : -part;
+            else v = (c == i) ? 1.0 / tl(i, i) : -part / tl(i, i);
+            X[i + c * kDiagLd] = v;
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+}
+
+// Cholesky of the jn x jn diagonal block at Ad (lower), in shared memory.  Writes L back
+// (lower triangle only; the strict upper triangle of the tile is never touched, as with
+// LAPACK's uplo = 'L') and L^-1 to Wd (ld = ldw, full block with zeros above).
+__device__ __forceinline__ int factor_chol_diag(const RunArgs &p, double *Ad, int jn, double *Wd,
+                                                double *smem, int info_base) {
+    const int tid = threadIdx.x;
+    double *D = smem;
+    double *X = smem + kNB * kDiagLd;
+    const int64_t lda = p.lda;
+    for (int e = tid; e < jn * jn; e += kThreads) {
+        const int r = e % jn, c = e / jn;
+        D[r + c * kDiagLd] = (r >= c) ? ld_cg(Ad + r + int64_t(c) * lda) : 0.0;
+    }
+    __syncthreads();
+    for (int j = 0; j < jn; ++j) {
+        const double djj = D[j + j * kDiagLd];
+        if (!(djj > 0.0)) {  // also catches NaN
+            if (tid == 0) report_error(p.ctl, MTD_ERR_NOT_POSITIVE_DEFINITE, info_base + j + 1);
+            return MTD_ERR_NOT_POSITIVE_DEFINITE;
+        }
+        const double s = sqrt(djj);
+        const double rs = 1.0 / s;
+        __syncthreads();
+        for (int r = j + 1 + tid; r < jn; r += kThreads) D[r + j * kDiagLd] *= rs;
+        if (tid == 0) D[j + j * kDiagLd] = s;
+        __syncthreads();
+        const int m = jn - j - 1;
+        for (int e = tid; e < m * m; e += kThreads) {
+            const int r = j + 1 + e % m, c = j + 1 + e / m;
+            if (r >= c) D[r + c * kDiagLd] -= D[r + j * kDiagLd] * D[c + j * kDiagLd];
+        }
+        __syncthreads();
+    }
+    lower_inverse<false>(jn, [&](int i, int l) { return D[i + l * kDiagLd]; }, X);
+    const int64_t ldw = p.tile;
+    for (int e = tid; e < jn * jn; e += kThreads) {
+        const int r = e % jn, c = e / jn;
+        if (r >= c) Ad[r + int64_t(c) * lda] = D[r + c * kDiagLd];
+        Wd[r + int64_t(c) * ldw] = X[r + c * kDiagLd];
+    }
+    return 0;
+}
+
+// No-pivot LU of the jn x jn diagonal block at Ad, in shared memory (what
+// cusolverDnDgetrf computes with ipiv = NULL).  Writes L\U back, L^-1 (unit lower) to
+// WLd and U^-1 (upper) to WUd.
+__device__ __forceinline__ int factor_lu_diag(const RunArgs &p, double *Ad, int jn, double *WLd, double *WUd,
+                                              double *smem, int info_base) {
+    const int tid = threadIdx.x;
+    double *D = smem;
+    double *XL = smem + kNB * kDiagLd;
+    double *XU = smem + 2 * kNB * kDiagLd;
+    const int64_t lda = p.lda;
+    for (int e = tid; e < jn * jn; e += kThreads) {
+        const int r = e % jn, c = e / jn;
+        D[r + c * kDiagLd] = ld_cg(Ad + r + int64_t(c) * lda);
+    }
+    __syncthreads();
+    for (int j = 0; j < jn; ++j) {
+        const double piv = D[j + j * kDiagLd];
+        if (piv == 0.0) {
+            if (tid == 0) report_error(p.ctl, MTD_ERR_SINGULAR, info_base + j + 1);
+            return MTD_ERR_SINGULAR;
+        }
+        const double rp = 1.0 / piv;
+        for (int r = j + 1 + tid; r < jn; r += kThreads) D[r + j * kDiagLd] *= rp;
+        __syncthreads();
+        const int m = jn - j - 1;
+        for (int e = tid; e < m * m; e += kThreads) {
+            const int r = j + 1 + e % m, c = j + 1 + e / m;
+            D[r + c * kDiagLd] -= D[r + j * kDiagLd] * D[j + c * kDiagLd];
+        }
+        __syncthreads();
+    }
+    lower_inverse<true>(jn, [&](int i, int l) { return D[i + l * kDiagLd]; }, XL);
+    // U^-1 = ((U^T)^-1)^T, and U^T is lower triangular.
+    lower_inverse<false>(jn, [&](int i, int l) { return D[l + i * kDiagLd]; }, XU);
+    const int64_t ldw = p.tile;
+    for (int e = tid; e < jn * jn; e += kThreads) {
+        const int r = e % jn, c = e / jn;
+        Ad[r + int64_t(c) * lda] = D[r + c * kDiagLd];
+        WLd[r + int64_t(c) * ldw] = XL[r + c * kDiagLd];
+        WUd[r + int64_t(c) * ldw] = XU[c + r * kDiagLd];
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------
+// POTRF(k,k): left-looking blocked Cholesky of one diagonal tile on one CTA.
+// ---------------------------------------------------------------------------------
+template <int VEC>
+__device__ int op_potrf(const RunArgs &p, const DevTask &t, double *smem) {
+    using Mn = BlockMma<64, 64, 2, 4, kBNContig, VEC>;
+    const TileView tv{p.a, p.lda, p.n, p.tile};
+    const int k = t.wi;
+    const int n = tv.ext(k);
+    double *A = tv.ptr(k, k);
+    double *W = p.ws_lower + int64_t(k) * p.tile * kNB;
+    const int64_t lda = p.lda;
+    for (int jb = 0; jb < n; jb += kNB) {
+        const int jn = min(kNB, n - jb);
+        if (jb > 0) {
+            // A[jb:n, jb:jb+jn] -= A[jb:n, 0:jb] * A[jb:jb+jn, 0:jb]^T (lower part of the block)
+            for (int r0 = jb; r0 < n; r0 += 64) {
+                const int mm = min(64, n - r0);
+                Mn m;
+                m.zero();
+                m.run(smem, A + r0, lda, A + jb, lda, mm, jn, jb);
+                m.sub_from(A + r0 + int64_t(jb) * lda, lda, mm, jn, r0 == jb, 0, 0);
+            }
+            block_fence_sync();
+        }
+        const int st = factor_chol_diag(p, A + jb + int64_t(jb) * lda, jn, W + jb, smem,
+                                        static_cast<int>(int64_t(k) * p.tile) + jb);
+        if (st) return st;
+        block_fence_sync();
+        // A[jb+jn:n, jb:jb+jn] = A[jb+jn:n, jb:jb+jn] * L_jj^-T
+        for (int r0 = jb + jn; r0 < n; r0 += 64) {
+            const int mm = min(64, n - r0);
+            Mn m;
+            m.zero();
+            m.run(smem, A + r0 + int64_t(jb) * lda, lda, W + jb, p.tile, mm, jn, jn);
+            m.store_to(A + r0 + int64_t(jb) * lda, lda, mm, jn);
+        }
+        block_fence_sync();
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------
+// GETRF(k,k) without pivoting: left-looking (Crout) blocked LU on one CTA.
+// ---------------------------------------------------------------------------------
+template <int VEC>
+__device__ int op_getrf(const RunArgs &p, const DevTask &t, double *smem) {
+    using Mk = BlockMma<64, 64, 2, 4, kBKContig, VEC>;
+    const TileView tv{p.a, p.lda, p.n, p.tile};
+    const int k = t.wi;
+    const int n = tv.ext(k);
+    double *A = tv.ptr(k, k);
+    double *WL = p.ws_lower + int64_t(k) * p.tile * kNB;
+    double *WU = p.ws_upper + int64_t(k) * p.tile * kNB;
+    const int64_t lda = p.lda;
+    for (int jb = 0; jb < n; jb += kNB) {
+        const int jn = min(kNB, n - jb);
+        if (jb > 0) {
+            // block column: A[jb:n, jb:jb+jn] -= A[jb:n, 0:jb] * A[0:jb, jb:jb+jn]
+            for (int r0 = jb; r0 < n; r0 += 64) {
+                const int mm = min(64, n - r0);
+                Mk m;
+                m.zero();
+                m.run(smem, A + r0, lda, A + int64_t(jb) * lda, lda, mm, jn, jb);
+                m.sub_from(A + r0 + int64_t(jb) * lda, lda, mm, jn);
+            }
+            // block row: A[jb:jb+jn, jb+jn:n] -= A[jb:jb+jn, 0:jb] * A[0:jb, jb+jn:n]
+            for (int c0 = jb + jn; c0 < n; c0 += 64) {
+                const int nn = min(64, n - c0);
+                Mk m;
+                m.zero();
+                m.run(smem, A + jb, lda, A + int64_t(c0) * lda, lda, jn, nn, jb);
+                m.sub_from(A + jb + int64_t(c0) * lda, lda, jn, nn);
+            }
+            block_fence_sync();
+        }
+        const int st = factor_lu_diag(p, A + jb + int64_t(jb) * lda, jn, WL + jb, WU + jb, smem,
+                                      static_cast<int>(int64_t(k) * p.tile) + jb);
+        if (st) return st;
+        block_fence_sync();
+        // L panel: A[jb+jn:n, jb:jb+jn] = A[...] * U_jj^-1
+        for (int r0 = jb + jn; r0 < n; r0 += 64) {
+            const int mm = min(64, n - r0);
+            Mk m;
+            m.zero();
+            m.run(smem, A + r0 + int64_t(jb) * lda, lda, WU + jb, p.tile, mm, jn, jn);
+            m.store_to(A + r0 + int64_t(jb) * lda, lda, mm, jn);
+        }
+        // U row: A[jb:jb+jn, jb+jn:n] = L_jj^-1 * A[...]
+        for (int c0 = jb + jn; c0 < n; c0 += 64) {
+            const int nn = min(64, n - c0);
+            Mk m;
+            m.zero();
+            m.run(smem, WL + jb, p.tile, A + jb + int64_t(c0) * lda, lda, jn, nn, jn);
+            m.store_to(A + jb + int64_t(c0) * lda, lda, jn, nn);
+        }
+        block_fence_sync();
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------
+// TRSM work items: kPanelRows-row (or -column) strips of the written tile, solved
+// left-looking over the kNB-wide diagonal blocks of the triangular tile.
+// ---------------------------------------------------------------------------------
+
+// A(i,k) = A(i,k) * L(k,k)^-T   (cublasDtrsm R, L, T, NonUnit; cholesky_mustard.cu:281)
+template <int VEC>
+__device__ int op_trsm_rlt(const RunArgs &p, const DevTask &t, int item, double *smem) {
+    using Mn = BlockMma<64, 64, 2, 4, kBNContig, VEC>;
+    const TileView tv{p.a, p.lda, p.n, p.tile};
+    const int k = t.aj;
+    const int r0 = item * kPanelRows;
+    const int mm = min(kPanelRows, tv.ext(t.wi) - r0);
+    const int nk = tv.ext(k);
+    const int64_t lda = p.lda;
+    double *X = tv.ptr(t.wi, t.wj) + r0;
+    const double *L = tv.ptr(k, k);
+    const double *W = p.ws_lower + int64_t(k) * p.tile * kNB;
+    for (int jb = 0; jb < nk; jb += kNB) {
+        const int jn = min(kNB, nk - jb);
+        if (jb > 0) {
+            Mn m;
+            m.zero();
+            m.run(smem, X, lda, L + jb, lda, mm, jn, jb);
+            m.sub_from(X + int64_t(jb) * lda, lda, mm, jn);
+            block_fence_sync();
+        }
+        Mn m;
+        m.zero();
+        m.run(smem, X + int64_t(jb) * lda, lda, W + jb, p.tile, mm, jn, jn);
+        m.store_to(X + int64_t(jb) * lda, lda, mm, jn);
+        block_fence_sync();
+    }
+    return 0;
+}
+
+// A(i,k) = A(i,k) * U(k,k)^-1   (cublasDtrsm R, U, N, NonUnit; lu_mustard.cu:459)
+template <int VEC>
+__device__ int op_trsm_run(const RunArgs &p, const DevTask &t, int item, double *smem) {
+    using Mk = BlockMma<64, 64, 2, 4, kBKContig, VEC>;
+    const TileView tv{p.a, p.lda, p.n, p.tile};
+    const int k = t.aj;
+    const int r0 = item * kPanelRows;
+    const int mm = min(kPanelRows, tv.ext(t.wi) - r0);
+    const int nk = tv.ext(k);
+    const int64_t lda = p.lda;
+    double *X = tv.ptr(t.wi, t.wj) + r0;
+    const double *U = tv.ptr(k, k);
+    const double *W = p.ws_upper + int64_t(k) * p.tile * kNB;
+    for (int jb = 0; jb < nk; jb += kNB) {
+        const int jn = min(kNB, nk - jb);
+        if (jb > 0) {
+            Mk m;
+            m.zero();
+            m.run(smem, X, lda, U + int64_t(jb) * lda, lda, mm, jn, jb);
+            m.sub_from(X + int64_t(jb) * lda, lda, mm, jn);
+            block_fence_sync();
+        }
+        Mk m;
+        m.zero();
+        m.run(smem, X + int64_t(jb) * lda, lda, W + jb, p.tile, mm, jn, jn);
+        m.store_to(X + int64_t(jb) * lda, lda, mm, jn);
+        block_fence_sync();
+    }
+    return 0;
+}
+
+// A(k,i) = L(k,k)^-1 * A(k,i), unit diagonal   (cublasDtrsm L, L, N, Unit; lu_mustard.cu:413)
+template <int VEC>
+__device__ int op_trsm_llnu(const RunArgs &p, const DevTask &t, int item, double *smem) {
+    using Mk = BlockMma<64, 64, 2, 4, kBKContig, VEC>;
+    const TileView tv{p.a, p.lda, p.n, p.tile};
+    const int k = t.ai;
+    const int c0 = item * kPanelRows;
+    const int nc = min(kPanelRows, tv.ext(t.wj) - c0);
+    const int nk = tv.ext(k);
+    const int64_t lda = p.lda;
+    double *X = tv.ptr(t.wi, t.wj) + int64_t(c0) * lda;
+    const double *L = tv.ptr(k, k);
+    const double *W = p.ws_lower + int64_t(k) * p.tile * kNB;
+    for (int jb = 0; jb < nk; jb += kNB) {
+        const int jn = min(kNB, nk - jb);
+        if (jb > 0) {
+            Mk m;
+            m.zero();
+            m.run(smem, L + jb, lda, X, lda, jn, nc, jb);
+            m.sub_from(X + jb, lda, jn, nc);
+            block_fence_sync();
+        }
+        Mk m;
+        m.zero();
+        m.run(smem, W + jb, p.tile, X + jb, lda, jn, nc, jn);
+        m.store_to(X + jb, lda, jn, nc);
+        block_fence_sync();
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------
+// Update work items: one kGemmTile x kGemmTile output block each.
+// ---------------------------------------------------------------------------------
+
+// A(j,i) -= A(j,k) A(i,k)^T   (cublasGemmEx N, T; cholesky_mustard.cu:376)
+template <int VEC>
+__device__ int op_gemm_nt(const RunArgs &p, const DevTask &t, int item, double *smem) {
+    using Mg = BlockMma<kGemmTile, kGemmTile, 2, 4, kBNContig, VEC>;
+    const TileView tv{p.a, p.lda, p.n, p.tile};
+    const int M = tv.ext(t.wi), N = tv.ext(t.wj), K = tv.ext(t.aj);
+    const int nbn = (N + kGemmTile - 1) / kGemmTile;
+    const int r0 = (item / nbn) * kGemmTile, c0 = (item % nbn) * kGemmTile;
+    const int mm = min(kGemmTile, M - r0), nn = min(kGemmTile, N - c0);
+    Mg m;
+    m.zero();
+    m.run(smem, tv.ptr(t.ai, t.aj) + r0, p.lda, tv.ptr(t.bi, t.bj) + c0, p.lda, mm, nn, K);
+    m.sub_from(tv.ptr(t.wi, t.wj) + r0 + int64_t(c0) * p.lda, p.lda, mm, nn);
+    return 0;
+}
+
+// A(i,j) -= A(i,k) A(k,j)   (cublasGemmEx N, N; lu_mustard.cu:511)
+template <int VEC>
+__device__ int op_gemm_nn(const RunArgs &p, const DevTask &t, int item, double *smem) {
+    using Mg = BlockMma<kGemmTile, kGemmTile, 2, 4, kBKContig, VEC>;
+    const TileView tv{p.a, p.lda, p.n, p.tile};
+    const int M = tv.ext(t.wi), N = tv.ext(t.wj), K = tv.ext(t.aj);
+    const int nbn = (N + kGemmTile - 1) / kGemmTile;
+    const int r0 = (item / nbn) * kGemmTile, c0 = (item % nbn) * kGemmTile;
+    const int mm = min(kGemmTile, M - r0), nn = min(kGemmTile, N - c0);
+    Mg m;
+    m.zero();
+    m.run(smem, tv.ptr(t.ai, t.aj) + r0, p.lda, tv.ptr(t.bi, t.bj) + int64_t(c0) * p.lda, p.lda, mm, nn, K);
+    m.sub_from(tv.ptr(t.wi, t.wj) + r0 + int64_t(c0) * p.lda, p.lda, mm, nn);
+    return 0;
+}
+
+// A(i,i) -= A(i,k) A(i,k)^T, lower triangle only   (cublasDsyrk L, N; cholesky_mustard.cu:327)
+template <int VEC>
+__device__ int op_syrk_ln(const RunArgs &p, const DevTask &t, int item, double *smem) {
+    using Mg = BlockMma<kGemmTile, kGemmTile, 2, 4, kBNContig, VEC>;
+    const TileView tv{p.a, p.lda, p.n, p.tile};
+    const int M = tv.ext(t.wi), K = tv.ext(t.aj);
+    int pb = 0;
+    while ((pb + 1) * (pb + 2) / 2 <= item) ++pb;
+    const int qb = item - pb * (pb + 1) / 2;
+    const int r0 = pb * kGemmTile, c0 = qb * kGemmTile;
+    const int mm = min(kGemmTile, M - r0), nn = min(kGemmTile, M - c0);
+    const double *A = tv.ptr(t.ai, t.aj);
+    Mg m;
+    m.zero();
+    m.run(smem, A + r0, p.lda, A + c0, p.lda, mm, nn, K);
+    m.sub_from(tv.ptr(t.wi, t.wj) + r0 + int64_t(c0) * p.lda, p.lda, mm, nn, pb == qb, 0, 0);
+    return 0;
+}
+
+// Shared memory (bytes) the largest operation needs.
+constexpr int kOpSmemBytes() {
+    constexpr int g1 = BlockMma<kGemmTile, kGemmTile, 2, 4, kBNContig, 2>::SMEM_DOUBLES;
+    constexpr int g2 = BlockMma<kGemmTile, kGemmTile, 2, 4, kBKContig, 2>::SMEM_DOUBLES;
+    constexpr int diag = 3 * kNB * kDiagLd;
+    constexpr int m = g1 > g2 ? g1 : g2;
+    return 8 * (m > diag ? m : diag);
+}
+
+}  // namespace mtd

@@ -1,0 +1,129 @@
+"""C-ABI library: loads, exports every declared symbol, and builds the reference's DAGs
+on the host exactly as the oracle's restatement of getSubgraphDependencies does."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from oracle import tiled
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols():
+    with open(os.path.join(ROOT, "include", "mustard_b200.h")) as f:
+        text = f.read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(mtd_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(mtd):
+    lib = ctypes.CDLL(mtd.lib_path())
+    names = _declared_symbols()
+    assert len(names) >= 20
+    for name in names:
+        assert hasattr(lib, name), name
+    # and the Python binding declares a signature for each of them
+    from mustard_b200 import _capi
+    assert set(names) <= set(_capi.SIGNATURES)
+
+
+def test_abi_version_and_strerror(mtd):
+    lib = mtd.lib()
+    assert lib.mtd_abi_version() == 1
+    for code in range(11):
+        assert lib.mtd_strerror(code)
+    assert lib.mtd_strerror(0) == b"ok"
+
+
+def _oracle_ops(kind):
+    return {"POTRF": mtd_op("OP_POTRF"), "TRSM_RLT": mtd_op("OP_TRSM_RLT"), "SYRK": mtd_op("OP_SYRK_LN"),
+            "GEMM_NT": mtd_op("OP_GEMM_NT"), "GETRF": mtd_op("OP_GETRF"), "TRSM_LLNU": mtd_op("OP_TRSM_LLNU"),
+            "TRSM_RUN": mtd_op("OP_TRSM_RUN"), "GEMM_NN": mtd_op("OP_GEMM_NN")}
+
+
+def mtd_op(name):
+    import mustard_b200
+    return getattr(mustard_b200, name)
+
+
+@pytest.mark.parametrize("kind", ["chol", "lu"])
+@pytest.mark.parametrize("n,b", [(600, 300), (600, 100), (1000, 128), (24000, 2048), (24000, 1000), (4000, 125)])
+def test_build_tiled_matches_oracle_dependencies(mtd, kind, n, b):
+    k = mtd.KIND_CHOLESKY if kind == "chol" else mtd.KIND_LU
+    g = mtd.TaskGraph(k, n, b).build_tiled()
+    t = (n + b - 1) // b
+    tasks = tiled.cholesky_tasks(t) if kind == "chol" else tiled.lu_tasks(t)
+    want = tiled.subgraph_dependencies(tasks)
+    assert g.num_tasks == len(tasks)
+    for i in range(len(tasks)):
+        assert g.deps(i) == want[i], i
+    g.close()
+
+
+def test_creator_mirror_records_reference_calls(mtd):
+    # The reference driver's capture sequence for Cholesky T=3 (cholesky_mustard.cu:224-395).
+    c = mtd.TiledGraphCreator(mtd.KIND_CUSTOM, 90, 30)
+    ops = _oracle_ops("chol")
+    for op, write, reads in tiled.cholesky_tasks(3):
+        c.beginCaptureOperation(ops[op], write, reads)
+        c.endCaptureOperation()
+    assert c.subgraphDependencies == tiled.subgraph_dependencies(tiled.cholesky_tasks(3))
+    with pytest.raises(mtd.MtdError):
+        c.endCaptureOperation()
+
+
+def test_custom_graph_adds_write_after_read_edges(mtd):
+    g = mtd.TaskGraph(mtd.KIND_CUSTOM, 300, 100)
+    g.add_task(mtd.OP_POTRF, (0, 0), [(0, 0)])                    # 0
+    g.add_task(mtd.OP_TRSM_RLT, (1, 0), [(0, 0), (1, 0)])         # 1 reads (0,0)
+    g.add_task(mtd.OP_POTRF, (0, 0), [(0, 0)])                    # 2 overwrites (0,0)
+    assert g.deps(2) == [0, 1]  # last writer 0, plus the reader 1 (write-after-read)
+
+
+@pytest.mark.parametrize("op,write,reads", [
+    ("OP_POTRF", (0, 1), [(0, 1)]),                 # off-diagonal POTRF
+    ("OP_GEMM_NT", (2, 1), [(2, 1), (2, 0)]),       # missing operand
+    ("OP_GEMM_NT", (2, 1), [(2, 1), (1, 0), (2, 0)]),  # operands swapped
+    ("OP_TRSM_RLT", (1, 0), [(1, 1), (1, 0)]),      # triangular tile not (k,k) of column k
+    ("OP_SYRK_LN", (1, 1), [(1, 0)]),               # output tile not read
+    ("OP_GEMM_NN", (1, 1), [(1, 0), (1, 1), (1, 1)]),
+    ("OP_POTRF", (5, 5), [(5, 5)]),                 # outside the matrix
+])
+def test_invalid_tasks_rejected(mtd, op, write, reads):
+    g = mtd.TaskGraph(mtd.KIND_CUSTOM, 300, 100)
+    with pytest.raises(mtd.MtdError) as e:
+        g.add_task(getattr(mtd, op), write, reads)
+    assert e.value.status == 1
+
+
+def test_invalid_graph_arguments(mtd):
+    for n, b in [(0, 1), (10, 0), (10, 11), (-5, 2)]:
+        with pytest.raises(mtd.MtdError):
+            mtd.TaskGraph(mtd.KIND_LU, n, b)
+    g = mtd.TaskGraph(mtd.KIND_LU, 100, 10).build_tiled()
+    with pytest.raises(mtd.MtdError) as e:
+        g.build_tiled()
+    assert e.value.status == 2
+
+
+def test_finalize_without_gpu_reports_no_device(mtd):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    g = mtd.TaskGraph(mtd.KIND_CHOLESKY, 600, 300).build_tiled()
+    with pytest.raises(mtd.MtdError) as e:
+        g.finalize()
+    assert e.value.status in (3, 8)
+
+
+def test_trsm_needs_matching_diagonal_factorisation(mtd):
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("finalize checks the device first")
+    g = mtd.TaskGraph(mtd.KIND_CUSTOM, 200, 100)
+    g.add_task(mtd.OP_TRSM_RLT, (1, 0), [(0, 0), (1, 0)])
+    with pytest.raises(mtd.MtdError) as e:
+        g.finalize()
+    assert e.value.status == 7

@@ -1,0 +1,174 @@
+"""Whole tiled factorisations on the GPU against the oracle (the reference's task list
+run sequentially with LAPACK/BLAS tiles), the reference's --verify criterion, and
+LAPACK.  FP64 parity bar: max |diff| / max |oracle| <= 1e-12."""
+import numpy as np
+import pytest
+
+from oracle import gen, tiled, verify
+from tests.gpu_util import from_dev, rel_diff, to_dev
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def factor(mtd, a, tile, kind, trace=False):
+    g = mtd.TaskGraph(mtd.KIND_CHOLESKY if kind == "chol" else mtd.KIND_LU, a.shape[0], tile).build_tiled()
+    if trace:
+        g.set_trace(True)
+    g.finalize()
+    d = to_dev(a)
+    info = g.run(d)
+    return from_dev(d), info, g
+
+
+def oracle_factor(a, tile, kind):
+    f = a.copy(order="F")
+    assert tiled.tiled_factor(f, tile, kind) == 0
+    return f
+
+
+@pytest.mark.parametrize("kind", ["chol", "lu"])
+def test_reference_config_n600_t2(mtd, kind):
+    # cholesky_mustard / lu_mustard -n=600 -t=2 --subgraph --verify (README.md:168-169)
+    a = gen.ref_spd(600)
+    out, info, g = factor(mtd, a, 300, kind)
+    assert info == 0
+    ref = oracle_factor(a, 300, kind)
+    if kind == "chol":
+        assert rel_diff(np.tril(out), np.tril(ref)) <= TOL
+        assert np.array_equal(np.triu(out, 1), np.triu(a, 1))
+        err = verify.ref_error_chol(a, out)
+    else:
+        assert rel_diff(out, ref) <= TOL
+        err = verify.ref_error_lu(a, out)
+    assert err <= verify.REF_TOLERANCE  # include/verify.h:69,127
+    g.close()
+
+
+@pytest.mark.parametrize("kind", ["chol", "lu"])
+@pytest.mark.parametrize("n,tile", [(1000, 384), (1030, 512), (2048, 512), (15, 3), (301, 100), (640, 128), (257, 64)])
+def test_tiled_parity(mtd, kind, n, tile):
+    a = gen.spd_input(n, 5) if kind == "chol" else gen.lu_input(n, 5)
+    out, info, g = factor(mtd, a, tile, kind)
+    assert info == 0
+    ref = oracle_factor(a, tile, kind)
+    if kind == "chol":
+        assert rel_diff(np.tril(out), np.tril(ref)) <= TOL
+        assert np.array_equal(np.triu(out, 1), np.triu(a, 1))
+        assert verify.normwise_residual_chol(a, out) < 1e-14
+    else:
+        assert rel_diff(out, ref) <= TOL
+        assert verify.normwise_residual_lu(a, out) < 1e-14
+    g.close()
+
+
+@pytest.mark.parametrize("kind", ["chol", "lu"])
+def test_repeat_runs_bitwise_identical(mtd, kind):
+    a = gen.spd_input(1200, 9) if kind == "chol" else gen.lu_input(1200, 9)
+    g = mtd.TaskGraph(mtd.KIND_CHOLESKY if kind == "chol" else mtd.KIND_LU, 1200, 256).build_tiled().finalize()
+    outs = []
+    for _ in range(3):
+        d = to_dev(a)
+        g.run(d)
+        outs.append(from_dev(d))
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[1], outs[2])
+    g.close()
+
+
+def test_not_positive_definite_reports_info(mtd):
+    n, tile = 600, 200
+    a = gen.spd_input(n, 4)
+    a[450, 450] = -1.0  # leading minor of order 451 is not positive definite
+    g = mtd.TaskGraph(mtd.KIND_CHOLESKY, n, tile).build_tiled().finalize()
+    d = to_dev(a)
+    with pytest.raises(mtd.MtdError) as e:
+        g.run(d)
+    assert e.value.status == 5
+    assert e.value.info == 451
+    # the context stays usable: a good matrix factors afterwards
+    d = to_dev(gen.spd_input(n, 4))
+    assert g.run(d) == 0
+    g.close()
+
+
+def test_zero_pivot_reports_info(mtd):
+    n, tile = 300, 100
+    a = np.asfortranarray(np.eye(n) * 2.0)
+    a[130, 130] = 0.0
+    g = mtd.TaskGraph(mtd.KIND_LU, n, tile).build_tiled().finalize()
+    with pytest.raises(mtd.MtdError) as e:
+        g.run(to_dev(a))
+    assert e.value.status == 6 and e.value.info == 131
+    g.close()
+
+
+def test_bounded_wait_times_out_cleanly(mtd):
+    # A deadline far shorter than one tile operation: waiting CTAs give up, record
+    # MTD_ERR_TIMEOUT and return; nothing hangs and the next run succeeds.
+    n, tile = 2048, 1024
+    a = gen.spd_input(n, 8)
+    g = mtd.TaskGraph(mtd.KIND_CHOLESKY, n, tile).build_tiled().set_timeout(1e-6).finalize()
+    with pytest.raises(mtd.MtdError) as e:
+        g.run(to_dev(a))
+    assert e.value.status == 4
+    g.set_timeout(10.0)
+    d = to_dev(a)
+    assert g.run(d) == 0
+    assert verify.normwise_residual_chol(a, from_dev(d)) < 1e-14
+    g.close()
+
+
+def test_one_call_drivers(mtd):
+    a = gen.spd_input(700, 12)
+    d = to_dev(a)
+    assert mtd.tiled_cholesky(d, 256) == 0
+    assert rel_diff(np.tril(from_dev(d)), np.tril(oracle_factor(a, 256, "chol"))) <= TOL
+    b = gen.lu_input(700, 12)
+    d = to_dev(b)
+    assert mtd.tiled_lu(d, 256) == 0
+    assert rel_diff(from_dev(d), oracle_factor(b, 256, "lu")) <= TOL
+
+
+def test_trace_and_stats(mtd):
+    a = gen.spd_input(1024, 1)
+    out, info, g = factor(mtd, a, 256, "chol", trace=True)
+    st = g.stats()
+    total_items = sum(g.items(t) for t in range(g.num_tasks))
+    assert st["tasks"] == g.num_tasks and st["items"] == total_items
+    assert 0.0 < st["busy_fraction"] <= 1.0 and st["span_ms"] > 0
+    recs = g.trace()
+    assert len(recs) == total_items
+    assert all(e >= s for s, e, _, _, _ in recs)
+    g.close()
+
+
+def test_device_generators_match_oracle(mtd):
+    import torch
+    n = 512
+    d = torch.empty((n, n), dtype=torch.float64, device="cuda").t()
+    mtd.generate(d, mtd.GEN_UNIFORM_DIAG, seed=21)
+    assert np.array_equal(from_dev(d), gen.lu_input(n, 21))
+    mtd.generate(d, mtd.GEN_SPD, seed=21, alpha=1.0)
+    assert rel_diff(from_dev(d), gen.spd_input(n, 21)) <= 1e-14
+
+
+def test_large_cholesky_against_lapack(mtd):
+    from scipy.linalg import lapack
+    n, tile = 6000, 1024
+    a = gen.spd_input(n, 2)
+    out, info, g = factor(mtd, a, tile, "chol")
+    ref, rinfo = lapack.dpotrf(a, lower=1, clean=1)
+    assert rinfo == 0
+    assert rel_diff(np.tril(out), ref) <= TOL
+    assert verify.probe_residual(a, out, "chol") < 1e-15
+    g.close()
+
+
+def test_large_lu_against_lapack(mtd):
+    n, tile = 6000, 768
+    a = gen.lu_input(n, 2)
+    out, info, g = factor(mtd, a, tile, "lu")
+    ref = tiled.lu_nopiv_lapack(a)
+    assert rel_diff(out, ref) <= TOL
+    assert verify.probe_residual(a, out, "lu") < 1e-15
+    g.close()
