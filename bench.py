@@ -171,6 +171,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer measurement")
     ap.add_argument("--trace", action="store_true", help="record per-item traces (adds busy fraction)")
+    ap.add_argument("--only", choices=["lu", "chol"], default=None,
+                    help="time one factorisation only (profiling runs; the metric needs both)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -218,17 +220,22 @@ def main():
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
 
     def step():
-        work.copy_(src_lu)
         ev[0].record(stream)
-        g_lu.run(work, stream=stream, sync=False)
+        if args.only != "chol":
+            work.copy_(src_lu)
+            ev[0].record(stream)
+            g_lu.run(work, stream=stream, sync=False)
         ev[1].record(stream)
-        work.copy_(src_ch)
         ev[2].record(stream)
-        g_ch.run(work, stream=stream, sync=False)
+        if args.only != "lu":
+            work.copy_(src_ch)
+            ev[2].record(stream)
+            g_ch.run(work, stream=stream, sync=False)
         ev[3].record(stream)
 
     def check_status():
-        for g in (g_lu, g_ch):
+        ran = [g for g, kind in ((g_lu, "lu"), (g_ch, "chol")) if args.only in (None, kind)]
+        for g in ran:
             rc, info = g.status()
             if rc != 0:
                 raise mtd.MtdError(rc, info)
@@ -262,7 +269,7 @@ def main():
         tt = torch.tensor([dev_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         dev_ms = float(tt.item())
-    flops_step = flops_lu(n) + flops_chol(n)
+    flops_step = (flops_lu(n) if args.only != "chol" else 0.0) + (flops_chol(n) if args.only != "lu" else 0.0)
     value = world * flops_step / (dev_ms * 1e-3) / 1e12
 
     # --- end to end through the public API with host buffers ---------------------
@@ -314,8 +321,8 @@ def main():
         "kernel": "mtd::persistent_kernel<2> (scheduler + all FP64 tile operations)",
         "peak_source": "measured: register-only mma.sync.m16n8k8.f64 probe on this GPU",
         "frac_of_datasheet_37": achieved / DATASHEET_FP64_TFLOPS,
-        "lu_tflops": flops_lu(n) / (t_lu / args.steps * 1e-3) / 1e12,
-        "chol_tflops": flops_chol(n) / (t_ch / args.steps * 1e-3) / 1e12,
+        "lu_tflops": flops_lu(n) / (t_lu / args.steps * 1e-3) / 1e12 if args.only != "chol" else None,
+        "chol_tflops": flops_chol(n) / (t_ch / args.steps * 1e-3) / 1e12 if args.only != "lu" else None,
     }
 
     cpu = None
@@ -339,7 +346,7 @@ def main():
                        "l2": "inputs (4.6 GB each) larger than the 126 MB L2"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
             "clocks": clocks.summary(),
-            "gpu_launches": args.steps * 2 * launches_per_run,
+            "gpu_launches": args.steps * (1 if args.only else 2) * launches_per_run,
             "wall_s_timed": wall1 - wall0,
         }
         if args.trace:

@@ -131,6 +131,14 @@ int mtd_graph_set_timeout(mtd_graph *g, double seconds);
  * returns after enqueueing and mtd_graph_status reports the outcome later. */
 int mtd_run(mtd_graph *g, double *dA, int64_t lda, void *stream, int *info_out);
 
+/* The same tasks and tile kernels executed as one host-launched CUDA graph: one kernel
+ * node per task (grid = its work items) whose node dependencies are the task's
+ * predecessors, so the CUDA graph executor resolves the DAG.  Replaces the reference's
+ * --tiled mode (mustard/mustard.h:155-159, :341-383; cholesky_mustard.cu:498-513).  The
+ * CUDA graph is built on the first call for a given (dA, lda) and reused.  Same
+ * status/info conventions as mtd_run. */
+int mtd_run_graph(mtd_graph *g, double *dA, int64_t lda, void *stream, int *info_out);
+
 /* Synchronise with the last run and return its status (and info). */
 int mtd_graph_status(mtd_graph *g, int *info_out);
 

@@ -130,6 +130,18 @@ class TaskGraph:
         _capi.check(rc, info.value)
         return info.value
 
+    def run_graph(self, a, stream=None, sync=True):
+        """Same factorisation through the host-launched CUDA-graph executor (the
+        reference's --tiled mode) instead of the persistent scheduler."""
+        ptr, n, ld = _matrix_ptr(a, self.n)
+        if n != self.n:
+            raise ValueError(f"matrix is {n}x{n}, graph expects {self.n}")
+        info = ctypes.c_int(0)
+        rc = self._lib.mtd_run_graph(self._h, ctypes.c_void_p(ptr), ld, _stream_handle(stream),
+                                     ctypes.byref(info) if sync else None)
+        _capi.check(rc, info.value)
+        return info.value
+
     def status(self):
         info = ctypes.c_int(0)
         rc = self._lib.mtd_graph_status(self._h, ctypes.byref(info))

@@ -42,6 +42,7 @@ SIGNATURES = {
     "mtd_graph_set_trace": (_i, [_vp, _i]),
     "mtd_graph_set_timeout": (_i, [_vp, _d]),
     "mtd_run": (_i, [_vp, _vp, _i64, _vp, ctypes.POINTER(_i)]),
+    "mtd_run_graph": (_i, [_vp, _vp, _i64, _vp, ctypes.POINTER(_i)]),
     "mtd_graph_status": (_i, [_vp, ctypes.POINTER(_i)]),
     "mtd_graph_last_stats": (_i, [_vp, ctypes.POINTER(RunStats)]),
     "mtd_graph_copy_trace": (ctypes.c_longlong, [_vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_longlong]),

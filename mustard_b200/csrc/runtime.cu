@@ -41,7 +41,14 @@ struct mtd_graph {
 
     cudaStream_t last_stream = nullptr;
     bool run_pending = false;
+    bool last_was_graph = false;
     int last_grid = 0;
+
+    // Host-launched CUDA-graph executor (built on first use for a given matrix).
+    cudaGraph_t cgraph = nullptr;
+    cudaGraphExec_t cexec = nullptr;
+    double *cgraph_a = nullptr;
+    int64_t cgraph_lda = 0;
 
     mtd_graph(int kind, int64_t n, int64_t tile) : dag(kind, n, tile) {}
 };
@@ -56,8 +63,91 @@ int smem_setup(int device) {
         if (cudaFuncSetAttribute(persistent_kernel<VEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  kOpSmemBytes()) != cudaSuccess)
             return MTD_ERR_CUDA;
+        if (cudaFuncSetAttribute(task_kernel<VEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, kOpSmemBytes()) !=
+            cudaSuccess)
+            return MTD_ERR_CUDA;
         done[device] = true;
     }
+    return MTD_OK;
+}
+
+bool use_vec2(const mtd_graph *g, const double *dA, int64_t lda) {
+    return (reinterpret_cast<uintptr_t>(dA) % 16 == 0) && (lda % 2 == 0) && (g->dag.tile() % 2 == 0) &&
+           (g->dag.n() % 2 == 0);
+}
+
+RunArgs make_args(const mtd_graph *g, double *dA, int64_t lda) {
+    RunArgs a{};
+    a.a = dA;
+    a.lda = lda;
+    a.n = g->dag.n();
+    a.tile = g->dag.tile();
+    a.tiles = g->dag.tiles();
+    a.n_tasks = g->dag.num_tasks();
+    a.tasks = g->d_tasks;
+    a.succ = g->d_succ;
+    a.deps = g->d_deps;
+    a.items_left = g->d_items_left;
+    for (int q = 0; q < kNumQueues; ++q) {
+        a.queue[q] = g->d_queue[q];
+        a.queue_cap[q] = g->queue_cap[q];
+    }
+    a.qctl = g->d_qctl;
+    a.ctl = g->d_ctl;
+    a.ws_lower = g->d_ws_lower;
+    a.ws_upper = g->d_ws_upper;
+    a.trace = g->d_trace;
+    a.trace_cap = g->trace_cap;
+    a.timeout_ns = static_cast<unsigned long long>(g->timeout_s * 1e9);
+    return a;
+}
+
+void release_cgraph(mtd_graph *g) {
+    if (g->cexec) cudaGraphExecDestroy(g->cexec);
+    if (g->cgraph) cudaGraphDestroy(g->cgraph);
+    g->cexec = nullptr;
+    g->cgraph = nullptr;
+    g->cgraph_a = nullptr;
+}
+
+// One kernel node per task (grid = its work items) with the task's predecessors as
+// node dependencies, after a node that clears the error word.
+int build_cgraph(mtd_graph *g, double *dA, int64_t lda) {
+    release_cgraph(g);
+    const RunArgs a = make_args(g, dA, lda);
+    const bool vec2 = use_vec2(g, dA, lda);
+    if (cudaGraphCreate(&g->cgraph, 0) != cudaSuccess) return MTD_ERR_CUDA;
+    cudaGraphNode_t reset;
+    {
+        cudaKernelNodeParams kp{};
+        void *args[] = {const_cast<RunArgs *>(&a)};
+        kp.func = reinterpret_cast<void *>(reset_ctl_kernel);
+        kp.gridDim = dim3(1);
+        kp.blockDim = dim3(32);
+        kp.kernelParams = args;
+        if (cudaGraphAddKernelNode(&reset, g->cgraph, nullptr, 0, &kp) != cudaSuccess) return MTD_ERR_CUDA;
+    }
+    const int nt = g->dag.num_tasks();
+    std::vector<cudaGraphNode_t> nodes(nt);
+    std::vector<cudaGraphNode_t> deps;
+    for (int t = 0; t < nt; ++t) {
+        deps.clear();
+        for (int d : g->dag.deps(t)) deps.push_back(nodes[d]);
+        if (deps.empty()) deps.push_back(reset);
+        int task = t;
+        void *args[] = {const_cast<RunArgs *>(&a), &task};
+        cudaKernelNodeParams kp{};
+        kp.func = vec2 ? reinterpret_cast<void *>(task_kernel<2>) : reinterpret_cast<void *>(task_kernel<1>);
+        kp.gridDim = dim3(static_cast<unsigned>(g->dag.items_of(t)));
+        kp.blockDim = dim3(kThreads);
+        kp.sharedMemBytes = kOpSmemBytes();
+        kp.kernelParams = args;
+        if (cudaGraphAddKernelNode(&nodes[t], g->cgraph, deps.data(), deps.size(), &kp) != cudaSuccess)
+            return MTD_ERR_CUDA;
+    }
+    if (cudaGraphInstantiate(&g->cexec, g->cgraph, 0) != cudaSuccess) return MTD_ERR_CUDA;
+    g->cgraph_a = dA;
+    g->cgraph_lda = lda;
     return MTD_OK;
 }
 
@@ -254,31 +344,8 @@ int mtd_run(mtd_graph *g, double *dA, int64_t lda, void *stream, int *info_out) 
     if (cudaGetDevice(&dev) != cudaSuccess || dev != g->device) return MTD_ERR_STATE;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
 
-    RunArgs a{};
-    a.a = dA;
-    a.lda = lda;
-    a.n = g->dag.n();
-    a.tile = g->dag.tile();
-    a.tiles = g->dag.tiles();
-    a.n_tasks = g->dag.num_tasks();
-    a.tasks = g->d_tasks;
-    a.succ = g->d_succ;
-    a.deps = g->d_deps;
-    a.items_left = g->d_items_left;
-    for (int q = 0; q < kNumQueues; ++q) {
-        a.queue[q] = g->d_queue[q];
-        a.queue_cap[q] = g->queue_cap[q];
-    }
-    a.qctl = g->d_qctl;
-    a.ctl = g->d_ctl;
-    a.ws_lower = g->d_ws_lower;
-    a.ws_upper = g->d_ws_upper;
-    a.trace = g->d_trace;
-    a.trace_cap = g->trace_cap;
-    a.timeout_ns = static_cast<unsigned long long>(g->timeout_s * 1e9);
-
-    const bool vec2 = (reinterpret_cast<uintptr_t>(dA) % 16 == 0) && (lda % 2 == 0) &&
-                      (g->dag.tile() % 2 == 0) && (g->dag.n() % 2 == 0);
+    const RunArgs a = make_args(g, dA, lda);
+    const bool vec2 = use_vec2(g, dA, lda);
     const int grid = g->num_sms;
     g->last_grid = grid;
     const int reset_blocks = static_cast<int>(std::min<long long>(
@@ -292,6 +359,32 @@ int mtd_run(mtd_graph *g, double *dA, int64_t lda, void *stream, int *info_out) 
         return MTD_ERR_CUDA;
     g->last_stream = s;
     g->run_pending = true;
+    g->last_was_graph = false;
+    if (info_out) return mtd_graph_status(g, info_out);
+    return MTD_OK;
+}
+
+int mtd_run_graph(mtd_graph *g, double *dA, int64_t lda, void *stream, int *info_out) {
+    if (!g || !dA) return MTD_ERR_INVALID_ARG;
+    if (!g->finalized) return MTD_ERR_STATE;
+    if (lda < g->dag.n()) return MTD_ERR_INVALID_ARG;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev != g->device) return MTD_ERR_STATE;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!g->cexec || g->cgraph_a != dA || g->cgraph_lda != lda) {
+        const int rc = build_cgraph(g, dA, lda);
+        if (rc) {
+            release_cgraph(g);
+            return rc;
+        }
+    }
+    if (cudaGraphLaunch(g->cexec, s) != cudaSuccess) return MTD_ERR_CUDA;
+    if (cudaMemcpyAsync(g->h_ctl, g->d_ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return MTD_ERR_CUDA;
+    g->last_stream = s;
+    g->run_pending = true;
+    g->last_was_graph = true;
+    g->last_grid = 0;
     if (info_out) return mtd_graph_status(g, info_out);
     return MTD_OK;
 }
@@ -304,7 +397,7 @@ int mtd_graph_status(mtd_graph *g, int *info_out) {
     const RunCtl &c = *g->h_ctl;
     if (info_out) *info_out = (c.error != 0 && c.info != 0x7fffffff) ? c.info : 0;
     if (c.error) return c.error;
-    if (c.tasks_done != g->dag.num_tasks()) return MTD_ERR_TIMEOUT;
+    if (!g->last_was_graph && c.tasks_done != g->dag.num_tasks()) return MTD_ERR_TIMEOUT;
     return MTD_OK;
 }
 
@@ -356,6 +449,7 @@ int mtd_graph_destroy(mtd_graph *g) {
     if (!g) return MTD_ERR_INVALID_ARG;
     if (g->run_pending && g->last_stream != nullptr) cudaStreamSynchronize(g->last_stream);
     else if (g->run_pending) cudaDeviceSynchronize();
+    release_cgraph(g);
     if (g->finalized) release_device(g);
     delete g;
     return MTD_OK;

@@ -156,6 +156,27 @@ __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const RunArgs p
     }
 }
 
+// One task as an ordinary launch (grid = its work items): the node kernel of the
+// host-launched CUDA-graph executor, the reference's --tiled mode
+// (mustard/mustard.h:155-159, cholesky_mustard.cu:498-513).
+template <int VEC>
+__global__ void __launch_bounds__(kThreads, 1) task_kernel(const RunArgs p, int task) {
+    extern __shared__ __align__(128) double smem[];
+    if (ld_volatile(&p.ctl->abort)) return;
+    const DevTask t = p.tasks[task];
+    dispatch<VEC>(p, t, static_cast<int>(blockIdx.x), smem);
+}
+
+__global__ void reset_ctl_kernel(const RunArgs p) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        p.ctl->tasks_done = 0;
+        p.ctl->error = 0;
+        p.ctl->info = 0x7fffffff;
+        p.ctl->abort = 0;
+        p.ctl->items_done = 0;
+    }
+}
+
 // Per-run reset: counters from their initial values, queues empty.
 __global__ void reset_kernel(const RunArgs p, const int *deps_init) {
     const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;

@@ -1,0 +1,71 @@
+"""Small, self-contained workloads for ncu captures of the persistent kernel.
+
+    python -m mustard_b200.profile_cases gemm  --n 6144 --tile 768
+        one Cholesky update step only: every GEMM_NT(j, i) of step k = 0 for j > i >= 1,
+        all independent, so the capture shows the GEMM work items and the scheduler
+        without the critical path
+    python -m mustard_b200.profile_cases chol --n 6144 --tile 512
+    python -m mustard_b200.profile_cases lu   --n 6144 --tile 512
+        a whole tiled factorisation
+
+Each case runs `--runs` launches (default 2: the first is the one to capture with
+`-c 1`), checks the run status, and prints the device time of the last launch.
+Inputs are the seeded generators of the benchmark (larger than L2 from n = 4096).
+"""
+import argparse
+import json
+
+import torch
+
+import mustard_b200 as mtd
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["gemm", "chol", "lu"])
+    ap.add_argument("--n", type=int, default=6144)
+    ap.add_argument("--tile", type=int, default=768)
+    ap.add_argument("--runs", type=int, default=2)
+    args = ap.parse_args()
+    n, b = args.n, args.tile
+    t = (n + b - 1) // b
+    a = torch.empty((n, n), dtype=torch.float64, device="cuda").t()
+    if args.case == "lu":
+        mtd.generate(a, mtd.GEN_UNIFORM_DIAG, seed=3)
+        g = mtd.TaskGraph(mtd.KIND_LU, n, b).build_tiled()
+        flops = 2.0 * n ** 3 / 3
+    elif args.case == "chol":
+        mtd.generate(a, mtd.GEN_SPD, seed=3)
+        g = mtd.TaskGraph(mtd.KIND_CHOLESKY, n, b).build_tiled()
+        flops = n ** 3 / 3.0
+    else:
+        mtd.generate(a, mtd.GEN_SPD, seed=3)
+        g = mtd.TaskGraph(mtd.KIND_CUSTOM, n, b)
+        flops = 0.0
+        ext = [min(b, n - i * b) for i in range(t)]
+        for i in range(1, t):
+            for j in range(i + 1, t):
+                g.add_task(mtd.OP_GEMM_NT, (j, i), [(j, i), (j, 0), (i, 0)])
+                flops += 2.0 * ext[j] * ext[i] * ext[0]
+    g.finalize()
+    src = a.clone()
+    s = torch.cuda.current_stream()
+    ms = 0.0
+    for _ in range(args.runs):
+        a.copy_(src)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        g.run(a, stream=s, sync=False)
+        e1.record(s)
+        torch.cuda.synchronize()
+        rc, info = g.status()
+        if rc:
+            raise mtd.MtdError(rc, info)
+        ms = e0.elapsed_time(e1)
+    print(json.dumps({"case": args.case, "n": n, "tile": b, "tasks": g.num_tasks, "ms": ms,
+                      "tflops": flops / (ms * 1e-3) / 1e12}))
+    g.close()
+
+
+if __name__ == "__main__":
+    main()
