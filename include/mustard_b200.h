@@ -108,6 +108,10 @@ int mtd_graph_num_tasks(const mtd_graph *g);
  * mustard/mustard.h:137) into out[0..cap); returns the full count or a negative status. */
 int mtd_graph_get_deps(const mtd_graph *g, int task, int *out, int cap);
 
+/* Number of device tasks after mtd_graph_finalize: the host tasks, with every nested
+ * diagonal factorisation counted as its sub-tasks (0 before finalize). */
+int mtd_graph_num_device_tasks(const mtd_graph *g);
+
 /* Number of device work items task `task` is split into (0 before finalize). */
 int mtd_graph_task_items(const mtd_graph *g, int task);
 
@@ -119,6 +123,13 @@ int mtd_graph_finalize(mtd_graph *g);
 
 /* Enable (1) or disable (0) the per-item device trace used for busy-fraction stats. */
 int mtd_graph_set_trace(mtd_graph *g, int enable);
+
+/* Sub-tile edge for nested diagonal factorisations (a multiple of 64; 0 disables).  A
+ * POTRF/GETRF task on a tile larger than this runs as a tiled factorisation of that tile
+ * with sub-tiles of this edge, spread over many SMs -- as the reference nests a tiled
+ * sub-LU when the tile exceeds MAX_TILE (lu_mustard.cu:133-254, :381-388).  Default 128.
+ * Must be called before mtd_graph_finalize. */
+int mtd_graph_set_nest(mtd_graph *g, int nest);
 
 /* Upper bound (seconds) on any single device-side wait; default 10 s. */
 int mtd_graph_set_timeout(mtd_graph *g, double seconds);

@@ -89,6 +89,11 @@ class TaskGraph:
         _capi.check(self._lib.mtd_graph_set_trace(self._h, 1 if enable else 0))
         return self
 
+    def set_nest(self, nest):
+        """Sub-tile edge of nested diagonal factorisations (multiple of 64; 0 = off)."""
+        _capi.check(self._lib.mtd_graph_set_nest(self._h, int(nest)))
+        return self
+
     def set_timeout(self, seconds):
         _capi.check(self._lib.mtd_graph_set_timeout(self._h, float(seconds)))
         return self
@@ -113,6 +118,11 @@ class TaskGraph:
 
     def items(self, task):
         return self._lib.mtd_graph_task_items(self._h, task)
+
+    @property
+    def num_device_tasks(self):
+        """Device tasks after finalize (nested diagonal factorisations expanded)."""
+        return self._lib.mtd_graph_num_device_tasks(self._h)
 
     # -- execution ---------------------------------------------------------
     def run(self, a, stream=None, sync=True, lda=None):

@@ -38,9 +38,11 @@ SIGNATURES = {
     "mtd_graph_num_tasks": (_i, [_vp]),
     "mtd_graph_get_deps": (_i, [_vp, _i, ctypes.POINTER(_i), _i]),
     "mtd_graph_task_items": (_i, [_vp, _i]),
+    "mtd_graph_num_device_tasks": (_i, [_vp]),
     "mtd_graph_finalize": (_i, [_vp]),
     "mtd_graph_set_trace": (_i, [_vp, _i]),
     "mtd_graph_set_timeout": (_i, [_vp, _d]),
+    "mtd_graph_set_nest": (_i, [_vp, _i]),
     "mtd_run": (_i, [_vp, _vp, _i64, _vp, ctypes.POINTER(_i)]),
     "mtd_run_graph": (_i, [_vp, _vp, _i64, _vp, ctypes.POINTER(_i)]),
     "mtd_graph_status": (_i, [_vp, ctypes.POINTER(_i)]),

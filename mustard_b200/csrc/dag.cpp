@@ -137,22 +137,22 @@ int Dag::build_reference_order() {
     return rc ? MTD_ERR_INVALID_ARG : MTD_OK;
 }
 
-int Dag::items_of(int ti) const {
-    const HostTask &t = tasks_[ti];
-    const int64_t m = extent(t.write.first), n = extent(t.write.second);
+int items_of(const DevTask &t) {
     switch (t.op) {
     case MTD_OP_GEMM_NT:
     case MTD_OP_GEMM_NN:
-        return static_cast<int>(ceil_div(m, kGemmTile) * ceil_div(n, kGemmTile));
+        return static_cast<int>(ceil_div(t.m, kGemmTile) * ceil_div(t.n, kGemmTile));
     case MTD_OP_SYRK_LN: {
-        int64_t b = ceil_div(m, kGemmTile);
+        const int64_t b = ceil_div(t.m, kGemmTile);
         return static_cast<int>(b * (b + 1) / 2);
     }
     case MTD_OP_TRSM_RLT:
     case MTD_OP_TRSM_RUN:
-        return static_cast<int>(ceil_div(m, kPanelRows));
+        return static_cast<int>(ceil_div(t.m, kPanelRows));
     case MTD_OP_TRSM_LLNU:
-        return static_cast<int>(ceil_div(n, kPanelRows));
+        return static_cast<int>(ceil_div(t.n, kPanelRows));
+    case kOpJoin:
+        return 0;
     default:
         return 1;
     }
@@ -176,12 +176,81 @@ int Dag::queue_of(int ti) const {
     }
 }
 
-int Dag::lower(std::vector<DevTask> &out, std::vector<int> &succ, std::vector<int> &pred_count,
-               int64_t queue_cap[kNumQueues]) const {
+namespace {
+
+DevTask make_task(int op, int queue, int64_t cr, int64_t cc, int64_t ar, int64_t ac, int64_t br, int64_t bc,
+                  int64_t m, int64_t n, int64_t k) {
+    DevTask d{};
+    d.op = op;
+    d.queue = queue;
+    d.cr = static_cast<int32_t>(cr);
+    d.cc = static_cast<int32_t>(cc);
+    d.ar = static_cast<int32_t>(ar);
+    d.ac = static_cast<int32_t>(ac);
+    d.br = static_cast<int32_t>(br);
+    d.bc = static_cast<int32_t>(bc);
+    d.m = static_cast<int32_t>(m);
+    d.n = static_cast<int32_t>(n);
+    d.k = static_cast<int32_t>(k);
+    d.n_items = items_of(d);
+    return d;
+}
+
+// The reference's tiled task list (cholesky_mustard.cu:224-395 / lu_mustard.cu:345-533)
+// over an s x s grid of sub-tiles of edge `b` starting at element (o, o) of an e x e
+// diagonal block; appends device tasks and their in-nest predecessor lists.
+void nested_factorisation(bool chol, int64_t o, int64_t e, int64_t b, std::vector<DevTask> &tasks,
+                          std::vector<std::vector<int>> &preds) {
+    const int s = static_cast<int>(ceil_div(e, b));
+    auto ext = [&](int p) { return std::min<int64_t>(b, e - int64_t(p) * b); };
+    auto org = [&](int p) { return o + int64_t(p) * b; };
+    std::map<TileId, int> last;
+    auto add = [&](const DevTask &d, TileId w, std::initializer_list<TileId> reads) {
+        std::vector<int> dep;
+        std::vector<TileId> tl(reads);
+        tl.push_back(w);
+        for (const auto &id : tl) {
+            auto it = last.find(id);
+            if (it != last.end()) dep.push_back(it->second);
+        }
+        std::sort(dep.begin(), dep.end());
+        dep.erase(std::unique(dep.begin(), dep.end()), dep.end());
+        last[w] = static_cast<int>(tasks.size());
+        tasks.push_back(d);
+        preds.push_back(dep);
+    };
+    for (int p = 0; p < s; ++p) {
+        const int64_t P = org(p), ep = ext(p);
+        if (chol) {
+            add(make_task(MTD_OP_POTRF, 0, P, P, P, P, 0, 0, ep, ep, ep), {p, p}, {{p, p}});
+            for (int q = p + 1; q < s; ++q)
+                add(make_task(MTD_OP_TRSM_RLT, 0, org(q), P, P, P, 0, 0, ext(q), ep, 0), {q, p}, {{p, p}, {q, p}});
+            for (int q = p + 1; q < s; ++q) {
+                add(make_task(MTD_OP_SYRK_LN, 0, org(q), org(q), org(q), P, 0, 0, ext(q), ext(q), ep), {q, q},
+                    {{q, q}, {q, p}});
+                for (int r = q + 1; r < s; ++r)
+                    add(make_task(MTD_OP_GEMM_NT, 0, org(r), org(q), org(r), P, org(q), P, ext(r), ext(q), ep),
+                        {r, q}, {{r, q}, {r, p}, {q, p}});
+            }
+        } else {
+            add(make_task(MTD_OP_GETRF, 0, P, P, P, P, 0, 0, ep, ep, ep), {p, p}, {{p, p}});
+            for (int q = p + 1; q < s; ++q)
+                add(make_task(MTD_OP_TRSM_LLNU, 0, P, org(q), P, P, 0, 0, ep, ext(q), 0), {p, q}, {{p, p}, {p, q}});
+            for (int q = p + 1; q < s; ++q) {
+                add(make_task(MTD_OP_TRSM_RUN, 0, org(q), P, P, P, 0, 0, ext(q), ep, 0), {q, p}, {{p, p}, {q, p}});
+                for (int r = p + 1; r < s; ++r)
+                    add(make_task(MTD_OP_GEMM_NN, 0, org(q), org(r), org(q), P, P, org(r), ext(q), ext(r), ep),
+                        {q, r}, {{q, p}, {p, r}, {q, r}});
+            }
+        }
+    }
+}
+
+}  // namespace
+
+int Dag::lower(int nest, Lowered &out) const {
     const int nt = num_tasks();
-    out.assign(nt, DevTask{});
-    pred_count.assign(nt, 0);
-    for (int q = 0; q < kNumQueues; ++q) queue_cap[q] = 0;
+    out = Lowered{};
 
     // A triangular solve reads the inverses of the diagonal blocks that the diagonal
     // factorisation of its triangular tile leaves in the workspace, so the last writer
@@ -197,28 +266,81 @@ int Dag::lower(std::vector<DevTask> &out, std::vector<int> &succ, std::vector<in
         writer[h.write] = t;
     }
 
-    std::vector<std::vector<int>> succs(nt);
-    for (int t = 0; t < nt; ++t) {
-        pred_count[t] = static_cast<int>(deps_[t].size());
-        for (int d : deps_[t]) succs[d].push_back(t);
-    }
-    succ.clear();
+    std::vector<DevTask> &dev = out.tasks;
+    std::vector<std::vector<int>> &preds = out.preds;
+    std::vector<std::vector<int>> entry(nt);
+    std::vector<int> exit_of(nt, -1);
+    out.host_items.assign(nt, 0);
+    const int64_t B = tile_;
     for (int t = 0; t < nt; ++t) {
         const HostTask &h = tasks_[t];
-        DevTask &d = out[t];
-        d.op = h.op;
-        d.queue = queue_of(t);
-        d.n_items = items_of(t);
-        d.wi = h.write.first;
-        d.wj = h.write.second;
-        d.ai = h.a.first;
-        d.aj = h.a.second;
-        d.bi = h.b.first;
-        d.bj = h.b.second;
-        d.succ_begin = static_cast<int32_t>(succ.size());
-        d.succ_count = static_cast<int32_t>(succs[t].size());
-        for (int s : succs[t]) succ.push_back(s);
-        queue_cap[d.queue] += d.n_items;
+        const int q = queue_of(t);
+        const int64_t wr = h.write.first * B, wc = h.write.second * B;
+        const int64_t em = extent(h.write.first), en = extent(h.write.second);
+        const int64_t ar = h.a.first * B, ac = h.a.second * B, br = h.b.first * B, bc = h.b.second * B;
+        const int first = static_cast<int>(dev.size());
+        const bool diag = h.op == MTD_OP_POTRF || h.op == MTD_OP_GETRF;
+        if (diag && nest > 0 && em > nest) {
+            nested_factorisation(h.op == MTD_OP_POTRF, wr, em, nest, dev, preds);
+            const int last = static_cast<int>(dev.size());
+            std::vector<char> has_succ(last - first, 0);
+            for (int d = first; d < last; ++d) {
+                for (int p : preds[d]) has_succ[p - first] = 1;  // in-nest edges only so far
+                if (preds[d].empty()) entry[t].push_back(d);
+            }
+            std::vector<int> sinks;
+            for (int d = first; d < last; ++d)
+                if (!has_succ[d - first]) sinks.push_back(d);
+            if (sinks.size() == 1) {
+                exit_of[t] = sinks[0];
+            } else {
+                exit_of[t] = static_cast<int>(dev.size());
+                dev.push_back(make_task(kOpJoin, 0, wr, wc, 0, 0, 0, 0, em, en, 0));
+                preds.push_back(sinks);
+            }
+        } else {
+            DevTask d{};
+            switch (h.op) {
+            case MTD_OP_POTRF:
+            case MTD_OP_GETRF:
+                d = make_task(h.op, q, wr, wc, wr, wc, 0, 0, em, em, em);
+                break;
+            case MTD_OP_TRSM_RLT:
+            case MTD_OP_TRSM_RUN:  // X = write tile (m x n), triangle = n x n at a
+            case MTD_OP_TRSM_LLNU: // X = write tile (m x n), triangle = m x m at a
+                d = make_task(h.op, q, wr, wc, ar, ac, 0, 0, em, en, 0);
+                break;
+            case MTD_OP_SYRK_LN:
+                d = make_task(h.op, q, wr, wc, ar, ac, 0, 0, em, em, extent(h.a.second));
+                break;
+            default:  // GEMM_NT / GEMM_NN
+                d = make_task(h.op, q, wr, wc, ar, ac, br, bc, em, en, extent(h.a.second));
+                break;
+            }
+            dev.push_back(d);
+            preds.emplace_back();
+            entry[t].push_back(first);
+            exit_of[t] = first;
+        }
+        for (int d = first; d < static_cast<int>(dev.size()); ++d) out.host_items[t] += dev[d].n_items;
+    }
+    // Host edges d -> t become exit(d) -> every entry of t.
+    for (int t = 0; t < nt; ++t)
+        for (int e : entry[t])
+            for (int d : deps_[t]) preds[e].push_back(exit_of[d]);
+
+    const int nd = static_cast<int>(dev.size());
+    std::vector<std::vector<int>> succs(nd);
+    for (int d = 0; d < nd; ++d) {
+        std::sort(preds[d].begin(), preds[d].end());
+        preds[d].erase(std::unique(preds[d].begin(), preds[d].end()), preds[d].end());
+        for (int p : preds[d]) succs[p].push_back(d);
+    }
+    for (int d = 0; d < nd; ++d) {
+        dev[d].succ_begin = static_cast<int32_t>(out.succ.size());
+        dev[d].succ_count = static_cast<int32_t>(succs[d].size());
+        for (int s : succs[d]) out.succ.push_back(s);
+        out.queue_cap[dev[d].queue] += dev[d].n_items;
     }
     return MTD_OK;
 }

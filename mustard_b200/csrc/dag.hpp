@@ -1,6 +1,7 @@
 // Host-side task DAG: the data the reference keeps in TiledGraphCreator
-// (mustard/mustard.h:132-384) -- task list, last-writer map, predecessor lists -- plus what
-// the device runtime needs (successor CSR, work-item counts, priorities).
+// (mustard/mustard.h:132-384) -- task list, last-writer map, predecessor lists -- and its
+// lowering to the device task table (element geometry, work items, priorities,
+// successor lists).
 #pragma once
 
 #include <cstdint>
@@ -22,6 +23,15 @@ struct HostTask {
     TileId b{0, 0};             // second operand (GEMM only)
 };
 
+// The device form of a graph.
+struct Lowered {
+    std::vector<DevTask> tasks;
+    std::vector<int> succ;                 // CSR payload, indexed by DevTask::succ_begin
+    std::vector<std::vector<int>> preds;   // per device task
+    std::vector<int> host_items;           // work items of each host task (all its device tasks)
+    int64_t queue_cap[kNumQueues] = {0, 0};
+};
+
 class Dag {
 public:
     Dag(int kind, int64_t n, int64_t tile);
@@ -40,12 +50,12 @@ public:
     const std::vector<int> &deps(int t) const { return deps_[t]; }
     const HostTask &task(int t) const { return tasks_[t]; }
 
-    // Fills the device task table, successor CSR and predecessor counts.
-    // Returns MTD_OK or MTD_ERR_BAD_DAG.
-    int lower(std::vector<DevTask> &tasks, std::vector<int> &succ, std::vector<int> &pred_count,
-              int64_t queue_cap[kNumQueues]) const;
-
-    int items_of(int t) const;
+    // Device lowering.  A diagonal factorisation of a tile larger than `nest` elements
+    // (nest > 0, a multiple of kNB) becomes a nested tiled factorisation with nest-sized
+    // sub-tiles -- the reference's own remedy for big diagonal tiles
+    // (recordSubgraph, mustard/lu_mustard.cu:133-254, used when B > MAX_TILE) -- so the
+    // critical path runs on many SMs.  Returns MTD_OK or MTD_ERR_BAD_DAG.
+    int lower(int nest, Lowered &out) const;
 
 private:
     int kind_;
@@ -59,5 +69,7 @@ private:
     bool valid_tile(const TileId &t) const;
     int queue_of(int t) const;
 };
+
+int items_of(const DevTask &t);
 
 }  // namespace mtd

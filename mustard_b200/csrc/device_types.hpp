@@ -6,22 +6,43 @@
 namespace mtd {
 
 constexpr int kNumQueues = 2;   // 0: critical path (diagonal, panel, next-panel updates); 1: rest
-constexpr int kThreads = 256;   // threads per persistent CTA
+#ifndef MTD_THREADS
+#define MTD_THREADS 512
+#endif
+constexpr int kThreads = MTD_THREADS;  // threads per persistent CTA
 constexpr int kGemmTile = 128;  // output sub-tile edge of one GEMM / SYRK work item
 constexpr int kPanelRows = 64;  // rows (or columns) of one TRSM work item
 constexpr int kNB = 64;         // diagonal block edge inside POTRF / GETRF (and inverse blocks)
+constexpr int kNestTile = 128;  // default sub-tile edge of a nested diagonal factorisation
 
-// One task of the DAG as the device sees it.
-struct DevTask {
+// Device-side operation codes: the public mtd_op values plus a zero-work join.
+constexpr int kOpJoin = 100;
+
+// One device task.  Geometry is in matrix elements (row, column origins of each block
+// inside the column-major matrix), so a task can cover a whole tile or a sub-tile of a
+// nested diagonal factorisation.
+//   GEMM_NT  C(m x n) -= A(m x k) * B(n x k)^T
+//   GEMM_NN  C(m x n) -= A(m x k) * B(k x n)
+//   SYRK_LN  C(m x m) -= A(m x k) * A^T (lower)
+//   TRSM_RLT X(m x n) = X * L^-T,  L = n x n at A's origin
+//   TRSM_RUN X(m x n) = X * U^-1,  U = n x n at A's origin
+//   TRSM_LLNU X(m x n) = L^-1 * X, L = m x m (unit) at A's origin
+//   POTRF / GETRF: the m x m block at C's origin
+// The inverse workspaces are indexed by absolute matrix row: the inverse of the kNB x kNB
+// diagonal block whose first row is r sits at ws[r + c * ws_ld], c < kNB.
+struct alignas(16) DevTask {
     int32_t op;
     int32_t queue;       // 0 or 1
-    int32_t n_items;
-    int32_t wi, wj;      // tile written
-    int32_t ai, aj;      // first operand tile (triangular tile for TRSM)
-    int32_t bi, bj;      // second operand tile (GEMM)
+    int32_t n_items;     // 0 for a join
+    int32_t cr, cc;      // output block origin
+    int32_t ar, ac;      // first operand (triangular block for TRSM)
+    int32_t br, bc;      // second operand (GEMM)
+    int32_t m, n, k;     // extents
     int32_t succ_begin;  // successors are succ[succ_begin, succ_begin + succ_count)
     int32_t succ_count;
+    int32_t pad[2];
 };
+static_assert(sizeof(DevTask) == 64, "DevTask is read as four 16-byte words");
 
 // Device-resident control block of one graph (one cache line per hot counter).
 struct alignas(128) QueueCtl {
@@ -44,10 +65,7 @@ struct alignas(128) RunCtl {
 struct RunArgs {
     double *a;             // matrix, column-major
     int64_t lda;
-    int64_t n;
-    int64_t tile;
-    int tiles;
-    int n_tasks;
+    int n_tasks;           // device tasks (including joins)
     const DevTask *tasks;
     const int *succ;
     int *deps;             // remaining predecessor counts (reset each run)
@@ -56,8 +74,9 @@ struct RunArgs {
     long long queue_cap[kNumQueues];
     QueueCtl *qctl;        // kNumQueues entries
     RunCtl *ctl;
-    double *ws_lower;      // per-step inverses of the diagonal blocks of L (tiles*tile*kNB)
-    double *ws_upper;      // per-step inverses of the diagonal blocks of U (LU only)
+    double *ws_lower;      // inverses of the diagonal blocks of L (ws_ld x kNB)
+    double *ws_upper;      // inverses of the diagonal blocks of U (LU only)
+    int64_t ws_ld;
     unsigned long long *trace;  // optional: 4 words per item (start, end, sm, task<<32|item)
     long long trace_cap;
     unsigned long long timeout_ns;

@@ -5,7 +5,7 @@
 #include <cstdlib>
 
 #include "../../include/mustard_b200.h"
-#include "mma.cuh"
+#include "tile_ops.cuh"
 
 using namespace mtd;
 
@@ -38,7 +38,7 @@ __global__ void uniform_kernel(double *a, int64_t n, int64_t lda, uint64_t seed,
 __global__ void __launch_bounds__(kThreads, 1) spd_kernel(double *c, int64_t ldc, const double *b, int64_t n,
                                                           double alpha) {
     extern __shared__ __align__(128) double smem[];
-    using M = BlockMma<kGemmTile, kGemmTile, 2, 4, kBNContig, 2>;
+    using M = GemmMma<kBNContig, 2>;
     const int r0 = blockIdx.x * kGemmTile, c0 = blockIdx.y * kGemmTile;
     const int mm = static_cast<int>(n - r0 < kGemmTile ? n - r0 : kGemmTile);
     const int nn = static_cast<int>(n - c0 < kGemmTile ? n - c0 : kGemmTile);
@@ -89,7 +89,7 @@ int mtd_generate(double *dA, int64_t n, int64_t lda, int which, uint64_t seed, d
         return MTD_ERR_OUT_OF_MEMORY;
     }
     uniform_kernel<<<4096, 256, 0, s>>>(b, n, n, seed, 0.0);
-    constexpr int smem = BlockMma<kGemmTile, kGemmTile, 2, 4, kBNContig, 2>::SMEM_DOUBLES * 8;
+    constexpr int smem = GemmMma<kBNContig, 2>::SMEM_DOUBLES * 8;
     cudaFuncSetAttribute(spd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     const dim3 grid(static_cast<unsigned>((n + kGemmTile - 1) / kGemmTile),
                     static_cast<unsigned>((n + kGemmTile - 1) / kGemmTile));

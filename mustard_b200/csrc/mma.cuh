@@ -52,9 +52,9 @@ __device__ __forceinline__ void dmma_16x8x8(double (&d)[4], const double (&a)[4]
         : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-template <int BM, int BN, int WARPS_M, int WARPS_N, int BL, int VEC, int STAGES = 3>
+template <int BM, int BN, int WARPS_M, int WARPS_N, int BL, int VEC, int STAGES = 3, int BK_ = 16>
 struct BlockMma {
-    static constexpr int BK = 16;
+    static constexpr int BK = BK_;
     static constexpr int WM = BM / WARPS_M;
     static constexpr int WN = BN / WARPS_N;
     static constexpr int FM = WM / 16;
@@ -64,7 +64,7 @@ struct BlockMma {
     static constexpr int A_STAGE = BK * LDA;
     static constexpr int B_STAGE = (BL == kBNContig) ? BK * LDB : BN * LDB;
     static constexpr int SMEM_DOUBLES = STAGES * (A_STAGE + B_STAGE);
-    static_assert(WARPS_M * WARPS_N * 32 == kThreads, "256 threads");
+    static_assert(WARPS_M * WARPS_N * 32 == kThreads, "one warp tile per warp of the CTA");
     static_assert(FM >= 1 && FN >= 1 && WM % 16 == 0 && WN % 8 == 0, "warp tile");
     static_assert(LDA % 16 == 4 && LDB % 16 == 4, "bank-conflict-free padding");
 

@@ -20,6 +20,9 @@ struct mtd_graph {
     int num_sms = 0;
     bool trace = false;
     double timeout_s = 10.0;
+    int nest = kNestTile;
+    Lowered low;   // device form, kept for the CUDA-graph executor and item queries
+    int n_dev = 0;
 
     DevTask *d_tasks = nullptr;
     int *d_succ = nullptr;
@@ -71,6 +74,8 @@ int smem_setup(int device) {
     return MTD_OK;
 }
 
+int64_t ws_ld(const mtd_graph *g) { return g->dag.n() + (g->dag.n() & 1); }
+
 bool use_vec2(const mtd_graph *g, const double *dA, int64_t lda) {
     return (reinterpret_cast<uintptr_t>(dA) % 16 == 0) && (lda % 2 == 0) && (g->dag.tile() % 2 == 0) &&
            (g->dag.n() % 2 == 0);
@@ -80,10 +85,7 @@ RunArgs make_args(const mtd_graph *g, double *dA, int64_t lda) {
     RunArgs a{};
     a.a = dA;
     a.lda = lda;
-    a.n = g->dag.n();
-    a.tile = g->dag.tile();
-    a.tiles = g->dag.tiles();
-    a.n_tasks = g->dag.num_tasks();
+    a.n_tasks = g->n_dev;
     a.tasks = g->d_tasks;
     a.succ = g->d_succ;
     a.deps = g->d_deps;
@@ -96,6 +98,7 @@ RunArgs make_args(const mtd_graph *g, double *dA, int64_t lda) {
     a.ctl = g->d_ctl;
     a.ws_lower = g->d_ws_lower;
     a.ws_upper = g->d_ws_upper;
+    a.ws_ld = ws_ld(g);
     a.trace = g->d_trace;
     a.trace_cap = g->trace_cap;
     a.timeout_ns = static_cast<unsigned long long>(g->timeout_s * 1e9);
@@ -127,18 +130,24 @@ int build_cgraph(mtd_graph *g, double *dA, int64_t lda) {
         kp.kernelParams = args;
         if (cudaGraphAddKernelNode(&reset, g->cgraph, nullptr, 0, &kp) != cudaSuccess) return MTD_ERR_CUDA;
     }
-    const int nt = g->dag.num_tasks();
+    const int nt = g->n_dev;
     std::vector<cudaGraphNode_t> nodes(nt);
     std::vector<cudaGraphNode_t> deps;
     for (int t = 0; t < nt; ++t) {
         deps.clear();
-        for (int d : g->dag.deps(t)) deps.push_back(nodes[d]);
+        for (int d : g->low.preds[t]) deps.push_back(nodes[d]);
         if (deps.empty()) deps.push_back(reset);
+        const int items = g->low.tasks[t].n_items;
+        if (items == 0) {
+            if (cudaGraphAddEmptyNode(&nodes[t], g->cgraph, deps.data(), deps.size()) != cudaSuccess)
+                return MTD_ERR_CUDA;
+            continue;
+        }
         int task = t;
         void *args[] = {const_cast<RunArgs *>(&a), &task};
         cudaKernelNodeParams kp{};
         kp.func = vec2 ? reinterpret_cast<void *>(task_kernel<2>) : reinterpret_cast<void *>(task_kernel<1>);
-        kp.gridDim = dim3(static_cast<unsigned>(g->dag.items_of(t)));
+        kp.gridDim = dim3(static_cast<unsigned>(items));
         kp.blockDim = dim3(kThreads);
         kp.sharedMemBytes = kOpSmemBytes();
         kp.kernelParams = args;
@@ -248,15 +257,24 @@ int mtd_graph_get_deps(const mtd_graph *g, int task, int *out, int cap) {
     return static_cast<int>(d.size());
 }
 
+int mtd_graph_num_device_tasks(const mtd_graph *g) { return g ? (g->finalized ? g->n_dev : 0) : -MTD_ERR_INVALID_ARG; }
+
 int mtd_graph_task_items(const mtd_graph *g, int task) {
     if (!g || task < 0 || task >= g->dag.num_tasks()) return -MTD_ERR_INVALID_ARG;
-    return g->finalized ? g->dag.items_of(task) : 0;
+    return g->finalized ? g->low.host_items[task] : 0;
 }
 
 int mtd_graph_set_trace(mtd_graph *g, int enable) {
     if (!g) return MTD_ERR_INVALID_ARG;
     if (g->finalized) return MTD_ERR_STATE;
     g->trace = enable != 0;
+    return MTD_OK;
+}
+
+int mtd_graph_set_nest(mtd_graph *g, int nest) {
+    if (!g || nest < 0 || nest % kNB != 0) return MTD_ERR_INVALID_ARG;
+    if (g->finalized) return MTD_ERR_STATE;
+    g->nest = nest;
     return MTD_OK;
 }
 
@@ -273,18 +291,20 @@ int mtd_graph_finalize(mtd_graph *g) {
     int rc = check_device(&g->device, &g->num_sms);
     if (rc) return rc;
 
-    std::vector<DevTask> tasks;
-    std::vector<int> succ, preds;
-    int64_t cap[kNumQueues];
-    rc = g->dag.lower(tasks, succ, preds, cap);
+    rc = g->dag.lower(g->nest, g->low);
     if (rc) return rc;
-    std::vector<int> roots;
-    for (int t = 0; t < static_cast<int>(preds.size()); ++t)
+    const std::vector<DevTask> &tasks = g->low.tasks;
+    const std::vector<int> &succ = g->low.succ;
+    const int64_t *cap = g->low.queue_cap;
+    const int nt = static_cast<int>(tasks.size());
+    std::vector<int> preds(nt), roots;
+    for (int t = 0; t < nt; ++t) {
+        preds[t] = static_cast<int>(g->low.preds[t].size());
         if (preds[t] == 0) roots.push_back(t);
+    }
     if (roots.empty()) return MTD_ERR_BAD_DAG;
-
-    const int nt = g->dag.num_tasks();
-    const size_t ws = size_t(g->dag.tiles()) * size_t(g->dag.tile()) * kNB;
+    g->n_dev = nt;
+    const size_t ws = size_t(ws_ld(g)) * kNB;
     g->total_items = 0;
     for (int q = 0; q < kNumQueues; ++q) {
         g->queue_cap[q] = cap[q];
@@ -397,7 +417,7 @@ int mtd_graph_status(mtd_graph *g, int *info_out) {
     const RunCtl &c = *g->h_ctl;
     if (info_out) *info_out = (c.error != 0 && c.info != 0x7fffffff) ? c.info : 0;
     if (c.error) return c.error;
-    if (!g->last_was_graph && c.tasks_done != g->dag.num_tasks()) return MTD_ERR_TIMEOUT;
+    if (!g->last_was_graph && c.tasks_done != g->n_dev) return MTD_ERR_TIMEOUT;
     return MTD_OK;
 }
 

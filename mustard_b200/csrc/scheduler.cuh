@@ -36,19 +36,42 @@ __device__ __forceinline__ unsigned long long ld_volatile(const unsigned long lo
 }
 __device__ __forceinline__ int ld_volatile(const int *p) { return *reinterpret_cast<const volatile int *>(p); }
 
-// Thread 0 of a CTA: push every work item of `task`.
-__device__ __forceinline__ void enqueue_task(const RunArgs &p, int task) {
-    const DevTask &t = p.tasks[task];
-    const int q = t.queue;
-    const unsigned long long n = static_cast<unsigned long long>(t.n_items);
-    const unsigned long long base = atomicAdd(&p.qctl[q].tail, n);
-    if (base + n > static_cast<unsigned long long>(p.queue_cap[q])) {
-        report_error(p.ctl, MTD_ERR_QUEUE, 0);
-        return;
+// Thread 0 of a CTA: `task` has no predecessors left.  Push every work item of it; a
+// join (no work items) completes on the spot, releasing its own successors.
+__device__ __forceinline__ void release_task(const RunArgs &p, int task) {
+    int stack[8];
+    int top = 0;
+    stack[top++] = task;
+    while (top > 0) {
+        const int tk = stack[--top];
+        const int q = __ldg(&p.tasks[tk].queue);
+        const int n_items = __ldg(&p.tasks[tk].n_items);
+        if (n_items > 0) {
+            const unsigned long long n = static_cast<unsigned long long>(n_items);
+            const unsigned long long base = atomicAdd(&p.qctl[q].tail, n);
+            if (base + n > static_cast<unsigned long long>(p.queue_cap[q])) {
+                report_error(p.ctl, MTD_ERR_QUEUE, 0);
+                return;
+            }
+            volatile unsigned long long *slots = p.queue[q];
+            for (unsigned long long i = 0; i < n; ++i)
+                slots[base + i] = (static_cast<unsigned long long>(tk) << 32) | i;
+            continue;
+        }
+        const int sb = __ldg(&p.tasks[tk].succ_begin), sc = __ldg(&p.tasks[tk].succ_count);
+        for (int s = 0; s < sc; ++s) {
+            const int succ = __ldg(&p.succ[sb + s]);
+            if (atomicSub(&p.deps[succ], 1) == 1) {
+                if (top == 8) {
+                    report_error(p.ctl, MTD_ERR_QUEUE, 0);
+                    return;
+                }
+                stack[top++] = succ;
+            }
+        }
+        __threadfence();
+        atomicAdd(&p.ctl->tasks_done, 1);
     }
-    volatile unsigned long long *slots = p.queue[q];
-    for (unsigned long long i = 0; i < n; ++i)
-        slots[base + i] = (static_cast<unsigned long long>(task) << 32) | i;
 }
 
 // Thread 0 of a CTA: claim one work item, waiting (bounded) while none is ready.
@@ -96,10 +119,10 @@ __device__ __forceinline__ void complete_item(const RunArgs &p, int task) {
     __threadfence();
     if (atomicSub(&p.items_left[task], 1) != 1) return;
     __threadfence();
-    const DevTask &t = p.tasks[task];
-    for (int s = 0; s < t.succ_count; ++s) {
-        const int succ = p.succ[t.succ_begin + s];
-        if (atomicSub(&p.deps[succ], 1) == 1) enqueue_task(p, succ);
+    const int sb = __ldg(&p.tasks[task].succ_begin), sc = __ldg(&p.tasks[task].succ_count);
+    for (int s = 0; s < sc; ++s) {
+        const int succ = __ldg(&p.succ[sb + s]);
+        if (atomicSub(&p.deps[succ], 1) == 1) release_task(p, succ);
     }
     __threadfence();
     atomicAdd(&p.ctl->tasks_done, 1);
@@ -137,7 +160,13 @@ __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const RunArgs p
         const int cmd = s_cmd, task = s_task, item = s_item;
         if (cmd != kCmdWork) break;
         const unsigned long long t_start = p.trace ? global_ns() : 0ull;
-        const DevTask t = p.tasks[task];
+        DevTask t;
+        {
+            const int4 *src = reinterpret_cast<const int4 *>(p.tasks + task);
+            int4 *dst = reinterpret_cast<int4 *>(&t);
+#pragma unroll
+            for (int w = 0; w < int(sizeof(DevTask) / sizeof(int4)); ++w) dst[w] = __ldg(src + w);
+        }
         const int st = dispatch<VEC>(p, t, item, smem);
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -164,7 +193,7 @@ __global__ void __launch_bounds__(kThreads, 1) task_kernel(const RunArgs p, int 
     extern __shared__ __align__(128) double smem[];
     if (ld_volatile(&p.ctl->abort)) return;
     const DevTask t = p.tasks[task];
-    dispatch<VEC>(p, t, static_cast<int>(blockIdx.x), smem);
+    if (t.n_items > 0) dispatch<VEC>(p, t, static_cast<int>(blockIdx.x), smem);
 }
 
 __global__ void reset_ctl_kernel(const RunArgs p) {
@@ -204,7 +233,7 @@ __global__ void reset_kernel(const RunArgs p, const int *deps_init) {
 // mustard/mustard.h:87-95).
 __global__ void seed_kernel(const RunArgs p, const int *roots, int n_roots) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
-        for (int r = 0; r < n_roots; ++r) enqueue_task(p, roots[r]);
+        for (int r = 0; r < n_roots; ++r) release_task(p, roots[r]);
         __threadfence();
     }
 }

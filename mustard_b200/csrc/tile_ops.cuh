@@ -5,8 +5,9 @@
 // updates are tensor-core DMMA block products (mma.cuh).  The diagonal factorisations
 // are left-looking blocked algorithms with kNB-wide diagonal blocks factored in shared
 // memory; while a block is in shared memory its triangular inverse is formed and left in
-// a per-step workspace, so every triangular solve of the step -- inside the diagonal
-// task and in the TRSM tasks that follow it -- becomes a block product as well.
+// the inverse workspace (indexed by the block's first matrix row), so every triangular
+// solve -- inside the diagonal task and in the TRSM tasks that follow it -- becomes a
+// block product as well.  Block geometry comes from the task (DevTask), in elements.
 #pragma once
 
 #include "device_types.hpp"
@@ -17,20 +18,38 @@ namespace mtd {
 
 constexpr int kDiagLd = kNB + 1;  // shared-memory leading dimension of a diagonal block
 
+// Engine shapes.  GEMM / SYRK items: kGemmTile x kGemmTile output per CTA; panel work
+// (TRSM strips, diagonal factorisations): 64 x 64 blocks.  Defaults measured best on B200
+// at N = 24000 (512-thread CTAs, 4 x 4 warps of 32 x 32, 32-deep k-slices, 3 stages: 25.4 /
+// 26.5 TFLOP/s Cholesky / LU at tile 768, against 22.2 / 23.8 for 256 threads and 16-deep
+// slices, where only two warps per SM sub-partition could not hide the DMMA latencies).
+#ifndef MTD_GEMM_WARPS_M
+#define MTD_GEMM_WARPS_M 4
+#endif
+#ifndef MTD_GEMM_STAGES
+#define MTD_GEMM_STAGES 3
+#endif
+#ifndef MTD_GEMM_BK
+#define MTD_GEMM_BK 32
+#endif
+#ifndef MTD_PANEL_WARPS_M
+#define MTD_PANEL_WARPS_M 4
+#endif
+constexpr int kGemmWarpsM = MTD_GEMM_WARPS_M;
+constexpr int kGemmWarpsN = kThreads / 32 / kGemmWarpsM;
+constexpr int kPanelWarpsM = MTD_PANEL_WARPS_M;
+constexpr int kPanelWarpsN = kThreads / 32 / kPanelWarpsM;
+template <int BL, int VEC>
+using GemmMma = BlockMma<kGemmTile, kGemmTile, kGemmWarpsM, kGemmWarpsN, BL, VEC, MTD_GEMM_STAGES, MTD_GEMM_BK>;
+template <int BL, int VEC>
+using PanelMma = BlockMma<64, 64, kPanelWarpsM, kPanelWarpsN, BL, VEC>;
+
 __device__ __forceinline__ void block_fence_sync() {
     __threadfence_block();
     __syncthreads();
 }
 
-struct TileView {
-    double *a;
-    int64_t lda, n, tile;
-    __device__ __forceinline__ double *ptr(int i, int j) const { return a + int64_t(i) * tile + int64_t(j) * tile * lda; }
-    __device__ __forceinline__ int ext(int t) const {
-        const int64_t e = n - int64_t(t) * tile;
-        return static_cast<int>(e < tile ? e : tile);
-    }
-};
+__device__ __forceinline__ double *at(const RunArgs &p, int r, int c) { return p.a + r + int64_t(c) * p.lda; }
 
 __device__ __forceinline__ void report_error(RunCtl *ctl, int code, int info) {
     if (info > 0) atomicMin(&ctl->info, info);
@@ -64,8 +83,8 @@ __device__ __forceinline__ void lower_inverse(int jn, TL tl, double *X) {
 }
 
 // Cholesky of the jn x jn diagonal block at Ad (lower), in shared memory.  Writes L back
-// (lower triangle only; the strict upper triangle of the tile is never touched, as with
-// LAPACK's uplo = 'L') and L^-1 to Wd (ld = ldw, full block with zeros above).
+// (lower triangle only; the strict upper triangle is never touched, as with LAPACK's
+// uplo = 'L') and L^-1 to Wd (ld = p.ws_ld, full block with zeros above).
 __device__ __forceinline__ int factor_chol_diag(const RunArgs &p, double *Ad, int jn, double *Wd,
                                                 double *smem, int info_base) {
     const int tid = threadIdx.x;
@@ -97,7 +116,7 @@ __device__ __forceinline__ int factor_chol_diag(const RunArgs &p, double *Ad, in
         __syncthreads();
     }
     lower_inverse<false>(jn, [&](int i, int l) { return D[i + l * kDiagLd]; }, X);
-    const int64_t ldw = p.tile;
+    const int64_t ldw = p.ws_ld;
     for (int e = tid; e < jn * jn; e += kThreads) {
         const int r = e % jn, c = e / jn;
         if (r >= c) Ad[r + int64_t(c) * lda] = D[r + c * kDiagLd];
@@ -140,7 +159,7 @@ __device__ __forceinline__ int factor_lu_diag(const RunArgs &p, double *Ad, int 
     lower_inverse<true>(jn, [&](int i, int l) { return D[i + l * kDiagLd]; }, XL);
     // U^-1 = ((U^T)^-1)^T, and U^T is lower triangular.
     lower_inverse<false>(jn, [&](int i, int l) { return D[l + i * kDiagLd]; }, XU);
-    const int64_t ldw = p.tile;
+    const int64_t ldw = p.ws_ld;
     for (int e = tid; e < jn * jn; e += kThreads) {
         const int r = e % jn, c = e / jn;
         Ad[r + int64_t(c) * lda] = D[r + c * kDiagLd];
@@ -151,17 +170,15 @@ __device__ __forceinline__ int factor_lu_diag(const RunArgs &p, double *Ad, int 
 }
 
 // ---------------------------------------------------------------------------------
-// POTRF(k,k): left-looking blocked Cholesky of one diagonal tile on one CTA.
+// POTRF: left-looking blocked Cholesky of the m x m diagonal block at (cr, cc), one CTA.
 // ---------------------------------------------------------------------------------
 template <int VEC>
 __device__ int op_potrf(const RunArgs &p, const DevTask &t, double *smem) {
-    using Mn = BlockMma<64, 64, 2, 4, kBNContig, VEC>;
-    const TileView tv{p.a, p.lda, p.n, p.tile};
-    const int k = t.wi;
-    const int n = tv.ext(k);
-    double *A = tv.ptr(k, k);
-    double *W = p.ws_lower + int64_t(k) * p.tile * kNB;
-    const int64_t lda = p.lda;
+    using Mn = PanelMma<kBNContig, VEC>;
+    const int n = t.m;
+    double *A = at(p, t.cr, t.cc);
+    double *W = p.ws_lower + t.cr;
+    const int64_t lda = p.lda, ldw = p.ws_ld;
     for (int jb = 0; jb < n; jb += kNB) {
         const int jn = min(kNB, n - jb);
         if (jb > 0) {
@@ -175,8 +192,7 @@ __device__ int op_potrf(const RunArgs &p, const DevTask &t, double *smem) {
             }
             block_fence_sync();
         }
-        const int st = factor_chol_diag(p, A + jb + int64_t(jb) * lda, jn, W + jb, smem,
-                                        static_cast<int>(int64_t(k) * p.tile) + jb);
+        const int st = factor_chol_diag(p, A + jb + int64_t(jb) * lda, jn, W + jb, smem, t.cc + jb);
         if (st) return st;
         block_fence_sync();
         // A[jb+jn:n, jb:jb+jn] = A[jb+jn:n, jb:jb+jn] * L_jj^-T
@@ -184,7 +200,7 @@ __device__ int op_potrf(const RunArgs &p, const DevTask &t, double *smem) {
             const int mm = min(64, n - r0);
             Mn m;
             m.zero();
-            m.run(smem, A + r0 + int64_t(jb) * lda, lda, W + jb, p.tile, mm, jn, jn);
+            m.run(smem, A + r0 + int64_t(jb) * lda, lda, W + jb, ldw, mm, jn, jn);
             m.store_to(A + r0 + int64_t(jb) * lda, lda, mm, jn);
         }
         block_fence_sync();
@@ -193,18 +209,16 @@ __device__ int op_potrf(const RunArgs &p, const DevTask &t, double *smem) {
 }
 
 // ---------------------------------------------------------------------------------
-// GETRF(k,k) without pivoting: left-looking (Crout) blocked LU on one CTA.
+// GETRF without pivoting: left-looking (Crout) blocked LU of the m x m block, one CTA.
 // ---------------------------------------------------------------------------------
 template <int VEC>
 __device__ int op_getrf(const RunArgs &p, const DevTask &t, double *smem) {
-    using Mk = BlockMma<64, 64, 2, 4, kBKContig, VEC>;
-    const TileView tv{p.a, p.lda, p.n, p.tile};
-    const int k = t.wi;
-    const int n = tv.ext(k);
-    double *A = tv.ptr(k, k);
-    double *WL = p.ws_lower + int64_t(k) * p.tile * kNB;
-    double *WU = p.ws_upper + int64_t(k) * p.tile * kNB;
-    const int64_t lda = p.lda;
+    using Mk = PanelMma<kBKContig, VEC>;
+    const int n = t.m;
+    double *A = at(p, t.cr, t.cc);
+    double *WL = p.ws_lower + t.cr;
+    double *WU = p.ws_upper + t.cr;
+    const int64_t lda = p.lda, ldw = p.ws_ld;
     for (int jb = 0; jb < n; jb += kNB) {
         const int jn = min(kNB, n - jb);
         if (jb > 0) {
@@ -226,8 +240,7 @@ __device__ int op_getrf(const RunArgs &p, const DevTask &t, double *smem) {
             }
             block_fence_sync();
         }
-        const int st = factor_lu_diag(p, A + jb + int64_t(jb) * lda, jn, WL + jb, WU + jb, smem,
-                                      static_cast<int>(int64_t(k) * p.tile) + jb);
+        const int st = factor_lu_diag(p, A + jb + int64_t(jb) * lda, jn, WL + jb, WU + jb, smem, t.cc + jb);
         if (st) return st;
         block_fence_sync();
         // L panel: A[jb+jn:n, jb:jb+jn] = A[...] * U_jj^-1
@@ -235,7 +248,7 @@ __device__ int op_getrf(const RunArgs &p, const DevTask &t, double *smem) {
             const int mm = min(64, n - r0);
             Mk m;
             m.zero();
-            m.run(smem, A + r0 + int64_t(jb) * lda, lda, WU + jb, p.tile, mm, jn, jn);
+            m.run(smem, A + r0 + int64_t(jb) * lda, lda, WU + jb, ldw, mm, jn, jn);
             m.store_to(A + r0 + int64_t(jb) * lda, lda, mm, jn);
         }
         // U row: A[jb:jb+jn, jb+jn:n] = L_jj^-1 * A[...]
@@ -243,7 +256,7 @@ __device__ int op_getrf(const RunArgs &p, const DevTask &t, double *smem) {
             const int nn = min(64, n - c0);
             Mk m;
             m.zero();
-            m.run(smem, WL + jb, p.tile, A + jb + int64_t(c0) * lda, lda, jn, nn, jn);
+            m.run(smem, WL + jb, ldw, A + jb + int64_t(c0) * lda, lda, jn, nn, jn);
             m.store_to(A + jb + int64_t(c0) * lda, lda, jn, nn);
         }
         block_fence_sync();
@@ -252,23 +265,21 @@ __device__ int op_getrf(const RunArgs &p, const DevTask &t, double *smem) {
 }
 
 // ---------------------------------------------------------------------------------
-// TRSM work items: kPanelRows-row (or -column) strips of the written tile, solved
-// left-looking over the kNB-wide diagonal blocks of the triangular tile.
+// TRSM work items: kPanelRows-row (or -column) strips of the block being solved,
+// left-looking over the kNB-wide diagonal blocks of the triangular block.
 // ---------------------------------------------------------------------------------
 
-// A(i,k) = A(i,k) * L(k,k)^-T   (cublasDtrsm R, L, T, NonUnit; cholesky_mustard.cu:281)
+// X = X * L^-T   (cublasDtrsm R, L, T, NonUnit; cholesky_mustard.cu:281)
 template <int VEC>
 __device__ int op_trsm_rlt(const RunArgs &p, const DevTask &t, int item, double *smem) {
-    using Mn = BlockMma<64, 64, 2, 4, kBNContig, VEC>;
-    const TileView tv{p.a, p.lda, p.n, p.tile};
-    const int k = t.aj;
+    using Mn = PanelMma<kBNContig, VEC>;
     const int r0 = item * kPanelRows;
-    const int mm = min(kPanelRows, tv.ext(t.wi) - r0);
-    const int nk = tv.ext(k);
-    const int64_t lda = p.lda;
-    double *X = tv.ptr(t.wi, t.wj) + r0;
-    const double *L = tv.ptr(k, k);
-    const double *W = p.ws_lower + int64_t(k) * p.tile * kNB;
+    const int mm = min(kPanelRows, t.m - r0);
+    const int nk = t.n;
+    const int64_t lda = p.lda, ldw = p.ws_ld;
+    double *X = at(p, t.cr + r0, t.cc);
+    const double *L = at(p, t.ar, t.ac);
+    const double *W = p.ws_lower + t.ar;
     for (int jb = 0; jb < nk; jb += kNB) {
         const int jn = min(kNB, nk - jb);
         if (jb > 0) {
@@ -280,26 +291,24 @@ __device__ int op_trsm_rlt(const RunArgs &p, const DevTask &t, int item, double 
         }
         Mn m;
         m.zero();
-        m.run(smem, X + int64_t(jb) * lda, lda, W + jb, p.tile, mm, jn, jn);
+        m.run(smem, X + int64_t(jb) * lda, lda, W + jb, ldw, mm, jn, jn);
         m.store_to(X + int64_t(jb) * lda, lda, mm, jn);
         block_fence_sync();
     }
     return 0;
 }
 
-// A(i,k) = A(i,k) * U(k,k)^-1   (cublasDtrsm R, U, N, NonUnit; lu_mustard.cu:459)
+// X = X * U^-1   (cublasDtrsm R, U, N, NonUnit; lu_mustard.cu:459)
 template <int VEC>
 __device__ int op_trsm_run(const RunArgs &p, const DevTask &t, int item, double *smem) {
-    using Mk = BlockMma<64, 64, 2, 4, kBKContig, VEC>;
-    const TileView tv{p.a, p.lda, p.n, p.tile};
-    const int k = t.aj;
+    using Mk = PanelMma<kBKContig, VEC>;
     const int r0 = item * kPanelRows;
-    const int mm = min(kPanelRows, tv.ext(t.wi) - r0);
-    const int nk = tv.ext(k);
-    const int64_t lda = p.lda;
-    double *X = tv.ptr(t.wi, t.wj) + r0;
-    const double *U = tv.ptr(k, k);
-    const double *W = p.ws_upper + int64_t(k) * p.tile * kNB;
+    const int mm = min(kPanelRows, t.m - r0);
+    const int nk = t.n;
+    const int64_t lda = p.lda, ldw = p.ws_ld;
+    double *X = at(p, t.cr + r0, t.cc);
+    const double *U = at(p, t.ar, t.ac);
+    const double *W = p.ws_upper + t.ar;
     for (int jb = 0; jb < nk; jb += kNB) {
         const int jn = min(kNB, nk - jb);
         if (jb > 0) {
@@ -311,26 +320,24 @@ __device__ int op_trsm_run(const RunArgs &p, const DevTask &t, int item, double 
         }
         Mk m;
         m.zero();
-        m.run(smem, X + int64_t(jb) * lda, lda, W + jb, p.tile, mm, jn, jn);
+        m.run(smem, X + int64_t(jb) * lda, lda, W + jb, ldw, mm, jn, jn);
         m.store_to(X + int64_t(jb) * lda, lda, mm, jn);
         block_fence_sync();
     }
     return 0;
 }
 
-// A(k,i) = L(k,k)^-1 * A(k,i), unit diagonal   (cublasDtrsm L, L, N, Unit; lu_mustard.cu:413)
+// X = L^-1 * X, unit diagonal   (cublasDtrsm L, L, N, Unit; lu_mustard.cu:413)
 template <int VEC>
 __device__ int op_trsm_llnu(const RunArgs &p, const DevTask &t, int item, double *smem) {
-    using Mk = BlockMma<64, 64, 2, 4, kBKContig, VEC>;
-    const TileView tv{p.a, p.lda, p.n, p.tile};
-    const int k = t.ai;
+    using Mk = PanelMma<kBKContig, VEC>;
     const int c0 = item * kPanelRows;
-    const int nc = min(kPanelRows, tv.ext(t.wj) - c0);
-    const int nk = tv.ext(k);
-    const int64_t lda = p.lda;
-    double *X = tv.ptr(t.wi, t.wj) + int64_t(c0) * lda;
-    const double *L = tv.ptr(k, k);
-    const double *W = p.ws_lower + int64_t(k) * p.tile * kNB;
+    const int nc = min(kPanelRows, t.n - c0);
+    const int nk = t.m;
+    const int64_t lda = p.lda, ldw = p.ws_ld;
+    double *X = at(p, t.cr, t.cc + c0);
+    const double *L = at(p, t.ar, t.ac);
+    const double *W = p.ws_lower + t.ar;
     for (int jb = 0; jb < nk; jb += kNB) {
         const int jn = min(kNB, nk - jb);
         if (jb > 0) {
@@ -342,7 +349,7 @@ __device__ int op_trsm_llnu(const RunArgs &p, const DevTask &t, int item, double
         }
         Mk m;
         m.zero();
-        m.run(smem, W + jb, p.tile, X + jb, lda, jn, nc, jn);
+        m.run(smem, W + jb, ldw, X + jb, lda, jn, nc, jn);
         m.store_to(X + jb, lda, jn, nc);
         block_fence_sync();
     }
@@ -353,61 +360,54 @@ __device__ int op_trsm_llnu(const RunArgs &p, const DevTask &t, int item, double
 // Update work items: one kGemmTile x kGemmTile output block each.
 // ---------------------------------------------------------------------------------
 
-// A(j,i) -= A(j,k) A(i,k)^T   (cublasGemmEx N, T; cholesky_mustard.cu:376)
+// C -= A B^T   (cublasGemmEx N, T; cholesky_mustard.cu:376)
 template <int VEC>
 __device__ int op_gemm_nt(const RunArgs &p, const DevTask &t, int item, double *smem) {
-    using Mg = BlockMma<kGemmTile, kGemmTile, 2, 4, kBNContig, VEC>;
-    const TileView tv{p.a, p.lda, p.n, p.tile};
-    const int M = tv.ext(t.wi), N = tv.ext(t.wj), K = tv.ext(t.aj);
-    const int nbn = (N + kGemmTile - 1) / kGemmTile;
+    using Mg = GemmMma<kBNContig, VEC>;
+    const int nbn = (t.n + kGemmTile - 1) / kGemmTile;
     const int r0 = (item / nbn) * kGemmTile, c0 = (item % nbn) * kGemmTile;
-    const int mm = min(kGemmTile, M - r0), nn = min(kGemmTile, N - c0);
+    const int mm = min(kGemmTile, t.m - r0), nn = min(kGemmTile, t.n - c0);
     Mg m;
     m.zero();
-    m.run(smem, tv.ptr(t.ai, t.aj) + r0, p.lda, tv.ptr(t.bi, t.bj) + c0, p.lda, mm, nn, K);
-    m.sub_from(tv.ptr(t.wi, t.wj) + r0 + int64_t(c0) * p.lda, p.lda, mm, nn);
+    m.run(smem, at(p, t.ar + r0, t.ac), p.lda, at(p, t.br + c0, t.bc), p.lda, mm, nn, t.k);
+    m.sub_from(at(p, t.cr + r0, t.cc + c0), p.lda, mm, nn);
     return 0;
 }
 
-// A(i,j) -= A(i,k) A(k,j)   (cublasGemmEx N, N; lu_mustard.cu:511)
+// C -= A B   (cublasGemmEx N, N; lu_mustard.cu:511)
 template <int VEC>
 __device__ int op_gemm_nn(const RunArgs &p, const DevTask &t, int item, double *smem) {
-    using Mg = BlockMma<kGemmTile, kGemmTile, 2, 4, kBKContig, VEC>;
-    const TileView tv{p.a, p.lda, p.n, p.tile};
-    const int M = tv.ext(t.wi), N = tv.ext(t.wj), K = tv.ext(t.aj);
-    const int nbn = (N + kGemmTile - 1) / kGemmTile;
+    using Mg = GemmMma<kBKContig, VEC>;
+    const int nbn = (t.n + kGemmTile - 1) / kGemmTile;
     const int r0 = (item / nbn) * kGemmTile, c0 = (item % nbn) * kGemmTile;
-    const int mm = min(kGemmTile, M - r0), nn = min(kGemmTile, N - c0);
+    const int mm = min(kGemmTile, t.m - r0), nn = min(kGemmTile, t.n - c0);
     Mg m;
     m.zero();
-    m.run(smem, tv.ptr(t.ai, t.aj) + r0, p.lda, tv.ptr(t.bi, t.bj) + int64_t(c0) * p.lda, p.lda, mm, nn, K);
-    m.sub_from(tv.ptr(t.wi, t.wj) + r0 + int64_t(c0) * p.lda, p.lda, mm, nn);
+    m.run(smem, at(p, t.ar + r0, t.ac), p.lda, at(p, t.br, t.bc + c0), p.lda, mm, nn, t.k);
+    m.sub_from(at(p, t.cr + r0, t.cc + c0), p.lda, mm, nn);
     return 0;
 }
 
-// A(i,i) -= A(i,k) A(i,k)^T, lower triangle only   (cublasDsyrk L, N; cholesky_mustard.cu:327)
+// C -= A A^T, lower triangle only   (cublasDsyrk L, N; cholesky_mustard.cu:327)
 template <int VEC>
 __device__ int op_syrk_ln(const RunArgs &p, const DevTask &t, int item, double *smem) {
-    using Mg = BlockMma<kGemmTile, kGemmTile, 2, 4, kBNContig, VEC>;
-    const TileView tv{p.a, p.lda, p.n, p.tile};
-    const int M = tv.ext(t.wi), K = tv.ext(t.aj);
+    using Mg = GemmMma<kBNContig, VEC>;
     int pb = 0;
     while ((pb + 1) * (pb + 2) / 2 <= item) ++pb;
     const int qb = item - pb * (pb + 1) / 2;
     const int r0 = pb * kGemmTile, c0 = qb * kGemmTile;
-    const int mm = min(kGemmTile, M - r0), nn = min(kGemmTile, M - c0);
-    const double *A = tv.ptr(t.ai, t.aj);
+    const int mm = min(kGemmTile, t.m - r0), nn = min(kGemmTile, t.m - c0);
     Mg m;
     m.zero();
-    m.run(smem, A + r0, p.lda, A + c0, p.lda, mm, nn, K);
-    m.sub_from(tv.ptr(t.wi, t.wj) + r0 + int64_t(c0) * p.lda, p.lda, mm, nn, pb == qb, 0, 0);
+    m.run(smem, at(p, t.ar + r0, t.ac), p.lda, at(p, t.ar + c0, t.ac), p.lda, mm, nn, t.k);
+    m.sub_from(at(p, t.cr + r0, t.cc + c0), p.lda, mm, nn, pb == qb, 0, 0);
     return 0;
 }
 
 // Shared memory (bytes) the largest operation needs.
 constexpr int kOpSmemBytes() {
-    constexpr int g1 = BlockMma<kGemmTile, kGemmTile, 2, 4, kBNContig, 2>::SMEM_DOUBLES;
-    constexpr int g2 = BlockMma<kGemmTile, kGemmTile, 2, 4, kBKContig, 2>::SMEM_DOUBLES;
+    constexpr int g1 = GemmMma<kBNContig, 2>::SMEM_DOUBLES;
+    constexpr int g2 = GemmMma<kBKContig, 2>::SMEM_DOUBLES;
     constexpr int diag = 3 * kNB * kDiagLd;
     constexpr int m = g1 > g2 ? g1 : g2;
     return 8 * (m > diag ? m : diag);

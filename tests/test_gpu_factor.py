@@ -134,7 +134,8 @@ def test_trace_and_stats(mtd):
     out, info, g = factor(mtd, a, 256, "chol", trace=True)
     st = g.stats()
     total_items = sum(g.items(t) for t in range(g.num_tasks))
-    assert st["tasks"] == g.num_tasks and st["items"] == total_items
+    assert st["tasks"] == g.num_device_tasks and st["items"] == total_items
+    assert g.num_device_tasks > g.num_tasks  # the 256-wide diagonal tiles are nested (128)
     assert 0.0 < st["busy_fraction"] <= 1.0 and st["span_ms"] > 0
     recs = g.trace()
     assert len(recs) == total_items
@@ -189,3 +190,29 @@ def test_cuda_graph_executor_matches_scheduler(mtd, kind):
     g.run_graph(d3)  # cached CUDA graph, second launch
     assert np.array_equal(from_dev(d3), y)
     g.close()
+
+
+@pytest.mark.parametrize("kind", ["chol", "lu"])
+@pytest.mark.parametrize("nest", [0, 64, 128, 256])
+def test_nested_diagonal_factorisation(mtd, kind, nest):
+    # POTRF / GETRF of a 640-wide tile lowered to a tiled sub-factorisation (or not: 0)
+    n, tile = 1400, 640
+    a = gen.spd_input(n, 13) if kind == "chol" else gen.lu_input(n, 13)
+    g = mtd.TaskGraph(mtd.KIND_CHOLESKY if kind == "chol" else mtd.KIND_LU, n, tile).build_tiled()
+    g.set_nest(nest).finalize()
+    if nest:
+        assert g.num_device_tasks > g.num_tasks
+    d = to_dev(a)
+    assert g.run(d) == 0
+    ref = oracle_factor(a, tile, kind)
+    out = from_dev(d)
+    if kind == "chol":
+        out, ref = np.tril(out), np.tril(ref)
+    assert rel_diff(out, ref) <= TOL
+    g.close()
+
+
+def test_nest_edge_must_be_multiple_of_64(mtd):
+    g = mtd.TaskGraph(mtd.KIND_CHOLESKY, 600, 300).build_tiled()
+    with pytest.raises(mtd.MtdError):
+        g.set_nest(100)
