@@ -43,7 +43,8 @@ typedef enum mtd_status {
     MTD_ERR_BAD_DAG = 7,         /* graph cannot be executed (see mtd_graph_finalize)   */
     MTD_ERR_NO_DEVICE = 8,       /* no CUDA device / not an sm_100 device               */
     MTD_ERR_OUT_OF_MEMORY = 9,   /* device allocation failed                            */
-    MTD_ERR_QUEUE = 10           /* ready-queue overflow (internal invariant broken)    */
+    MTD_ERR_QUEUE = 10,          /* ready-queue overflow (internal invariant broken)    */
+    MTD_ERR_TOO_LARGE = 11       /* problem exceeds mtd_factor_noalloc's fixed scratch  */
 } mtd_status;
 
 typedef enum mtd_kind {
@@ -170,6 +171,32 @@ int mtd_tiled_cholesky(double *dA, int64_t n, int64_t lda, int64_t tile, void *s
                        int *info_out);
 int mtd_tiled_lu(double *dA, int64_t n, int64_t lda, int64_t tile, void *stream,
                  int *info_out);
+
+/* ---- factorisation without any device allocation ----
+ *
+ * No counterpart in the reference.  Every other entry point gets its task table, ready
+ * queues, counters and inverse workspace from cudaMalloc.  Some callers cannot do that:
+ * code that runs while a stream is being captured into a CUDA graph (a cudaMalloc there
+ * breaks the capture), applications whose device memory is owned entirely by a pool
+ * allocator (PyTorch's caching allocator, RAPIDS RMM) that must not see raw allocations,
+ * and latency-critical services that cannot afford an allocation, or its failure, on the
+ * request path.  This entry point serves them: it runs the same tiled LU (kind
+ * MTD_KIND_LU) or Cholesky (MTD_KIND_CHOLESKY) as mtd_tiled_lu / mtd_tiled_cholesky, but
+ * all of its device scratch lives in one fixed, file-scope device array of 24 MiB inside
+ * this library (every GPU that loads the library holds it until the process exits).  It
+ * calls no cudaMalloc, cudaFree, cudaMallocHost or other allocating CUDA routine; the task
+ * list is assembled in ordinary host memory and copied into the array.
+ *
+ * Limits: n <= 16384 and, for the chosen tile, at most 32768 device tasks, 131072
+ * dependency edges and 262144 work items; larger problems return MTD_ERR_TOO_LARGE.
+ * The first call on a device looks up the array's device address (and sets the kernel's
+ * shared-memory limit); make that first call before any stream capture.
+ * All calls share the one array: calls whose work overlaps on the GPU (different streams,
+ * host threads, or graphs) race and corrupt each other's results; serialise them.  The
+ * call waits for its stream and returns the run's status; info_out (may be NULL)
+ * receives LAPACK-style info as with mtd_run. */
+int mtd_factor_noalloc(int kind, double *dA, int64_t n, int64_t lda, int64_t tile, void *stream,
+                       int *info_out);
 
 /* ---- inputs: device generators (the reference builds its input on the host,
  *      include/gen.h:23-38; these make the seeded inputs of the benchmark shapes) ---- */

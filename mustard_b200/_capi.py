@@ -8,11 +8,12 @@ _LIB_PATH = os.path.join(_HERE, "lib", "libmustard_b200.so")
 OK = 0
 ERR_INVALID_ARG, ERR_STATE, ERR_CUDA, ERR_TIMEOUT = 1, 2, 3, 4
 ERR_NOT_POSITIVE_DEFINITE, ERR_SINGULAR, ERR_BAD_DAG = 5, 6, 7
-ERR_NO_DEVICE, ERR_OUT_OF_MEMORY, ERR_QUEUE = 8, 9, 10
+ERR_NO_DEVICE, ERR_OUT_OF_MEMORY, ERR_QUEUE, ERR_TOO_LARGE = 8, 9, 10, 11
 STATUS_NAMES = {
     0: "MTD_OK", 1: "MTD_ERR_INVALID_ARG", 2: "MTD_ERR_STATE", 3: "MTD_ERR_CUDA",
     4: "MTD_ERR_TIMEOUT", 5: "MTD_ERR_NOT_POSITIVE_DEFINITE", 6: "MTD_ERR_SINGULAR",
     7: "MTD_ERR_BAD_DAG", 8: "MTD_ERR_NO_DEVICE", 9: "MTD_ERR_OUT_OF_MEMORY", 10: "MTD_ERR_QUEUE",
+    11: "MTD_ERR_TOO_LARGE",
 }
 
 KIND_LU, KIND_CHOLESKY, KIND_CUSTOM = 0, 1, 2
@@ -51,6 +52,7 @@ SIGNATURES = {
     "mtd_graph_destroy": (_i, [_vp]),
     "mtd_tiled_cholesky": (_i, [_vp, _i64, _i64, _i64, _vp, ctypes.POINTER(_i)]),
     "mtd_tiled_lu": (_i, [_vp, _i64, _i64, _i64, _vp, ctypes.POINTER(_i)]),
+    "mtd_factor_noalloc": (_i, [_i, _vp, _i64, _i64, _i64, _vp, ctypes.POINTER(_i)]),
     "mtd_generate": (_i, [_vp, _i64, _i64, _i, ctypes.c_uint64, _d, _vp]),
     "mtd_generate_reference_host": (_i, [ctypes.POINTER(_d), _i64]),
     "mtd_probe_fp64_peak": (_i, [ctypes.POINTER(_d)]),

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -12,6 +13,17 @@
 #include "scheduler.cuh"
 
 using namespace mtd;
+
+// Device scratch of mtd_factor_noalloc: task table, successor lists, counters, ready
+// queues, control block and inverse workspaces of one factorisation, carved from this
+// one array at 256-byte boundaries.  Its size and the limits below are fixed; every GPU
+// that loads the library holds the array until the process exits.
+constexpr size_t kNoAllocBytes = size_t(24) << 20;
+constexpr int64_t kNoAllocMaxN = 16384;
+constexpr int kNoAllocMaxTasks = 32768;
+constexpr int kNoAllocMaxEdges = 131072;
+constexpr long long kNoAllocMaxItems = 262144;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 struct mtd_graph {
     Dag dag;
@@ -219,6 +231,7 @@ const char *mtd_strerror(int status) {
     case MTD_ERR_NO_DEVICE: return "no sm_100 CUDA device";
     case MTD_ERR_OUT_OF_MEMORY: return "device allocation failed";
     case MTD_ERR_QUEUE: return "ready-queue overflow";
+    case MTD_ERR_TOO_LARGE: return "problem exceeds the fixed scratch of mtd_factor_noalloc";
     default: return "unknown status";
     }
 }
@@ -497,3 +510,135 @@ int mtd_tiled_lu(double *dA, int64_t n, int64_t lda, int64_t tile, void *stream,
 }
 
 }  // extern "C"
+
+namespace {
+
+// Per-device set-up of mtd_factor_noalloc, done by the first call on each device: in host
+// code the array's name is only a host-side stand-in, so its device address comes from
+// cudaGetSymbolAddress with that device current.
+int noalloc_scratch(int device, unsigned char **out) {
+    static std::mutex mu;
+    static unsigned char *addr[64] = {nullptr};
+    if (device < 0 || device >= 64) return MTD_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[device]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) {
+            cudaGetLastError();
+            return MTD_ERR_CUDA;
+        }
+        addr[device] = static_cast<unsigned char *>(p);
+    }
+    int rc = smem_setup<2>(device);
+    if (!rc) rc = smem_setup<1>(device);
+    if (rc) return rc;
+    *out = addr[device];
+    return MTD_OK;
+}
+
+// Bump allocation inside the fixed scratch (256-byte aligned pieces).
+struct ScratchCarver {
+    unsigned char *base;
+    size_t used = 0;
+    template <typename T>
+    T *take(size_t count) {
+        used = (used + 255) & ~size_t(255);
+        T *p = reinterpret_cast<T *>(base + used);
+        used += (count ? count : 1) * sizeof(T);
+        return p;
+    }
+};
+
+}  // namespace
+
+extern "C" int mtd_factor_noalloc(int kind, double *dA, int64_t n, int64_t lda, int64_t tile, void *stream,
+                                  int *info_out) {
+    if (info_out) *info_out = 0;
+    if (kind != MTD_KIND_LU && kind != MTD_KIND_CHOLESKY) return MTD_ERR_INVALID_ARG;
+    if (!dA || n <= 0 || tile <= 0 || tile > n || lda < n) return MTD_ERR_INVALID_ARG;
+    if (n > kNoAllocMaxN) return MTD_ERR_TOO_LARGE;
+
+    // The task graph: host memory only.
+    Dag dag(kind, n, tile);
+    int rc = dag.build_reference_order();
+    if (rc) return rc;
+    Lowered low;
+    rc = dag.lower(kNestTile, low);
+    if (rc) return rc;
+    const int nt = static_cast<int>(low.tasks.size());
+    const long long items = low.queue_cap[0] + low.queue_cap[1];
+    if (nt > kNoAllocMaxTasks || static_cast<long long>(low.succ.size()) > kNoAllocMaxEdges ||
+        items > kNoAllocMaxItems)
+        return MTD_ERR_TOO_LARGE;
+    std::vector<int> deps_init(nt), roots;
+    for (int t = 0; t < nt; ++t) {
+        deps_init[t] = static_cast<int>(low.preds[t].size());
+        if (deps_init[t] == 0) roots.push_back(t);
+    }
+    if (roots.empty()) return MTD_ERR_BAD_DAG;
+
+    int device = 0, sms = 0;
+    rc = check_device(&device, &sms);
+    if (rc) return rc;
+    unsigned char *scratch = nullptr;
+    rc = noalloc_scratch(device, &scratch);
+    if (rc) return rc;
+
+    const int64_t wld = n + (n & 1);
+    ScratchCarver sc{scratch};
+    RunArgs a{};
+    DevTask *d_tasks = sc.take<DevTask>(nt);
+    int *d_succ = sc.take<int>(low.succ.size());
+    int *d_deps_init = sc.take<int>(nt);
+    int *d_roots = sc.take<int>(roots.size());
+    a.deps = sc.take<int>(nt);
+    a.items_left = sc.take<int>(nt);
+    for (int q = 0; q < kNumQueues; ++q) {
+        a.queue[q] = sc.take<unsigned long long>(size_t(low.queue_cap[q]));
+        a.queue_cap[q] = low.queue_cap[q];
+    }
+    a.qctl = sc.take<QueueCtl>(kNumQueues);
+    a.ctl = sc.take<RunCtl>(1);
+    a.ws_lower = sc.take<double>(size_t(wld) * kNB);
+    a.ws_upper = kind == MTD_KIND_LU ? sc.take<double>(size_t(wld) * kNB) : nullptr;
+    if (sc.used > kNoAllocBytes) return MTD_ERR_TOO_LARGE;
+    a.a = dA;
+    a.lda = lda;
+    a.n_tasks = nt;
+    a.tasks = d_tasks;
+    a.succ = d_succ;
+    a.ws_ld = wld;
+    a.trace = nullptr;
+    a.trace_cap = 0;
+    a.timeout_ns = 10ull * 1000000000ull;
+
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    bool ok = cudaMemcpyAsync(d_tasks, low.tasks.data(), nt * sizeof(DevTask), cudaMemcpyHostToDevice, s) ==
+              cudaSuccess;
+    ok = ok && (low.succ.empty() || cudaMemcpyAsync(d_succ, low.succ.data(), low.succ.size() * sizeof(int),
+                                                    cudaMemcpyHostToDevice, s) == cudaSuccess);
+    ok = ok && cudaMemcpyAsync(d_deps_init, deps_init.data(), nt * sizeof(int), cudaMemcpyHostToDevice, s) ==
+                   cudaSuccess;
+    ok = ok && cudaMemcpyAsync(d_roots, roots.data(), roots.size() * sizeof(int), cudaMemcpyHostToDevice, s) ==
+                   cudaSuccess;
+    if (!ok) return MTD_ERR_CUDA;
+    // reset_kernel zeroes the counters and control block and empties the queues, so
+    // nothing left in the array by an earlier call leaks into this one; the inverse
+    // workspace is always written by a diagonal factorisation before it is read.
+    const bool vec2 = (reinterpret_cast<uintptr_t>(dA) % 16 == 0) && (lda % 2 == 0) && (tile % 2 == 0) &&
+                      (n % 2 == 0);
+    const int reset_blocks =
+        static_cast<int>(std::min<long long>(1024, (std::max<long long>(items, nt) + kThreads - 1) / kThreads));
+    reset_kernel<<<std::max(reset_blocks, 1), kThreads, 0, s>>>(a, d_deps_init);
+    seed_kernel<<<1, 32, 0, s>>>(a, d_roots, static_cast<int>(roots.size()));
+    if (vec2) persistent_kernel<2><<<sms, kThreads, kOpSmemBytes(), s>>>(a);
+    else persistent_kernel<1><<<sms, kThreads, kOpSmemBytes(), s>>>(a);
+    if (cudaGetLastError() != cudaSuccess) return MTD_ERR_CUDA;
+    RunCtl c;
+    if (cudaMemcpyAsync(&c, a.ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, s) != cudaSuccess) return MTD_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return MTD_ERR_CUDA;
+    if (info_out) *info_out = (c.error != 0 && c.info != 0x7fffffff) ? c.info : 0;
+    if (c.error) return c.error;
+    if (c.tasks_done != nt) return MTD_ERR_TIMEOUT;
+    return MTD_OK;
+}
