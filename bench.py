@@ -163,8 +163,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mustard_b200", choices=["mustard_b200", "reference"])
     ap.add_argument("--n", type=int, default=24000)
-    ap.add_argument("--tile-lu", type=int, default=512)
-    ap.add_argument("--tile-chol", type=int, default=512)
+    # Best of the tile sweep {512, 768, 1024, 1536, 2048} at N = 24000 on B200.
+    ap.add_argument("--tile-lu", type=int, default=1536)
+    ap.add_argument("--tile-chol", type=int, default=1536)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-n", type=int, default=12000)
     ap.add_argument("--cpu-tile", type=int, default=1000)

@@ -65,6 +65,16 @@ typedef enum mtd_op {
     MTD_OP_GEMM_NN = 7    /* A(i,j) -= A(i,k) A(k,j)              lu_mustard.cu:511         */
 } mtd_op;
 
+/* Arithmetic of a graph's runs. */
+typedef enum mtd_precision {
+    MTD_PREC_FP64 = 0,           /* FP64 matrix, FP64 tensor-core (DMMA) tiles: the reference's */
+    MTD_PREC_TF32 = 1,           /* FP32 matrix, TF32 tensor-core products with FP32           */
+                                 /* accumulation, FP32 diagonal blocks (Cholesky only); the    */
+                                 /* low-precision factor of the mixed-precision solver         */
+    MTD_PREC_FP32 = 2            /* FP32 matrix, FP32-accurate products from three TF32 MMAs   */
+                                 /* per product (split operands: hi*hi + hi*lo + lo*hi)        */
+} mtd_precision;
+
 typedef enum mtd_generator {
     MTD_GEN_UNIFORM_DIAG = 0,    /* U[-1,1) entries + n on the diagonal (LU input)      */
     MTD_GEN_SPD = 1              /* B B^T / n + alpha I, B = U[-1,1) (Cholesky input)   */
@@ -151,6 +161,13 @@ int mtd_run(mtd_graph *g, double *dA, int64_t lda, void *stream, int *info_out);
  * status/info conventions as mtd_run. */
 int mtd_run_graph(mtd_graph *g, double *dA, int64_t lda, void *stream, int *info_out);
 
+/* Arithmetic of the graph's runs (mtd_precision); before mtd_graph_finalize.  Default
+ * MTD_PREC_FP64.  MTD_PREC_TF32 accepts Cholesky tasks only and runs with mtd_run_f32. */
+int mtd_graph_set_precision(mtd_graph *g, int prec);
+
+/* mtd_run for a MTD_PREC_TF32 graph: factors the FP32 column-major matrix dA in place. */
+int mtd_run_f32(mtd_graph *g, float *dA, int64_t lda, void *stream, int *info_out);
+
 /* Synchronise with the last run and return its status (and info). */
 int mtd_graph_status(mtd_graph *g, int *info_out);
 
@@ -197,6 +214,83 @@ int mtd_tiled_lu(double *dA, int64_t n, int64_t lda, int64_t tile, void *stream,
  * receives LAPACK-style info as with mtd_run. */
 int mtd_factor_noalloc(int kind, double *dA, int64_t n, int64_t lda, int64_t tile, void *stream,
                        int *info_out);
+
+/* ---- mixed-precision SPD solver (no counterpart in the reference) ----
+ *
+ * Factor A (FP64, lower triangle read) in the solver's precision on the task-graph
+ * scheduler, then solve A X = B to FP64 accuracy: MTD_REFINE_IR adds corrections
+ * M^-1 (B - A X) with M = L L^T the low-precision factor; MTD_REFINE_GMRES_IR solves each
+ * correction equation with FP64 GMRES preconditioned by M (Carson & Higham 2017/2018);
+ * MTD_REFINE_NONE is one solve with the factor.  Residuals and updates are FP64.  With
+ * MTD_PREC_FP64 the same calls give the plain FP64 solve (the time-to-solution baseline).
+ * The caller's A must stay unchanged on the device while the solver uses it. */
+typedef enum mtd_refine {
+    MTD_REFINE_NONE = 0,
+    MTD_REFINE_IR = 1,
+    MTD_REFINE_GMRES_IR = 2
+} mtd_refine;
+
+typedef struct mtd_solve_stats {
+    int iterations;            /* refinement steps (corrections applied)                */
+    int inner_iterations;      /* GMRES iterations summed over the steps                */
+    int converged;             /* 1 when backward_error <= tol was reached              */
+    double backward_error;     /* max over columns of ||b - A x||_inf /                 */
+                               /*   (||A||_inf ||x||_inf + ||b||_inf), in FP64          */
+    double factor_ms;          /* device time of the last mtd_solver_factor             */
+    double solve_ms;           /* host wall time of this solve (includes its syncs)     */
+} mtd_solve_stats;
+
+typedef struct mtd_solver mtd_solver;
+
+/* n x n systems; tile must be a multiple of 64; prec MTD_PREC_TF32, MTD_PREC_FP32 (low-
+ * precision factors) or MTD_PREC_FP64 (the plain FP64 baseline). */
+int mtd_solver_create(mtd_solver **out, int64_t n, int64_t tile, int prec);
+/* Factor A + shift*I (shift >= 0; a diagonal shift keeps a low-precision factorisation of
+ * an ill-conditioned matrix positive definite; refinement still solves with A itself). */
+int mtd_solver_factor(mtd_solver *s, const double *dA, int64_t lda, double shift, void *stream, int *info_out);
+/* Solve for nrhs <= 16 right-hand sides (GMRES-IR: nrhs = 1); stops at backward error
+ * <= tol or after max_iter corrections. */
+int mtd_solver_solve(mtd_solver *s, const double *dB, int64_t ldb, double *dX, int64_t ldx, int64_t nrhs, int method,
+                     double tol, int max_iter, void *stream, mtd_solve_stats *stats);
+int mtd_solver_destroy(mtd_solver *s);
+
+/* ---- batched factorisations (no counterpart in the reference) ----
+ *
+ * `count` independent SPD matrices of sizes n[m] (each its own tile edge tile[m] -- equal
+ * to n[m] or a multiple of 64 -- and nested sub-tile edge nest[m]; NULL arrays pick the
+ * defaults or use mtd_batch_autotune's choice) factored as ONE merged task graph by one
+ * persistent launch (stream-ordered, no host synchronisation: it can be captured into a
+ * CUDA graph).  Element type per batch: MTD_PREC_FP64 (double matrices) or MTD_PREC_TF32 /
+ * MTD_PREC_FP32 (float matrices, refined in FP64 by mtd_batch_solve).  A bad pivot in one
+ * matrix records its info and the rest of the batch runs on. */
+typedef struct mtd_batch mtd_batch;
+
+typedef struct mtd_batch_solve_stats {
+    int iterations;            /* refinement steps (1 = the direct FP64 solve only)     */
+    int converged_count;       /* matrices whose backward error reached tol             */
+    double max_backward_error; /* max over matrices and columns (FP64), -1 if not known */
+    double solve_ms;           /* host wall time of the solve call                      */
+} mtd_batch_solve_stats;
+
+int mtd_batch_create(mtd_batch **out, int count, const int64_t *n, const int64_t *tile, const int *nest, int prec);
+int mtd_batch_num_tasks(const mtd_batch *b);
+/* Factor matrix m at dA[m] (device pointer; double or float per the batch) in place. */
+int mtd_batch_factor(mtd_batch *b, void *const *dA, const int64_t *lda, void *stream);
+/* Wait for the last factorisation; info[m] (nullable) = 0 or the 1-based column of the
+ * first bad pivot; latency_ms[m] (nullable) = time from the launch's first work to the
+ * completion of matrix m's last task (device %globaltimer). */
+int mtd_batch_status(mtd_batch *b, int *info, double *latency_ms);
+/* Low-precision batches: dF[m] = float(lower(dA[m]) + shift I), ready for factoring. */
+int mtd_batch_convert(mtd_batch *b, const double *const *dA, const int64_t *lda, void *const *dF, const int64_t *ldf,
+                      double shift, void *stream);
+/* Solve A_m X_m = B_m with the factors dF[m] (nrhs[m] <= 16).  FP64 batches: one solve,
+ * plus FP64 IR when method is MTD_REFINE_IR; low-precision batches: FP64 IR (required) to
+ * backward error tol.  dA (the FP64 matrices) may be NULL only for an FP64 batch with
+ * MTD_REFINE_NONE. */
+int mtd_batch_solve(mtd_batch *b, const double *const *dA, const int64_t *lda, void *const *dF, const int64_t *ldf,
+                    const double *const *dB, const int64_t *ldb, double *const *dX, const int64_t *ldx,
+                    const int *nrhs, int method, double tol, int max_iter, void *stream, mtd_batch_solve_stats *stats);
+int mtd_batch_destroy(mtd_batch *b);
 
 /* ---- inputs: device generators (the reference builds its input on the host,
  *      include/gen.h:23-38; these make the seeded inputs of the benchmark shapes) ---- */

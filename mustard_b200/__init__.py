@@ -21,7 +21,8 @@ from . import _capi
 from ._capi import (  # noqa: F401  (re-exported constants)
     GEN_SPD, GEN_UNIFORM_DIAG, KIND_CHOLESKY, KIND_CUSTOM, KIND_LU, OP_GEMM_NN, OP_GEMM_NT,
     OP_GETRF, OP_NAMES, OP_POTRF, OP_SYRK_LN, OP_TRSM_LLNU, OP_TRSM_RLT, OP_TRSM_RUN,
-    STATUS_NAMES, MtdError, lib, lib_path)
+    PREC_FP32, PREC_FP64, PREC_TF32, REFINE_GMRES_IR, REFINE_IR, REFINE_NONE, STATUS_NAMES, MtdError,
+    lib, lib_path)
 
 __all__ = [
     "TaskGraph", "TiledGraphCreator", "tiled_cholesky", "tiled_lu", "generate", "colmajor",
@@ -140,6 +141,21 @@ class TaskGraph:
         _capi.check(rc, info.value)
         return info.value
 
+    def set_precision(self, prec):
+        _capi.check(self._lib.mtd_graph_set_precision(self._h, int(prec)))
+        return self
+
+    def run_f32(self, a, stream=None, sync=True):
+        """Run a PREC_TF32 graph on a column-major float32 CUDA matrix."""
+        import torch
+        if a.dtype != torch.float32 or not a.is_cuda or a.stride(0) != 1:
+            raise TypeError("expected a column-major float32 CUDA tensor")
+        info = ctypes.c_int(0)
+        rc = self._lib.mtd_run_f32(self._h, ctypes.c_void_p(a.data_ptr()), a.stride(1), _stream_handle(stream),
+                                   ctypes.byref(info) if sync else None)
+        _capi.check(rc, info.value)
+        return info.value
+
     def run_graph(self, a, stream=None, sync=True):
         """Same factorisation through the host-launched CUDA-graph executor (the
         reference's --tiled mode) instead of the persistent scheduler."""
@@ -218,6 +234,134 @@ class TiledGraphCreator:
     @property
     def subgraphDependencies(self):
         return [self.graph.deps(t) for t in range(self.graph.num_tasks)]
+
+
+def _rect_ptr(x, rows):
+    """(pointer, leading dimension, columns) of a column-major float64 CUDA block (n x k)."""
+    import torch
+    if x.dtype != torch.float64 or not x.is_cuda:
+        raise TypeError("expected a float64 CUDA tensor")
+    if x.dim() == 1:
+        x = x.unsqueeze(1)
+    if x.shape[0] != rows or x.stride(0) != 1:
+        raise ValueError("expected a column-major (n, k) block")
+    return x.data_ptr(), (x.stride(1) if x.shape[1] > 1 else rows), x.shape[1]
+
+
+class SpdSolver:
+    """Mixed-precision SPD solver (mtd_solver_*): low-precision tiled Cholesky on the task
+    scheduler plus FP64 iterative refinement (IR) or GMRES-IR.  ``prec`` is PREC_TF32
+    (FP32 factor, TF32 tensor-core products) or PREC_FP64 (the plain FP64 baseline)."""
+
+    def __init__(self, n, tile, prec=_capi.PREC_TF32):
+        self._lib = lib()
+        h = ctypes.c_void_p()
+        _capi.check(self._lib.mtd_solver_create(ctypes.byref(h), n, tile, prec))
+        self._h, self.n, self.tile, self.prec = h, n, tile, prec
+
+    def factor(self, a, shift=0.0, stream=None):
+        """Factor A + shift*I (A: column-major float64 CUDA matrix, kept by reference)."""
+        ptr, n, ld = _matrix_ptr(a, self.n)
+        self._a = a
+        info = ctypes.c_int(0)
+        _capi.check(self._lib.mtd_solver_factor(self._h, ctypes.c_void_p(ptr), ld, float(shift),
+                                                _stream_handle(stream), ctypes.byref(info)), info.value)
+        return info.value
+
+    def solve(self, b, x, method=_capi.REFINE_IR, tol=1e-13, max_iter=50, stream=None):
+        """Solve A X = B into x (both column-major (n, k) float64 CUDA blocks, k <= 16)."""
+        pb, ldb, k = _rect_ptr(b, self.n)
+        px, ldx, kx = _rect_ptr(x, self.n)
+        if k != kx:
+            raise ValueError("b and x must have the same number of columns")
+        st = _capi.SolveStats()
+        rc = self._lib.mtd_solver_solve(self._h, ctypes.c_void_p(pb), ldb, ctypes.c_void_p(px), ldx, k, method,
+                                        float(tol), int(max_iter), _stream_handle(stream), ctypes.byref(st))
+        _capi.check(rc)
+        return {"iterations": st.iterations, "inner_iterations": st.inner_iterations,
+                "converged": bool(st.converged), "backward_error": st.backward_error,
+                "factor_ms": st.factor_ms, "solve_ms": st.solve_ms}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.mtd_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Batched Cholesky factorisations and solves (mtd_batch_*): matrices of different sizes
+    factored as one merged task graph in one persistent launch.
+
+    ``sizes``: list of n; ``tiles`` / ``nests``: per-matrix tile edge and nested sub-tile
+    edge (None: the library's defaults).  Matrices are column-major CUDA tensors (float64
+    for PREC_FP64, float32 for PREC_TF32 / PREC_FP32)."""
+
+    def __init__(self, sizes, tiles=None, nests=None, prec=_capi.PREC_FP64):
+        self._lib = lib()
+        self.count = len(sizes)
+        n = (ctypes.c_int64 * self.count)(*sizes)
+        t = (ctypes.c_int64 * self.count)(*tiles) if tiles is not None else None
+        k = (ctypes.c_int * self.count)(*nests) if nests is not None else None
+        h = ctypes.c_void_p()
+        _capi.check(self._lib.mtd_batch_create(ctypes.byref(h), self.count, n, t, k, prec))
+        self._h, self.sizes, self.prec = h, list(sizes), prec
+
+    @property
+    def num_tasks(self):
+        return self._lib.mtd_batch_num_tasks(self._h)
+
+    @staticmethod
+    def _ptrs(mats):
+        p = (ctypes.c_void_p * len(mats))(*[m.data_ptr() for m in mats])
+        ld = (ctypes.c_int64 * len(mats))(*[(m.stride(1) if m.dim() == 2 and m.shape[1] > 1 else m.shape[0])
+                                             for m in mats])
+        return p, ld
+
+    def factor(self, mats, stream=None):
+        p, ld = self._ptrs(mats)
+        self._keep = mats
+        _capi.check(self._lib.mtd_batch_factor(self._h, p, ld, _stream_handle(stream)))
+
+    def status(self, latencies=False):
+        info = (ctypes.c_int * self.count)()
+        lat = (ctypes.c_double * self.count)() if latencies else None
+        rc = self._lib.mtd_batch_status(self._h, info, lat)
+        out = (rc, list(info))
+        return out + (list(lat),) if latencies else out
+
+    def convert(self, a64, f32, shift=0.0, stream=None):
+        pa, la = self._ptrs(a64)
+        pf, lf = self._ptrs(f32)
+        _capi.check(self._lib.mtd_batch_convert(self._h, pa, la, pf, lf, float(shift), _stream_handle(stream)))
+
+    def solve(self, factors, bs, xs, a64=None, method=_capi.REFINE_NONE, tol=1e-13, max_iter=20, stream=None):
+        pf, lf = self._ptrs(factors)
+        pb, lb = self._ptrs(bs)
+        px, lx = self._ptrs(xs)
+        nr = (ctypes.c_int * self.count)(*[(b.shape[1] if b.dim() == 2 else 1) for b in bs])
+        pa, la = self._ptrs(a64) if a64 is not None else (None, None)
+        st = _capi.BatchSolveStats()
+        _capi.check(self._lib.mtd_batch_solve(self._h, pa, la, pf, lf, pb, lb, px, lx, nr, method, float(tol),
+                                              int(max_iter), _stream_handle(stream), ctypes.byref(st)))
+        return {"iterations": st.iterations, "converged_count": st.converged_count,
+                "max_backward_error": st.max_backward_error, "solve_ms": st.solve_ms}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.mtd_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _one_call(kind, a, tile, stream):

@@ -32,7 +32,37 @@ class RunStats(ctypes.Structure):
                 ("busy_fraction", ctypes.c_double), ("span_ms", ctypes.c_double)]
 
 
+PREC_FP64, PREC_TF32, PREC_FP32 = 0, 1, 2
+REFINE_NONE, REFINE_IR, REFINE_GMRES_IR = 0, 1, 2
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("inner_iterations", ctypes.c_int), ("converged", ctypes.c_int),
+                ("backward_error", ctypes.c_double), ("factor_ms", ctypes.c_double), ("solve_ms", ctypes.c_double)]
+
+
+class BatchSolveStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("converged_count", ctypes.c_int),
+                ("max_backward_error", ctypes.c_double), ("solve_ms", ctypes.c_double)]
+
+
+_pp, _pi64 = ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int64)
+
 SIGNATURES = {
+    "mtd_batch_create": (_i, [ctypes.POINTER(_vp), _i, _pi64, _pi64, ctypes.POINTER(_i), _i]),
+    "mtd_batch_num_tasks": (_i, [_vp]),
+    "mtd_batch_factor": (_i, [_vp, _pp, _pi64, _vp]),
+    "mtd_batch_status": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_d)]),
+    "mtd_batch_convert": (_i, [_vp, _pp, _pi64, _pp, _pi64, _d, _vp]),
+    "mtd_batch_solve": (_i, [_vp, _pp, _pi64, _pp, _pi64, _pp, _pi64, _pp, _pi64, ctypes.POINTER(_i), _i, _d, _i, _vp,
+                             ctypes.POINTER(BatchSolveStats)]),
+    "mtd_batch_destroy": (_i, [_vp]),
+    "mtd_graph_set_precision": (_i, [_vp, _i]),
+    "mtd_run_f32": (_i, [_vp, _vp, _i64, _vp, ctypes.POINTER(_i)]),
+    "mtd_solver_create": (_i, [ctypes.POINTER(_vp), _i64, _i64, _i]),
+    "mtd_solver_factor": (_i, [_vp, _vp, _i64, _d, _vp, ctypes.POINTER(_i)]),
+    "mtd_solver_solve": (_i, [_vp, _vp, _i64, _vp, _i64, _i64, _i, _d, _i, _vp, ctypes.POINTER(SolveStats)]),
+    "mtd_solver_destroy": (_i, [_vp]),
     "mtd_graph_create": (_i, [ctypes.POINTER(_vp), _i, _i64, _i64]),
     "mtd_graph_add_task": (_i, [_vp, _i, _i, _i, ctypes.POINTER(_i), _i]),
     "mtd_graph_build_tiled": (_i, [_vp]),

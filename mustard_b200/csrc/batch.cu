@@ -1,0 +1,671 @@
+// Batched factorisations and solves: many independent SPD matrices of different sizes
+// run as ONE merged task graph on the persistent scheduler (one launch: graph-capturable),
+// then solved with per-matrix triangular solves, in FP64 or in low precision with FP64
+// iterative refinement.  No counterpart in the reference.
+//
+// Each matrix gets the reference's tiled Cholesky DAG for its own tile edge (chosen per
+// size by the caller or by mtd_batch_autotune), lowered with nested diagonal
+// factorisations, and the DAGs are concatenated with every task tagged by its matrix.  A
+// bad pivot records LAPACK-style info for that matrix only; the rest of the batch runs on.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/mustard_b200.h"
+#include "dag.hpp"
+#include "device_types.hpp"
+
+namespace mtd {
+int launch_run(const RunArgs &a, const int *deps_init, const int *roots, int n_roots, long long total_items,
+               int prec, bool vec2, int grid, cudaStream_t s);
+}
+using namespace mtd;
+
+namespace {
+
+constexpr int kSB = 64;        // solve block (= inverse block edge)
+constexpr int kMaxRhs = 16;
+constexpr int kBT = 256;       // threads of the batched solve kernels
+constexpr int kInfoOk = 0x7f7f7f7f;  // per-matrix info sentinel (bytes 0x7f): no bad pivot
+
+// Per-matrix arguments of the solve kernels.
+struct SolveMat {
+    const double *a;  // FP64 matrix (lower triangle read), for residuals
+    int64_t lda;
+    const void *f;    // factor (element type of the batch)
+    int64_t ldf;
+    int64_t ws_off, ws_ld;
+    const double *b;
+    int64_t ldb;
+    double *x;
+    int64_t ldx;
+    double *r;        // residual scratch, n x nrhs (ld n)
+    void *d;          // low-precision correction scratch, n x nrhs (ld n)
+    double *rowsum;   // n scratch for ||A||_inf
+    int n, nrhs;
+};
+
+// Forward then backward substitution with L and the inverses of its 64 x 64 diagonal
+// blocks, on the n x nrhs block Y (ld ldy), one CTA per matrix.
+enum { kOnX = 0, kOnD = 1, kOnR = 2 };  // which block of SolveMat the solve overwrites
+
+template <typename T>
+__global__ void __launch_bounds__(kBT) batch_trsv_kernel(const SolveMat *mats, const T *ws, int target) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *Ls = reinterpret_cast<T *>(smem_raw);  // [kSB][kSB + 1]
+    T *Ys = Ls + kSB * (kSB + 1);             // [kMaxRhs][kSB]
+    T *Acc = Ys + kMaxRhs * kSB;              // [kMaxRhs][kSB]
+    const SolveMat &sm = mats[blockIdx.x];
+    const int n = sm.n, nrhs = sm.nrhs, tid = threadIdx.x;
+    const T *L = static_cast<const T *>(sm.f);
+    const int64_t ldl = sm.ldf;
+    const T *W = ws + sm.ws_off;
+    const int64_t ldw = sm.ws_ld;
+    T *Y = target == kOnX ? reinterpret_cast<T *>(sm.x)
+                          : (target == kOnR ? reinterpret_cast<T *>(sm.r) : static_cast<T *>(sm.d));
+    const int64_t ldy = target == kOnX ? sm.ldx : n;
+    const int nb = (n + kSB - 1) / kSB;
+    for (int pass = 0; pass < 2; ++pass) {
+        const bool back = pass == 1;
+        for (int s = 0; s < nb; ++s) {
+            const int j = back ? nb - 1 - s : s;
+            const int rj = min(kSB, n - j * kSB);
+            __syncthreads();
+            for (int e = tid; e < kSB * nrhs; e += kBT) {
+                const int r = e % kSB, c = e / kSB;
+                Acc[c * kSB + r] = r < rj ? Y[(int64_t(j) * kSB + r) + c * ldy] : T(0);
+            }
+            for (int t = 0; t < s; ++t) {
+                const int k = back ? nb - 1 - t : t;
+                const int rk = min(kSB, n - k * kSB);
+                __syncthreads();
+                for (int e = tid; e < kSB * kSB; e += kBT) {
+                    const int a = e % kSB, c = e / kSB;
+                    if (!back) Ls[a * (kSB + 1) + c] = (a < rj && c < rk) ? L[(int64_t(j) * kSB + a) + (int64_t(k) * kSB + c) * ldl] : T(0);
+                    else Ls[c * (kSB + 1) + a] = (a < rk && c < rj) ? L[(int64_t(k) * kSB + a) + (int64_t(j) * kSB + c) * ldl] : T(0);
+                }
+                for (int e = tid; e < kSB * nrhs; e += kBT) {
+                    const int r = e % kSB, c = e / kSB;
+                    Ys[c * kSB + r] = r < rk ? Y[(int64_t(k) * kSB + r) + c * ldy] : T(0);
+                }
+                __syncthreads();
+                for (int o = tid; o < kSB * nrhs; o += kBT) {
+                    const int r = o % kSB, c = o / kSB;
+                    T acc = T(0);
+#pragma unroll 8
+                    for (int q = 0; q < kSB; ++q) acc += Ls[r * (kSB + 1) + q] * Ys[c * kSB + q];
+                    Acc[c * kSB + r] -= acc;
+                }
+            }
+            __syncthreads();
+            for (int e = tid; e < kSB * kSB; e += kBT) {
+                const int a = e % kSB, c = e / kSB;
+                const T v = (a < rj && c < rj) ? W[(int64_t(j) * kSB + a) + int64_t(c) * ldw] : T(0);
+                if (!back) Ls[a * (kSB + 1) + c] = v;
+                else Ls[c * (kSB + 1) + a] = v;
+            }
+            __syncthreads();
+            for (int o = tid; o < kSB * nrhs; o += kBT) {
+                const int r = o % kSB, c = o / kSB;
+                T acc = T(0);
+#pragma unroll 8
+                for (int q = 0; q < kSB; ++q) acc += Ls[r * (kSB + 1) + q] * Acc[c * kSB + q];
+                if (r < rj) Y[(int64_t(j) * kSB + r) + c * ldy] = acc;
+            }
+        }
+    }
+}
+
+// r = b - A_sym x, then the matrix's normwise backward error (max over its columns) into
+// berr[m]; one CTA per matrix.  A's infinity norm comes from anorm[m] (computed by
+// batch_anorm_kernel).
+__global__ void __launch_bounds__(kBT) batch_residual_kernel(const SolveMat *mats, const double *anorm, double *berr) {
+    __shared__ double As[kSB][kSB + 1];
+    __shared__ double red[3][kMaxRhs][kBT / 32];
+    const SolveMat &sm = mats[blockIdx.x];
+    const int n = sm.n, nrhs = sm.nrhs, tid = threadIdx.x;
+    for (int64_t e = tid; e < int64_t(n) * nrhs; e += kBT) {
+        const int64_t i = e % n, c = e / n;
+        sm.r[i + c * n] = sm.b[i + c * sm.ldb];
+    }
+    const int nb = (n + kSB - 1) / kSB;
+    for (int I = 0; I < nb; ++I) {
+        for (int J = 0; J <= I; ++J) {
+            const int ri = min(kSB, n - I * kSB), cj = min(kSB, n - J * kSB);
+            __syncthreads();
+            for (int e = tid; e < kSB * kSB; e += kBT) {
+                const int r = e % kSB, c = e / kSB;
+                double v = 0.0;
+                if (r < ri && c < cj) {
+                    if (I != J || r >= c) v = sm.a[(int64_t(I) * kSB + r) + (int64_t(J) * kSB + c) * sm.lda];
+                    else v = sm.a[(int64_t(J) * kSB + c) + (int64_t(I) * kSB + r) * sm.lda];
+                }
+                As[r][c] = v;
+            }
+            __syncthreads();
+            for (int o = tid; o < kSB * nrhs; o += kBT) {
+                const int r = o % kSB, c = o / kSB;
+                if (r < ri) {
+                    double s = 0.0;
+                    for (int k = 0; k < cj; ++k) s += As[r][k] * sm.x[(int64_t(J) * kSB + k) + c * sm.ldx];
+                    sm.r[(int64_t(I) * kSB + r) + int64_t(c) * n] -= s;
+                }
+            }
+            __syncthreads();
+            if (I != J) {
+                for (int o = tid; o < kSB * nrhs; o += kBT) {
+                    const int r = o % kSB, c = o / kSB;
+                    if (r < cj) {
+                        double s = 0.0;
+                        for (int k = 0; k < ri; ++k) s += As[k][r] * sm.x[(int64_t(I) * kSB + k) + c * sm.ldx];
+                        sm.r[(int64_t(J) * kSB + r) + int64_t(c) * n] -= s;
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // column maxima of |r|, |x|, |b|
+    for (int c = 0; c < nrhs; ++c) {
+        double mr = 0.0, mx = 0.0, mb = 0.0;
+        for (int i = tid; i < n; i += kBT) {
+            mr = fmax(mr, fabs(sm.r[i + int64_t(c) * n]));
+            mx = fmax(mx, fabs(sm.x[i + int64_t(c) * sm.ldx]));
+            mb = fmax(mb, fabs(sm.b[i + int64_t(c) * sm.ldb]));
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+        }
+        if ((tid & 31) == 0) {
+            red[0][c][tid >> 5] = mr;
+            red[1][c][tid >> 5] = mx;
+            red[2][c][tid >> 5] = mb;
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double worst = 0.0;
+        for (int c = 0; c < nrhs; ++c) {
+            double mr = 0.0, mx = 0.0, mb = 0.0;
+            for (int w = 0; w < kBT / 32; ++w) {
+                mr = fmax(mr, red[0][c][w]);
+                mx = fmax(mx, red[1][c][w]);
+                mb = fmax(mb, red[2][c][w]);
+            }
+            const double den = anorm[blockIdx.x] * mx + mb;
+            worst = fmax(worst, den > 0 ? mr / den : mr);
+        }
+        berr[blockIdx.x] = worst;
+    }
+}
+
+// ||A_sym||_inf per matrix (max row sum of |A| over the full symmetric matrix).
+__global__ void __launch_bounds__(kBT) batch_anorm_kernel(const SolveMat *mats, double *anorm) {
+    __shared__ double red[kBT / 32];
+    const SolveMat &sm = mats[blockIdx.x];
+    const int n = sm.n, tid = threadIdx.x;
+    double best = 0.0;
+    for (int i = tid; i < n; i += kBT) {
+        double s = 0.0;
+        for (int j = 0; j <= i; ++j) s += fabs(sm.a[i + int64_t(j) * sm.lda]);  // row i, lower part
+        for (int j = i + 1; j < n; ++j) s += fabs(sm.a[j + int64_t(i) * sm.lda]);  // column i below
+        best = fmax(best, s);
+    }
+    for (int o = 16; o > 0; o >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if ((tid & 31) == 0) red[tid >> 5] = best;
+    __syncthreads();
+    if (tid == 0) {
+        double m = 0.0;
+        for (int w = 0; w < kBT / 32; ++w) m = fmax(m, red[w]);
+        anorm[blockIdx.x] = m;
+    }
+}
+
+// d = r / max|r| per column (rounded to T), or x += max|r| * d; one CTA per matrix.
+template <typename T>
+__global__ void __launch_bounds__(kBT) batch_scale_kernel(const SolveMat *mats, double *colscale, bool to_low) {
+    __shared__ double red[kBT / 32];
+    const SolveMat &sm = mats[blockIdx.x];
+    const int n = sm.n, tid = threadIdx.x;
+    double *scale = colscale + int64_t(blockIdx.x) * kMaxRhs;
+    T *d = static_cast<T *>(sm.d);
+    for (int c = 0; c < sm.nrhs; ++c) {
+        if (to_low) {
+            double m = 0.0;
+            for (int i = tid; i < n; i += kBT) m = fmax(m, fabs(sm.r[i + int64_t(c) * n]));
+            for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+            __syncthreads();
+            if ((tid & 31) == 0) red[tid >> 5] = m;
+            __syncthreads();
+            double s = 0.0;
+            for (int w = 0; w < kBT / 32; ++w) s = fmax(s, red[w]);
+            if (s == 0.0) s = 1.0;
+            if (tid == 0) scale[c] = s;
+            for (int i = tid; i < n; i += kBT) d[i + int64_t(c) * n] = static_cast<T>(sm.r[i + int64_t(c) * n] / s);
+        } else {
+            const double s = scale[c];
+            for (int i = tid; i < n; i += kBT) sm.x[i + int64_t(c) * sm.ldx] += s * static_cast<double>(d[i + int64_t(c) * n]);
+        }
+    }
+}
+
+// x += r (FP64 correction), one CTA per matrix.
+__global__ void batch_add_kernel(const SolveMat *mats) {
+    const SolveMat &sm = mats[blockIdx.x];
+    for (int64_t e = threadIdx.x; e < int64_t(sm.n) * sm.nrhs; e += blockDim.x) {
+        const int64_t i = e % sm.n, c = e / sm.n;
+        sm.x[i + c * sm.ldx] += sm.r[i + c * sm.n];
+    }
+}
+
+// X = B (columns), one CTA per matrix.
+__global__ void batch_copy_rhs_kernel(const SolveMat *mats, bool zero) {
+    const SolveMat &sm = mats[blockIdx.x];
+    for (int64_t e = threadIdx.x; e < int64_t(sm.n) * sm.nrhs; e += blockDim.x) {
+        const int64_t i = e % sm.n, c = e / sm.n;
+        sm.x[i + c * sm.ldx] = zero ? 0.0 : sm.b[i + c * sm.ldb];
+    }
+}
+
+// dst = lower triangle of src (+ shift on the diagonal), as float; grid (chunks, count).
+__global__ void batch_convert_kernel(const SolveMat *mats, double shift) {
+    const SolveMat &sm = mats[blockIdx.y];
+    const int64_t n = sm.n, total = n * n;
+    float *f = static_cast<float *>(const_cast<void *>(sm.f));
+    for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t i = e % n, j = e / n;
+        if (i < j) continue;
+        double v = sm.a[i + j * sm.lda];
+        if (i == j) v += shift;
+        f[i + j * sm.ldf] = static_cast<float>(v);
+    }
+}
+
+template <typename T>
+int dalloc(T **p, size_t count) {
+    if (cudaMalloc(reinterpret_cast<void **>(p), std::max<size_t>(count, 1) * sizeof(T)) != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return MTD_ERR_OUT_OF_MEMORY;
+    }
+    return MTD_OK;
+}
+
+}  // namespace
+
+struct mtd_batch {
+    int count = 0;
+    int prec = MTD_PREC_FP64;
+    int sms = 148;
+    std::vector<int64_t> n, tile, ws_off, ws_ld, rhs_off;
+    std::vector<int> nest;
+    int n_dev = 0, n_roots = 0;
+    long long total_items = 0;
+    long long qcap[kNumQueues] = {0, 0};
+    DevTask *d_tasks = nullptr;
+    int *d_succ = nullptr, *d_deps_init = nullptr, *d_deps = nullptr, *d_items_left = nullptr, *d_roots = nullptr;
+    unsigned long long *d_queue[kNumQueues] = {nullptr, nullptr};
+    QueueCtl *d_qctl = nullptr;
+    RunCtl *d_ctl = nullptr;
+    RunCtl *h_ctl = nullptr;       // pinned
+    unsigned char *d_ws = nullptr;
+    BatchMat *d_mats = nullptr;
+    BatchMat *h_mats = nullptr;    // pinned staging of the per-run table
+    int *d_info = nullptr;
+    unsigned long long *d_done = nullptr;
+    cudaStream_t last_stream = nullptr;
+    bool pending = false;
+    // solve state
+    SolveMat *d_solve = nullptr, *h_solve = nullptr;  // pinned staging
+    double *d_r = nullptr, *d_rowsum = nullptr, *d_anorm = nullptr, *d_berr = nullptr, *d_scale = nullptr;
+    double *h_berr = nullptr;      // pinned
+    void *d_low = nullptr;
+    int64_t rhs_total = 0;
+};
+
+namespace {
+
+size_t batch_elem(const mtd_batch *b) { return b->prec == MTD_PREC_FP64 ? sizeof(double) : sizeof(float); }
+
+void release(mtd_batch *b) {
+    cudaFree(b->d_tasks);
+    cudaFree(b->d_succ);
+    cudaFree(b->d_deps_init);
+    cudaFree(b->d_deps);
+    cudaFree(b->d_items_left);
+    cudaFree(b->d_roots);
+    for (int q = 0; q < kNumQueues; ++q) cudaFree(b->d_queue[q]);
+    cudaFree(b->d_qctl);
+    cudaFree(b->d_ctl);
+    if (b->h_ctl) cudaFreeHost(b->h_ctl);
+    cudaFree(b->d_ws);
+    cudaFree(b->d_mats);
+    if (b->h_mats) cudaFreeHost(b->h_mats);
+    cudaFree(b->d_info);
+    cudaFree(b->d_done);
+    cudaFree(b->d_solve);
+    if (b->h_solve) cudaFreeHost(b->h_solve);
+    cudaFree(b->d_r);
+    cudaFree(b->d_rowsum);
+    cudaFree(b->d_anorm);
+    cudaFree(b->d_berr);
+    cudaFree(b->d_scale);
+    if (b->h_berr) cudaFreeHost(b->h_berr);
+    cudaFree(b->d_low);
+}
+
+// Default tile for a size when the caller gives none: one tile up to 512 (its diagonal
+// factorisation nested at 128), 512-wide tiles above.
+int64_t default_tile(int64_t n) { return n <= 512 ? n : 512; }
+
+}  // namespace
+
+extern "C" {
+
+int mtd_batch_create(mtd_batch **out, int count, const int64_t *n, const int64_t *tile, const int *nest, int prec) {
+    if (!out) return MTD_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (count <= 0 || !n || (prec != MTD_PREC_FP64 && prec != MTD_PREC_TF32 && prec != MTD_PREC_FP32))
+        return MTD_ERR_INVALID_ARG;
+    mtd_batch *b = new (std::nothrow) mtd_batch();
+    if (!b) return MTD_ERR_OUT_OF_MEMORY;
+    b->count = count;
+    b->prec = prec;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (major != 10) {
+        delete b;
+        return MTD_ERR_NO_DEVICE;
+    }
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
+
+    std::vector<DevTask> tasks;
+    std::vector<int> succ, deps_init, roots;
+    int64_t ws_total = 0, rhs_total = 0;
+    int rc = MTD_OK;
+    for (int m = 0; m < count && !rc; ++m) {
+        const int64_t nm = n[m];
+        const int64_t tm = tile ? tile[m] : default_tile(nm);
+        const int km = nest ? nest[m] : (nm > kNestTile ? kNestTile : 0);
+        if (nm <= 0 || nm > (int64_t(1) << 20) || tm <= 0 || tm > nm || (tm != nm && tm % kSB != 0) || km < 0 ||
+            km % kSB != 0) {
+            rc = MTD_ERR_INVALID_ARG;
+            break;
+        }
+        b->n.push_back(nm);
+        b->tile.push_back(tm);
+        b->nest.push_back(km);
+        Dag dag(MTD_KIND_CHOLESKY, nm, tm);
+        rc = dag.build_reference_order();
+        Lowered low;
+        if (!rc) rc = dag.lower(km, low);
+        if (rc) break;
+        const int base = static_cast<int>(tasks.size());
+        const int sbase = static_cast<int>(succ.size());
+        for (size_t t = 0; t < low.tasks.size(); ++t) {
+            DevTask d = low.tasks[t];
+            d.mat = m;
+            d.succ_begin += sbase;
+            tasks.push_back(d);
+            deps_init.push_back(static_cast<int>(low.preds[t].size()));
+            if (low.preds[t].empty()) roots.push_back(base + static_cast<int>(t));
+        }
+        for (int s : low.succ) succ.push_back(s + base);
+        for (int q = 0; q < kNumQueues; ++q) b->qcap[q] += low.queue_cap[q];
+        const int64_t wld = (nm + 3) & ~int64_t(3);
+        b->ws_off.push_back(ws_total);
+        b->ws_ld.push_back(wld);
+        ws_total += wld * kSB;
+        b->rhs_off.push_back(rhs_total);
+        rhs_total += nm * kMaxRhs;
+    }
+    if (!rc && roots.empty()) rc = MTD_ERR_BAD_DAG;
+    b->n_dev = static_cast<int>(tasks.size());
+    b->n_roots = static_cast<int>(roots.size());
+    b->total_items = b->qcap[0] + b->qcap[1];
+    b->rhs_total = rhs_total;
+    const int nt = b->n_dev;
+    if (!rc) rc = dalloc(&b->d_tasks, nt);
+    if (!rc) rc = dalloc(&b->d_succ, succ.size());
+    if (!rc) rc = dalloc(&b->d_deps_init, nt);
+    if (!rc) rc = dalloc(&b->d_deps, nt);
+    if (!rc) rc = dalloc(&b->d_items_left, nt);
+    if (!rc) rc = dalloc(&b->d_roots, roots.size());
+    for (int q = 0; q < kNumQueues && !rc; ++q) rc = dalloc(&b->d_queue[q], size_t(b->qcap[q]));
+    if (!rc) rc = dalloc(&b->d_qctl, kNumQueues);
+    if (!rc) rc = dalloc(&b->d_ctl, 1);
+    if (!rc) rc = dalloc(&b->d_ws, size_t(ws_total) * batch_elem(b));
+    if (!rc) rc = dalloc(&b->d_mats, count);
+    if (!rc) rc = dalloc(&b->d_info, count);
+    if (!rc) rc = dalloc(&b->d_done, count);
+    if (!rc && cudaMallocHost(reinterpret_cast<void **>(&b->h_ctl), sizeof(RunCtl)) != cudaSuccess) rc = MTD_ERR_OUT_OF_MEMORY;
+    if (!rc && cudaMallocHost(reinterpret_cast<void **>(&b->h_mats), count * sizeof(BatchMat)) != cudaSuccess)
+        rc = MTD_ERR_OUT_OF_MEMORY;
+    if (!rc) {
+        bool ok = cudaMemcpy(b->d_tasks, tasks.data(), nt * sizeof(DevTask), cudaMemcpyHostToDevice) == cudaSuccess;
+        ok = ok && (succ.empty() ||
+                    cudaMemcpy(b->d_succ, succ.data(), succ.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess);
+        ok = ok && cudaMemcpy(b->d_deps_init, deps_init.data(), nt * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
+        ok = ok && cudaMemcpy(b->d_roots, roots.data(), roots.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
+        ok = ok && cudaMemset(b->d_ctl, 0, sizeof(RunCtl)) == cudaSuccess;
+        if (!ok) rc = MTD_ERR_CUDA;
+    }
+    if (rc) {
+        release(b);
+        delete b;
+        return rc;
+    }
+    std::memset(b->h_ctl, 0, sizeof(RunCtl));
+    *out = b;
+    return MTD_OK;
+}
+
+int mtd_batch_num_tasks(const mtd_batch *b) { return b ? b->n_dev : -MTD_ERR_INVALID_ARG; }
+
+int mtd_batch_factor(mtd_batch *b, void *const *dA, const int64_t *lda, void *stream) {
+    if (!b || !dA || !lda) return MTD_ERR_INVALID_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int64_t epc = 16 / static_cast<int64_t>(batch_elem(b));
+    bool vec2 = true;
+    for (int m = 0; m < b->count; ++m) {
+        if (!dA[m] || lda[m] < b->n[m]) return MTD_ERR_INVALID_ARG;
+        b->h_mats[m] = BatchMat{dA[m], lda[m], b->ws_off[m], b->ws_ld[m]};
+        vec2 = vec2 && reinterpret_cast<uintptr_t>(dA[m]) % 16 == 0 && lda[m] % epc == 0 && b->n[m] % epc == 0 &&
+               b->tile[m] % epc == 0;
+    }
+    if (cudaMemcpyAsync(b->d_mats, b->h_mats, b->count * sizeof(BatchMat), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemsetAsync(b->d_info, 0x7f, b->count * sizeof(int), s) != cudaSuccess ||
+        cudaMemsetAsync(b->d_done, 0, b->count * sizeof(unsigned long long), s) != cudaSuccess)
+        return MTD_ERR_CUDA;
+    RunArgs a{};
+    a.n_tasks = b->n_dev;
+    a.tasks = b->d_tasks;
+    a.succ = b->d_succ;
+    a.deps = b->d_deps;
+    a.items_left = b->d_items_left;
+    for (int q = 0; q < kNumQueues; ++q) {
+        a.queue[q] = b->d_queue[q];
+        a.queue_cap[q] = b->qcap[q];
+    }
+    a.qctl = b->d_qctl;
+    a.ctl = b->d_ctl;
+    a.ws_lower = b->d_ws;
+    a.ws_upper = nullptr;
+    a.timeout_ns = 10ull * 1000000000ull;
+    a.mats = b->d_mats;
+    a.mat_info = b->d_info;
+    a.mat_done_ns = b->d_done;
+    int rc = launch_run(a, b->d_deps_init, b->d_roots, b->n_roots, b->total_items, b->prec, vec2, b->sms, s);
+    if (rc) return rc;
+    if (cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, s) != cudaSuccess) return MTD_ERR_CUDA;
+    b->last_stream = s;
+    b->pending = true;
+    return MTD_OK;
+}
+
+int mtd_batch_status(mtd_batch *b, int *info, double *latency_ms) {
+    if (!b) return MTD_ERR_INVALID_ARG;
+    if (!b->pending) return MTD_ERR_STATE;
+    if (cudaStreamSynchronize(b->last_stream) != cudaSuccess) return MTD_ERR_CUDA;
+    if (info) {
+        if (cudaMemcpy(info, b->d_info, b->count * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return MTD_ERR_CUDA;
+        for (int m = 0; m < b->count; ++m)
+            if (info[m] == kInfoOk) info[m] = 0;
+    }
+    if (latency_ms) {
+        std::vector<unsigned long long> done(b->count);
+        if (cudaMemcpy(done.data(), b->d_done, b->count * sizeof(unsigned long long), cudaMemcpyDeviceToHost) !=
+            cudaSuccess)
+            return MTD_ERR_CUDA;
+        for (int m = 0; m < b->count; ++m)
+            latency_ms[m] = done[m] > b->h_ctl->start_ns ? double(done[m] - b->h_ctl->start_ns) * 1e-6 : -1.0;
+    }
+    if (b->h_ctl->error) return b->h_ctl->error;
+    if (b->h_ctl->tasks_done != b->n_dev) return MTD_ERR_TIMEOUT;
+    return MTD_OK;
+}
+
+int mtd_batch_solve(mtd_batch *b, const double *const *dA, const int64_t *lda, void *const *dF, const int64_t *ldf,
+                    const double *const *dB, const int64_t *ldb, double *const *dX, const int64_t *ldx,
+                    const int *nrhs, int method, double tol, int max_iter, void *stream, mtd_batch_solve_stats *stats) {
+    if (!b || !dF || !ldf || !dB || !ldb || !dX || !ldx || !nrhs || max_iter < 0) return MTD_ERR_INVALID_ARG;
+    if (method != MTD_REFINE_NONE && method != MTD_REFINE_IR) return MTD_ERR_INVALID_ARG;
+    const bool low = b->prec != MTD_PREC_FP64;
+    if ((method == MTD_REFINE_IR || low) && (!dA || !lda)) return MTD_ERR_INVALID_ARG;
+    if (low && method == MTD_REFINE_NONE) return MTD_ERR_INVALID_ARG;  // a low-precision factor needs refinement
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int count = b->count;
+    int rc = MTD_OK;
+    if (!b->h_berr) {
+        if (!b->h_solve && cudaMallocHost(reinterpret_cast<void **>(&b->h_solve), count * sizeof(SolveMat)) != cudaSuccess)
+            return MTD_ERR_OUT_OF_MEMORY;
+        if (cudaMallocHost(reinterpret_cast<void **>(&b->h_berr), count * sizeof(double)) != cudaSuccess)
+            return MTD_ERR_OUT_OF_MEMORY;
+        if (!b->d_solve) rc = dalloc(&b->d_solve, count);
+        if (!rc) rc = dalloc(&b->d_r, size_t(b->rhs_total));
+        if (!rc) rc = dalloc(&b->d_anorm, count);
+        if (!rc) rc = dalloc(&b->d_berr, count);
+        if (!rc) rc = dalloc(&b->d_scale, size_t(count) * kMaxRhs);
+        if (!rc && cudaMalloc(&b->d_low, size_t(b->rhs_total) * sizeof(float)) != cudaSuccess) rc = MTD_ERR_OUT_OF_MEMORY;
+        if (rc) return rc;
+    }
+    for (int m = 0; m < count; ++m) {
+        if (nrhs[m] < 1 || nrhs[m] > kMaxRhs || ldb[m] < b->n[m] || ldx[m] < b->n[m] || ldf[m] < b->n[m])
+            return MTD_ERR_INVALID_ARG;
+        if (dA && lda[m] < b->n[m]) return MTD_ERR_INVALID_ARG;
+        SolveMat &sm = b->h_solve[m];
+        sm.a = dA ? dA[m] : nullptr;
+        sm.lda = dA ? lda[m] : 0;
+        sm.f = dF[m];
+        sm.ldf = ldf[m];
+        sm.ws_off = b->ws_off[m];
+        sm.ws_ld = b->ws_ld[m];
+        sm.b = dB[m];
+        sm.ldb = ldb[m];
+        sm.x = dX[m];
+        sm.ldx = ldx[m];
+        sm.r = b->d_r + b->rhs_off[m];
+        sm.d = static_cast<float *>(b->d_low) + b->rhs_off[m];
+        sm.rowsum = nullptr;
+        sm.n = static_cast<int>(b->n[m]);
+        sm.nrhs = nrhs[m];
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    if (cudaMemcpyAsync(b->d_solve, b->h_solve, count * sizeof(SolveMat), cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return MTD_ERR_CUDA;
+    const size_t smem64 = (kSB * (kSB + 1) + 2 * kMaxRhs * kSB) * sizeof(double);
+    const size_t smem32 = (kSB * (kSB + 1) + 2 * kMaxRhs * kSB) * sizeof(float);
+    cudaFuncSetAttribute(batch_trsv_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem64));
+    const double *ws64 = reinterpret_cast<const double *>(b->d_ws);
+    const float *ws32 = reinterpret_cast<const float *>(b->d_ws);
+    mtd_batch_solve_stats st{};
+    double worst = -1.0;
+    if (!low) {  // one FP64 solve: x = (L L^T)^-1 b
+        batch_copy_rhs_kernel<<<count, kBT, 0, s>>>(b->d_solve, false);
+        batch_trsv_kernel<double><<<count, kBT, smem64, s>>>(b->d_solve, ws64, kOnX);
+        st.iterations = 1;
+    } else {
+        batch_copy_rhs_kernel<<<count, kBT, 0, s>>>(b->d_solve, true);  // x = 0
+    }
+    if (dA) {
+        batch_anorm_kernel<<<count, kBT, 0, s>>>(b->d_solve, b->d_anorm);
+        for (int it = 0;; ++it) {
+            batch_residual_kernel<<<count, kBT, 0, s>>>(b->d_solve, b->d_anorm, b->d_berr);
+            if (cudaMemcpyAsync(b->h_berr, b->d_berr, count * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess)
+                return MTD_ERR_CUDA;
+            worst = 0.0;
+            int done = 0;
+            for (int m = 0; m < count; ++m) {
+                worst = std::max(worst, b->h_berr[m]);
+                done += b->h_berr[m] <= tol;
+            }
+            st.converged_count = done;
+            if (method == MTD_REFINE_NONE) break;
+            if ((it > 0 || !low) && done == count) break;
+            if (it >= max_iter) break;
+            if (low) {  // x += M^-1 r through the low-precision factor
+                batch_scale_kernel<float><<<count, kBT, 0, s>>>(b->d_solve, b->d_scale, true);
+                batch_trsv_kernel<float><<<count, kBT, smem32, s>>>(b->d_solve, ws32, kOnD);
+                batch_scale_kernel<float><<<count, kBT, 0, s>>>(b->d_solve, b->d_scale, false);
+            } else {    // x += (L L^T)^-1 r in FP64
+                batch_trsv_kernel<double><<<count, kBT, smem64, s>>>(b->d_solve, ws64, kOnR);
+                batch_add_kernel<<<count, kBT, 0, s>>>(b->d_solve);
+            }
+            st.iterations = it + 1;
+        }
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) return MTD_ERR_CUDA;
+    st.max_backward_error = worst;
+    st.solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (stats) *stats = st;
+    return rc;
+}
+
+int mtd_batch_convert(mtd_batch *b, const double *const *dA, const int64_t *lda, void *const *dF, const int64_t *ldf,
+                      double shift, void *stream) {
+    if (!b || !dA || !lda || !dF || !ldf || b->prec == MTD_PREC_FP64) return MTD_ERR_INVALID_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!b->h_solve) {
+        if (cudaMallocHost(reinterpret_cast<void **>(&b->h_solve), b->count * sizeof(SolveMat)) != cudaSuccess)
+            return MTD_ERR_OUT_OF_MEMORY;
+        if (dalloc(&b->d_solve, b->count)) return MTD_ERR_OUT_OF_MEMORY;
+    }
+    for (int m = 0; m < b->count; ++m) {
+        if (lda[m] < b->n[m] || ldf[m] < b->n[m]) return MTD_ERR_INVALID_ARG;
+        SolveMat sm{};
+        sm.a = dA[m];
+        sm.lda = lda[m];
+        sm.f = dF[m];
+        sm.ldf = ldf[m];
+        sm.n = static_cast<int>(b->n[m]);
+        b->h_solve[m] = sm;
+    }
+    if (cudaMemcpyAsync(b->d_solve, b->h_solve, b->count * sizeof(SolveMat), cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return MTD_ERR_CUDA;
+    batch_convert_kernel<<<dim3(16, b->count), 256, 0, s>>>(b->d_solve, shift);
+    // the staging buffer is reused by the next call: wait until the copy has been consumed
+    if (cudaStreamSynchronize(s) != cudaSuccess) return MTD_ERR_CUDA;
+    return cudaGetLastError() == cudaSuccess ? MTD_OK : MTD_ERR_CUDA;
+}
+
+int mtd_batch_destroy(mtd_batch *b) {
+    if (!b) return MTD_ERR_INVALID_ARG;
+    if (b->pending && b->last_stream) cudaStreamSynchronize(b->last_stream);
+    cudaDeviceSynchronize();
+    release(b);
+    delete b;
+    return MTD_OK;
+}
+
+}  // extern "C"

@@ -40,9 +40,18 @@ struct alignas(16) DevTask {
     int32_t m, n, k;     // extents
     int32_t succ_begin;  // successors are succ[succ_begin, succ_begin + succ_count)
     int32_t succ_count;
-    int32_t pad[2];
+    int32_t mat;         // matrix of a batched run (index into RunArgs::mats), else 0
+    int32_t pad;
 };
 static_assert(sizeof(DevTask) == 64, "DevTask is read as four 16-byte words");
+
+// One matrix of a batched run.
+struct BatchMat {
+    void *a;         // column-major matrix (element type of the run)
+    int64_t lda;
+    int64_t ws_off;  // this matrix's slice of the inverse workspaces (elements)
+    int64_t ws_ld;
+};
 
 // Device-resident control block of one graph (one cache line per hot counter).
 struct alignas(128) QueueCtl {
@@ -58,12 +67,13 @@ struct alignas(128) RunCtl {
     int info;       // LAPACK-style info (1-based global column), 0 if none
     int abort;      // set with error; every CTA polls it
     unsigned long long items_done;
-    char pad[104];
+    unsigned long long start_ns;  // earliest %globaltimer at which a CTA started popping
+    char pad[96];
 };
 
 // Everything the persistent kernel needs for one run (passed by value).
 struct RunArgs {
-    double *a;             // matrix, column-major
+    void *a;               // matrix, column-major (double, or float for the low-precision factor)
     int64_t lda;
     int n_tasks;           // device tasks (including joins)
     const DevTask *tasks;
@@ -74,12 +84,18 @@ struct RunArgs {
     long long queue_cap[kNumQueues];
     QueueCtl *qctl;        // kNumQueues entries
     RunCtl *ctl;
-    double *ws_lower;      // inverses of the diagonal blocks of L (ws_ld x kNB)
-    double *ws_upper;      // inverses of the diagonal blocks of U (LU only)
+    void *ws_lower;        // inverses of the diagonal blocks of L (ws_ld x kNB, matrix type)
+    void *ws_upper;        // inverses of the diagonal blocks of U (LU only)
     int64_t ws_ld;
     unsigned long long *trace;  // optional: 4 words per item (start, end, sm, task<<32|item)
     long long trace_cap;
     unsigned long long timeout_ns;
+    // Batched runs only (mats == nullptr otherwise): per-matrix geometry, per-matrix
+    // LAPACK-style info (INT_MAX = success), and the %globaltimer time at which each
+    // matrix's last task finished (for per-matrix latency).
+    const BatchMat *mats;
+    int *mat_info;
+    unsigned long long *mat_done_ns;
 };
 
 }  // namespace mtd

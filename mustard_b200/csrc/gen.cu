@@ -89,7 +89,7 @@ int mtd_generate(double *dA, int64_t n, int64_t lda, int which, uint64_t seed, d
         return MTD_ERR_OUT_OF_MEMORY;
     }
     uniform_kernel<<<4096, 256, 0, s>>>(b, n, n, seed, 0.0);
-    constexpr int smem = GemmMma<kBNContig, 2>::SMEM_DOUBLES * 8;
+    constexpr int smem = GemmMma<kBNContig, 2>::SMEM_BYTES;
     cudaFuncSetAttribute(spd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     const dim3 grid(static_cast<unsigned>((n + kGemmTile - 1) / kGemmTile),
                     static_cast<unsigned>((n + kGemmTile - 1) / kGemmTile));

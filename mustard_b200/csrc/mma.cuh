@@ -1,21 +1,30 @@
-// FP64 block-GEMM engine for one CTA of 256 threads on sm_100a.
+// Block-GEMM engine for one CTA on sm_100a, FP64 (DMMA) or FP32 storage with TF32 MMA.
 //
 // acc(BM x BN) += A(BM x K) * B(K x BN), operands read from global memory (L2) into a
 // multi-stage shared-memory ring with cp.async.cg (16-byte, L1-bypassing: tiles written
 // by other CTAs of the persistent kernel are never read from a stale L1 line), and
-// multiplied with the FP64 tensor-core instruction mma.sync.m16n8k8.f64.  sm_100a's
-// tcgen05 MMA has no FP64 kind, so DMMA is the FP64 tensor path on B200; a register-only
-// probe measures it at the same 37 TFLOP/s as the datasheet's FP64 figure.
+// multiplied on the tensor cores with warp-level MMA:
+//   T = double: mma.sync.m16n8k8.f64 (DMMA).  sm_100a's tcgen05 MMA has no FP64 kind, so
+//               DMMA is the FP64 tensor path on B200; a register-only probe measures it at
+//               the same 37 TFLOP/s as the datasheet's FP64 figure.
+//   T = float : mma.sync.m16n8k8.tf32 with FP32 accumulation (operands rounded to TF32
+//               with cvt.rna); used by the low-precision factorisation of the mixed-
+//               precision solver.
+// Both shapes share one fragment layout: A (g, t), (g+8, t), (g, t+4), (g+8, t+4);
+// B (k = t, n = g), (k = t+4, n = g); C (g, 2t), (g, 2t+1), (g+8, 2t), (g+8, 2t+1), with
+// g = lane / 4 and t = lane % 4.
 //
 // Layouts (column-major global memory):
 //   A(m, k) = A[m + k * lda]                                   ("m-contiguous")
 //   B(k, n) = B[n + k * ldb]   when BL == kBNContig            (Cholesky: B = L(i,k)^T)
 //   B(k, n) = B[k + n * ldb]   when BL == kBKContig            (LU:       B = U(k,j))
-// Shared-memory rows are padded to 4 (mod 16) doubles so every fragment load of a
-// half-warp touches 16 distinct 8-byte bank pairs.
+// Shared-memory rows are padded so every fragment load is bank-conflict-free: for 8-byte
+// elements a half-warp touches 16 distinct bank pairs (row pad = 4 mod 16), for 4-byte
+// elements a warp touches 32 distinct banks (row pad = 8 mod 32, 4 mod 32 for k-rows).
 //
-// VEC == 2: 16-byte copies; needs 16-byte aligned bases, even leading dimensions and
-// even extents (the host checks).  VEC == 1: 8-byte loads through registers, any shape.
+// VEC == 2: 16-byte copies; needs 16-byte aligned bases and leading dimensions and
+// extents that are multiples of 16 bytes' worth of elements (the host checks).
+// VEC == 1: element loads through registers, any shape.
 #pragma once
 
 #include <cstdint>
@@ -43,32 +52,108 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 __device__ __forceinline__ double ld_cg(const double *p) { return __ldcg(p); }
+__device__ __forceinline__ float ld_cg(const float *p) { return __ldcg(p); }
 
-__device__ __forceinline__ void dmma_16x8x8(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
+__device__ __forceinline__ void mma_16x8x8(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
     asm volatile(
         "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
         "{%0,%1,%2,%3};\n"
         : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
         : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
+__device__ __forceinline__ void dmma_16x8x8(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
+    mma_16x8x8(d, a, b);
+}
 
-template <int BM, int BN, int WARPS_M, int WARPS_N, int BL, int VEC, int STAGES = 3, int BK_ = 16>
-struct BlockMma {
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+    return r;
+}
+
+// TF32 product with FP32 accumulation.  The FP32 operand bits go to the tensor core as they
+// are: it reads the TF32 part (sign, exponent, top 10 mantissa bits), i.e. truncates.  A
+// cvt.rna per fragment element would round to nearest instead, but costs six instructions
+// per MMA and made the FP32-storage GEMM issue-bound at a third of the TF32 peak.
+__device__ __forceinline__ void mma_16x8x8(float (&d)[4], const float (&a)[4], const float (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(__float_as_uint(a[0])), "r"(__float_as_uint(a[1])), "r"(__float_as_uint(a[2])),
+          "r"(__float_as_uint(a[3])), "r"(__float_as_uint(b[0])), "r"(__float_as_uint(b[1])));
+}
+
+// FP32-accurate products from TF32 tensor cores: each operand is split into a TF32 head
+// (the top 19 bits, by masking) and the exact FP32 remainder (x = hi + lo), and
+// d += lo_a*hi_b + hi_a*lo_b + hi_a*hi_b (lo*lo is below FP32 roundoff; the remainders
+// enter the tensor core truncated to TF32, an error of ~2^-21 relative of a term that is
+// itself 2^-10 of the product).  Three MMAs per product; accuracy close to FP32.
+__device__ __forceinline__ void mma_16x8x8_x3(float (&d)[4], const float (&a)[4], const float (&b)[2]) {
+    uint32_t ah[4], al[4], bh[2], bl[2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        ah[i] = __float_as_uint(a[i]) & 0xffffe000u;
+        al[i] = __float_as_uint(a[i] - __uint_as_float(ah[i]));
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        bh[i] = __float_as_uint(b[i]) & 0xffffe000u;
+        bl[i] = __float_as_uint(b[i] - __uint_as_float(bh[i]));
+    }
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(al[0]), "r"(al[1]), "r"(al[2]), "r"(al[3]), "r"(bh[0]), "r"(bh[1]));
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(ah[0]), "r"(ah[1]), "r"(ah[2]), "r"(ah[3]), "r"(bl[0]), "r"(bl[1]));
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(ah[0]), "r"(ah[1]), "r"(ah[2]), "r"(ah[3]), "r"(bh[0]), "r"(bh[1]));
+}
+
+template <int SPLIT>
+__device__ __forceinline__ void mma_op(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
+    mma_16x8x8(d, a, b);
+}
+template <int SPLIT>
+__device__ __forceinline__ void mma_op(float (&d)[4], const float (&a)[4], const float (&b)[2]) {
+    if constexpr (SPLIT == 3) mma_16x8x8_x3(d, a, b);
+    else mma_16x8x8(d, a, b);
+}
+
+template <typename T>
+struct SmemPad {
+    static constexpr int a = sizeof(T) == 8 ? 4 : 8;  // rows of A and of n-contiguous B
+    static constexpr int bk = 4;                        // rows of k-contiguous B
+    static constexpr int a_mod = sizeof(T) == 8 ? 16 : 32;
+};
+
+template <typename T, int BM, int BN, int WARPS_M, int WARPS_N, int BL, int VEC, int STAGES = 3, int BK_ = 16,
+          int SPLIT = 1>
+struct BlockMmaT {
     static constexpr int BK = BK_;
+    static constexpr int EPC = 16 / int(sizeof(T));  // elements per 16-byte copy
     static constexpr int WM = BM / WARPS_M;
     static constexpr int WN = BN / WARPS_N;
     static constexpr int FM = WM / 16;
     static constexpr int FN = WN / 8;
-    static constexpr int LDA = BM + 4;
-    static constexpr int LDB = (BL == kBNContig) ? BN + 4 : BK + 4;
+    static constexpr int LDA = BM + SmemPad<T>::a;
+    static constexpr int LDB = (BL == kBNContig) ? BN + SmemPad<T>::a : BK + SmemPad<T>::bk;
     static constexpr int A_STAGE = BK * LDA;
     static constexpr int B_STAGE = (BL == kBNContig) ? BK * LDB : BN * LDB;
-    static constexpr int SMEM_DOUBLES = STAGES * (A_STAGE + B_STAGE);
+    static constexpr int SMEM_ELEMS = STAGES * (A_STAGE + B_STAGE);
+    static constexpr int SMEM_BYTES = SMEM_ELEMS * int(sizeof(T));
     static_assert(WARPS_M * WARPS_N * 32 == kThreads, "one warp tile per warp of the CTA");
     static_assert(FM >= 1 && FN >= 1 && WM % 16 == 0 && WN % 8 == 0, "warp tile");
-    static_assert(LDA % 16 == 4 && LDB % 16 == 4, "bank-conflict-free padding");
+    static_assert(LDA % SmemPad<T>::a_mod == SmemPad<T>::a, "bank-conflict-free padding (A)");
+    static_assert((LDA * int(sizeof(T))) % 16 == 0 && (LDB * int(sizeof(T))) % 16 == 0, "16-byte rows");
+    static_assert(BK % 8 == 0 && BM % EPC == 0 && BN % EPC == 0 && BK % EPC == 0, "copy granularity");
 
-    double acc[FM][FN][4];
+    T acc[FM][FN][4];
 
     __device__ __forceinline__ void zero() {
 #pragma unroll
@@ -76,22 +161,21 @@ struct BlockMma {
 #pragma unroll
             for (int j = 0; j < FN; ++j)
 #pragma unroll
-                for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
+                for (int v = 0; v < 4; ++v) acc[i][j][v] = T(0);
     }
 
     // ---- global -> shared stage loads ----
-    __device__ __forceinline__ static void load_a(double *As, const double *A, int64_t lda, int M, int K,
-                                                  int k0) {
+    __device__ __forceinline__ static void load_a(T *As, const T *A, int64_t lda, int M, int K, int k0) {
         const int tid = threadIdx.x;
         if (VEC == 2) {
-            constexpr int CH = BK * (BM / 2);
+            constexpr int CH = BK * (BM / EPC);
 #pragma unroll
             for (int c = tid; c < CH; c += kThreads) {
-                const int col = c / (BM / 2);
-                const int row = 2 * (c % (BM / 2));
+                const int col = c / (BM / EPC);
+                const int row = EPC * (c % (BM / EPC));
                 const int kk = k0 + col;
                 const bool ok = row < M && kk < K;
-                const double *src = ok ? A + row + int64_t(kk) * lda : A;
+                const T *src = ok ? A + row + int64_t(kk) * lda : A;
                 cp_async16(As + col * LDA + row, src, ok);
             }
         } else {
@@ -100,24 +184,23 @@ struct BlockMma {
                 const int col = e / BM;
                 const int row = e % BM;
                 const int kk = k0 + col;
-                As[col * LDA + row] = (row < M && kk < K) ? ld_cg(A + row + int64_t(kk) * lda) : 0.0;
+                As[col * LDA + row] = (row < M && kk < K) ? ld_cg(A + row + int64_t(kk) * lda) : T(0);
             }
         }
     }
 
-    __device__ __forceinline__ static void load_b(double *Bs, const double *B, int64_t ldb, int N, int K,
-                                                  int k0) {
+    __device__ __forceinline__ static void load_b(T *Bs, const T *B, int64_t ldb, int N, int K, int k0) {
         const int tid = threadIdx.x;
         if (BL == kBNContig) {
             if (VEC == 2) {
-                constexpr int CH = BK * (BN / 2);
+                constexpr int CH = BK * (BN / EPC);
 #pragma unroll
                 for (int c = tid; c < CH; c += kThreads) {
-                    const int col = c / (BN / 2);
-                    const int n = 2 * (c % (BN / 2));
+                    const int col = c / (BN / EPC);
+                    const int n = EPC * (c % (BN / EPC));
                     const int kk = k0 + col;
                     const bool ok = n < N && kk < K;
-                    const double *src = ok ? B + n + int64_t(kk) * ldb : B;
+                    const T *src = ok ? B + n + int64_t(kk) * ldb : B;
                     cp_async16(Bs + col * LDB + n, src, ok);
                 }
             } else {
@@ -126,19 +209,19 @@ struct BlockMma {
                     const int col = e / BN;
                     const int n = e % BN;
                     const int kk = k0 + col;
-                    Bs[col * LDB + n] = (n < N && kk < K) ? ld_cg(B + n + int64_t(kk) * ldb) : 0.0;
+                    Bs[col * LDB + n] = (n < N && kk < K) ? ld_cg(B + n + int64_t(kk) * ldb) : T(0);
                 }
             }
         } else {
             if (VEC == 2) {
-                constexpr int CH = BN * (BK / 2);
+                constexpr int CH = BN * (BK / EPC);
 #pragma unroll
                 for (int c = tid; c < CH; c += kThreads) {
-                    const int n = c / (BK / 2);
-                    const int k = 2 * (c % (BK / 2));
+                    const int n = c / (BK / EPC);
+                    const int k = EPC * (c % (BK / EPC));
                     const int kk = k0 + k;
                     const bool ok = n < N && kk < K;
-                    const double *src = ok ? B + kk + int64_t(n) * ldb : B;
+                    const T *src = ok ? B + kk + int64_t(n) * ldb : B;
                     cp_async16(Bs + n * LDB + k, src, ok);
                 }
             } else {
@@ -147,13 +230,13 @@ struct BlockMma {
                     const int n = e / BK;
                     const int k = e % BK;
                     const int kk = k0 + k;
-                    Bs[n * LDB + k] = (n < N && kk < K) ? ld_cg(B + kk + int64_t(n) * ldb) : 0.0;
+                    Bs[n * LDB + k] = (n < N && kk < K) ? ld_cg(B + kk + int64_t(n) * ldb) : T(0);
                 }
             }
         }
     }
 
-    __device__ __forceinline__ void compute_stage(const double *As, const double *Bs) {
+    __device__ __forceinline__ void compute_stage(const T *As, const T *Bs) {
         const int lane = threadIdx.x & 31;
         const int warp = threadIdx.x >> 5;
         const int wm0 = (warp / WARPS_N) * WM;
@@ -162,7 +245,7 @@ struct BlockMma {
         const int t = lane & 3;
 #pragma unroll
         for (int ks = 0; ks < BK; ks += 8) {
-            double bf[FN][2];
+            T bf[FN][2];
 #pragma unroll
             for (int j = 0; j < FN; ++j) {
                 const int n = wn0 + j * 8 + g;
@@ -177,25 +260,25 @@ struct BlockMma {
 #pragma unroll
             for (int i = 0; i < FM; ++i) {
                 const int m = wm0 + i * 16 + g;
-                double af[4];
+                T af[4];
                 af[0] = As[(ks + t) * LDA + m];
                 af[1] = As[(ks + t) * LDA + m + 8];
                 af[2] = As[(ks + t + 4) * LDA + m];
                 af[3] = As[(ks + t + 4) * LDA + m + 8];
 #pragma unroll
-                for (int j = 0; j < FN; ++j) dmma_16x8x8(acc[i][j], af, bf[j]);
+                for (int j = 0; j < FN; ++j) mma_op<SPLIT>(acc[i][j], af, bf[j]);
             }
         }
     }
 
     // acc += A(M x K) * B(K x N).  M <= BM, N <= BN; rows/columns beyond M/N and depth
-    // beyond K are zero-filled.  All 256 threads must call; shared memory is free again
-    // on return.
-    __device__ __forceinline__ void run(double *smem, const double *A, int64_t lda, const double *B,
-                                        int64_t ldb, int M, int N, int K) {
+    // beyond K are zero-filled.  All threads of the CTA must call; shared memory is free
+    // again on return.
+    __device__ __forceinline__ void run(void *smem_raw, const T *A, int64_t lda, const T *B, int64_t ldb, int M,
+                                        int N, int K) {
         if (K <= 0) return;
-        double *As = smem;
-        double *Bs = smem + STAGES * A_STAGE;
+        T *As = static_cast<T *>(smem_raw);
+        T *Bs = As + STAGES * A_STAGE;
         const int ktiles = (K + BK - 1) / BK;
 #pragma unroll
         for (int s = 0; s < STAGES - 1; ++s) {
@@ -244,20 +327,23 @@ struct BlockMma {
     }
 
     // C(r, c) -= acc(r, c); with lower_only, only where (r + r0) >= (c + c0).
-    __device__ __forceinline__ void sub_from(double *C, int64_t ldc, int M, int N, bool lower_only = false,
-                                             int r0 = 0, int c0 = 0) const {
-        for_each(M, N, [&](int r, int c, double v) {
+    __device__ __forceinline__ void sub_from(T *C, int64_t ldc, int M, int N, bool lower_only = false, int r0 = 0,
+                                             int c0 = 0) const {
+        for_each(M, N, [&](int r, int c, T v) {
             if (!lower_only || r + r0 >= c + c0) {
-                double *p = C + r + int64_t(c) * ldc;
+                T *p = C + r + int64_t(c) * ldc;
                 *p = ld_cg(p) - v;
             }
         });
     }
 
     // C(r, c) = acc(r, c).
-    __device__ __forceinline__ void store_to(double *C, int64_t ldc, int M, int N) const {
-        for_each(M, N, [&](int r, int c, double v) { C[r + int64_t(c) * ldc] = v; });
+    __device__ __forceinline__ void store_to(T *C, int64_t ldc, int M, int N) const {
+        for_each(M, N, [&](int r, int c, T v) { C[r + int64_t(c) * ldc] = v; });
     }
 };
+
+template <int BM, int BN, int WARPS_M, int WARPS_N, int BL, int VEC, int STAGES = 3, int BK_ = 16>
+using BlockMma = BlockMmaT<double, BM, BN, WARPS_M, WARPS_N, BL, VEC, STAGES, BK_>;
 
 }  // namespace mtd

@@ -33,6 +33,7 @@ struct mtd_graph {
     bool trace = false;
     double timeout_s = 10.0;
     int nest = kNestTile;
+    int prec = MTD_PREC_FP64;  // element type of the matrix runs factor
     Lowered low;   // device form, kept for the CUDA-graph executor and item queries
     int n_dev = 0;
 
@@ -48,8 +49,8 @@ struct mtd_graph {
     QueueCtl *d_qctl = nullptr;
     RunCtl *d_ctl = nullptr;
     RunCtl *h_ctl = nullptr;  // pinned copy of the control block, filled at the end of a run
-    double *d_ws_lower = nullptr;
-    double *d_ws_upper = nullptr;
+    unsigned char *d_ws_lower = nullptr;  // inverse workspaces, elements of the run's type
+    unsigned char *d_ws_upper = nullptr;
     unsigned long long *d_trace = nullptr;
     long long trace_cap = 0;
     long long total_items = 0;
@@ -75,25 +76,36 @@ int smem_setup(int device) {
     static bool done[64] = {false};
     if (device < 0 || device >= 64) return MTD_ERR_INVALID_ARG;
     if (!done[device]) {
-        if (cudaFuncSetAttribute(persistent_kernel<VEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 kOpSmemBytes()) != cudaSuccess)
-            return MTD_ERR_CUDA;
-        if (cudaFuncSetAttribute(task_kernel<VEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, kOpSmemBytes()) !=
-            cudaSuccess)
+        const int bytes = kOpSmemBytes();
+        if (cudaFuncSetAttribute(persistent_kernel<VEC, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 bytes) != cudaSuccess ||
+            cudaFuncSetAttribute(persistent_kernel<VEC, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 bytes) != cudaSuccess ||
+            cudaFuncSetAttribute(persistent_kernel<VEC, float, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 bytes) != cudaSuccess ||
+            cudaFuncSetAttribute(task_kernel<VEC, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
+                cudaSuccess)
             return MTD_ERR_CUDA;
         done[device] = true;
     }
     return MTD_OK;
 }
 
-int64_t ws_ld(const mtd_graph *g) { return g->dag.n() + (g->dag.n() & 1); }
+// Leading dimension of the inverse workspace: N rounded up to a multiple of 4 so every
+// 64-column block starts on a 16-byte boundary for either element size.
+int64_t ws_ld(const mtd_graph *g) { return (g->dag.n() + 3) & ~int64_t(3); }
 
-bool use_vec2(const mtd_graph *g, const double *dA, int64_t lda) {
-    return (reinterpret_cast<uintptr_t>(dA) % 16 == 0) && (lda % 2 == 0) && (g->dag.tile() % 2 == 0) &&
-           (g->dag.n() % 2 == 0);
+size_t elem_size(const mtd_graph *g) { return g->prec == MTD_PREC_FP64 ? sizeof(double) : sizeof(float); }
+
+// 16-byte copies need 16-byte aligned bases and leading dimensions and extents that are
+// whole 16-byte chunks of elements.
+bool use_vec2(const mtd_graph *g, const void *dA, int64_t lda) {
+    const int64_t epc = 16 / static_cast<int64_t>(elem_size(g));
+    return (reinterpret_cast<uintptr_t>(dA) % 16 == 0) && (lda % epc == 0) && (g->dag.tile() % epc == 0) &&
+           (g->dag.n() % epc == 0);
 }
 
-RunArgs make_args(const mtd_graph *g, double *dA, int64_t lda) {
+RunArgs make_args(const mtd_graph *g, void *dA, int64_t lda) {
     RunArgs a{};
     a.a = dA;
     a.lda = lda;
@@ -158,7 +170,8 @@ int build_cgraph(mtd_graph *g, double *dA, int64_t lda) {
         int task = t;
         void *args[] = {const_cast<RunArgs *>(&a), &task};
         cudaKernelNodeParams kp{};
-        kp.func = vec2 ? reinterpret_cast<void *>(task_kernel<2>) : reinterpret_cast<void *>(task_kernel<1>);
+        kp.func = vec2 ? reinterpret_cast<void *>(task_kernel<2, double>)
+                       : reinterpret_cast<void *>(task_kernel<1, double>);
         kp.gridDim = dim3(static_cast<unsigned>(items));
         kp.blockDim = dim3(kThreads);
         kp.sharedMemBytes = kOpSmemBytes();
@@ -317,7 +330,7 @@ int mtd_graph_finalize(mtd_graph *g) {
     }
     if (roots.empty()) return MTD_ERR_BAD_DAG;
     g->n_dev = nt;
-    const size_t ws = size_t(ws_ld(g)) * kNB;
+    const size_t ws = size_t(ws_ld(g)) * kNB * elem_size(g);  // bytes
     g->total_items = 0;
     for (int q = 0; q < kNumQueues; ++q) {
         g->queue_cap[q] = cap[q];
@@ -327,6 +340,13 @@ int mtd_graph_finalize(mtd_graph *g) {
     bool needs_upper = false;
     for (const auto &t : tasks)
         if (t.op == MTD_OP_GETRF) needs_upper = true;
+    if (g->prec != MTD_PREC_FP64) {
+        // the low-precision factor is Cholesky-only
+        for (const auto &t : tasks)
+            if (t.op != MTD_OP_POTRF && t.op != MTD_OP_TRSM_RLT && t.op != MTD_OP_SYRK_LN && t.op != MTD_OP_GEMM_NT &&
+                t.op != kOpJoin)
+                return MTD_ERR_INVALID_ARG;
+    }
 
     rc = MTD_OK;
     rc = rc ? rc : dev_alloc(&g->d_tasks, nt);
@@ -351,8 +371,8 @@ int mtd_graph_finalize(mtd_graph *g) {
                     cudaMemcpy(g->d_succ, succ.data(), succ.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess);
         ok = ok && cudaMemcpy(g->d_deps_init, preds.data(), nt * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
         ok = ok && cudaMemcpy(g->d_roots, roots.data(), roots.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
-        ok = ok && cudaMemset(g->d_ws_lower, 0, ws * sizeof(double)) == cudaSuccess;
-        if (needs_upper) ok = ok && cudaMemset(g->d_ws_upper, 0, ws * sizeof(double)) == cudaSuccess;
+        ok = ok && cudaMemset(g->d_ws_lower, 0, ws) == cudaSuccess;
+        if (needs_upper) ok = ok && cudaMemset(g->d_ws_upper, 0, ws) == cudaSuccess;
         ok = ok && cudaMemset(g->d_ctl, 0, sizeof(RunCtl)) == cudaSuccess;
         if (!ok) rc = MTD_ERR_CUDA;
     }
@@ -369,7 +389,38 @@ int mtd_graph_finalize(mtd_graph *g) {
     return MTD_OK;
 }
 
-int mtd_run(mtd_graph *g, double *dA, int64_t lda, void *stream, int *info_out) {
+}  // extern "C"
+
+namespace mtd {
+
+// Reset, seed and launch one persistent run (shared by graphs, batches and the
+// no-allocation entry point's sibling paths).  Stream-ordered; no host synchronisation.
+int launch_run(const RunArgs &a, const int *deps_init, const int *roots, int n_roots, long long total_items,
+               int prec, bool vec2, int grid, cudaStream_t s) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return MTD_ERR_NO_DEVICE;
+    int rc = smem_setup<2>(dev);
+    if (!rc) rc = smem_setup<1>(dev);
+    if (rc) return rc;
+    const int reset_blocks = static_cast<int>(std::min<long long>(
+        1024, std::max<long long>(1, (std::max<long long>(total_items, a.n_tasks) + kThreads - 1) / kThreads)));
+    reset_kernel<<<reset_blocks, kThreads, 0, s>>>(a, deps_init);
+    seed_kernel<<<1, 32, 0, s>>>(a, roots, n_roots);
+    const int bytes = kOpSmemBytes();
+    const bool fp64 = prec == MTD_PREC_FP64;
+    const bool x3 = prec == MTD_PREC_FP32;
+    if (fp64 && vec2) persistent_kernel<2, double><<<grid, kThreads, bytes, s>>>(a);
+    else if (fp64) persistent_kernel<1, double><<<grid, kThreads, bytes, s>>>(a);
+    else if (x3 && vec2) persistent_kernel<2, float, 3><<<grid, kThreads, bytes, s>>>(a);
+    else if (x3) persistent_kernel<1, float, 3><<<grid, kThreads, bytes, s>>>(a);
+    else if (vec2) persistent_kernel<2, float><<<grid, kThreads, bytes, s>>>(a);
+    else persistent_kernel<1, float><<<grid, kThreads, bytes, s>>>(a);
+    return cudaGetLastError() == cudaSuccess ? MTD_OK : MTD_ERR_CUDA;
+}
+
+}  // namespace mtd
+
+static int run_persistent(mtd_graph *g, void *dA, int64_t lda, void *stream, int *info_out) {
     if (!g || !dA) return MTD_ERR_INVALID_ARG;
     if (!g->finalized) return MTD_ERR_STATE;
     if (lda < g->dag.n()) return MTD_ERR_INVALID_ARG;
@@ -378,16 +429,11 @@ int mtd_run(mtd_graph *g, double *dA, int64_t lda, void *stream, int *info_out) 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
 
     const RunArgs a = make_args(g, dA, lda);
-    const bool vec2 = use_vec2(g, dA, lda);
     const int grid = g->num_sms;
     g->last_grid = grid;
-    const int reset_blocks = static_cast<int>(std::min<long long>(
-        1024, std::max<long long>(1, (std::max<long long>(g->total_items, a.n_tasks) + kThreads - 1) / kThreads)));
-    reset_kernel<<<reset_blocks, kThreads, 0, s>>>(a, g->d_deps_init);
-    seed_kernel<<<1, 32, 0, s>>>(a, g->d_roots, g->n_roots);
-    if (vec2) persistent_kernel<2><<<grid, kThreads, kOpSmemBytes(), s>>>(a);
-    else persistent_kernel<1><<<grid, kThreads, kOpSmemBytes(), s>>>(a);
-    if (cudaGetLastError() != cudaSuccess) return MTD_ERR_CUDA;
+    const int rc = launch_run(a, g->d_deps_init, g->d_roots, g->n_roots, g->total_items, g->prec,
+                              use_vec2(g, dA, lda), grid, s);
+    if (rc) return rc;
     if (cudaMemcpyAsync(g->h_ctl, g->d_ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, s) != cudaSuccess)
         return MTD_ERR_CUDA;
     g->last_stream = s;
@@ -397,8 +443,28 @@ int mtd_run(mtd_graph *g, double *dA, int64_t lda, void *stream, int *info_out) 
     return MTD_OK;
 }
 
+extern "C" {
+
+int mtd_run(mtd_graph *g, double *dA, int64_t lda, void *stream, int *info_out) {
+    if (g && g->prec != MTD_PREC_FP64) return MTD_ERR_STATE;
+    return run_persistent(g, dA, lda, stream, info_out);
+}
+
+int mtd_run_f32(mtd_graph *g, float *dA, int64_t lda, void *stream, int *info_out) {
+    if (g && g->prec == MTD_PREC_FP64) return MTD_ERR_STATE;
+    return run_persistent(g, dA, lda, stream, info_out);
+}
+
+int mtd_graph_set_precision(mtd_graph *g, int prec) {
+    if (!g || (prec != MTD_PREC_FP64 && prec != MTD_PREC_TF32 && prec != MTD_PREC_FP32)) return MTD_ERR_INVALID_ARG;
+    if (g->finalized) return MTD_ERR_STATE;
+    g->prec = prec;
+    return MTD_OK;
+}
+
 int mtd_run_graph(mtd_graph *g, double *dA, int64_t lda, void *stream, int *info_out) {
     if (!g || !dA) return MTD_ERR_INVALID_ARG;
+    if (g->prec != MTD_PREC_FP64) return MTD_ERR_STATE;
     if (!g->finalized) return MTD_ERR_STATE;
     if (lda < g->dag.n()) return MTD_ERR_INVALID_ARG;
     int dev = 0;
@@ -631,8 +697,8 @@ extern "C" int mtd_factor_noalloc(int kind, double *dA, int64_t n, int64_t lda, 
         static_cast<int>(std::min<long long>(1024, (std::max<long long>(items, nt) + kThreads - 1) / kThreads));
     reset_kernel<<<std::max(reset_blocks, 1), kThreads, 0, s>>>(a, d_deps_init);
     seed_kernel<<<1, 32, 0, s>>>(a, d_roots, static_cast<int>(roots.size()));
-    if (vec2) persistent_kernel<2><<<sms, kThreads, kOpSmemBytes(), s>>>(a);
-    else persistent_kernel<1><<<sms, kThreads, kOpSmemBytes(), s>>>(a);
+    if (vec2) persistent_kernel<2, double><<<sms, kThreads, kOpSmemBytes(), s>>>(a);
+    else persistent_kernel<1, double><<<sms, kThreads, kOpSmemBytes(), s>>>(a);
     if (cudaGetLastError() != cudaSuccess) return MTD_ERR_CUDA;
     RunCtl c;
     if (cudaMemcpyAsync(&c, a.ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, s) != cudaSuccess) return MTD_ERR_CUDA;
@@ -642,3 +708,10 @@ extern "C" int mtd_factor_noalloc(int kind, double *dA, int64_t n, int64_t lda, 
     if (c.tasks_done != nt) return MTD_ERR_TIMEOUT;
     return MTD_OK;
 }
+
+// Internal accessors for the solver (mustard_b200/csrc/solver.cu): the inverse diagonal
+// blocks a finalised graph's last run left in its workspace.
+namespace mtd {
+void *graph_ws_lower(mtd_graph *g) { return g ? g->d_ws_lower : nullptr; }
+int64_t graph_ws_ld(mtd_graph *g) { return g ? ws_ld(g) : 0; }
+}  // namespace mtd

@@ -124,31 +124,48 @@ __device__ __forceinline__ void complete_item(const RunArgs &p, int task) {
         const int succ = __ldg(&p.succ[sb + s]);
         if (atomicSub(&p.deps[succ], 1) == 1) release_task(p, succ);
     }
+    // the last task of a batched matrix (its DAG's only sink) stamps the matrix's finish time
+    if (sc == 0 && p.mat_done_ns) p.mat_done_ns[__ldg(&p.tasks[task].mat)] = global_ns();
     __threadfence();
     atomicAdd(&p.ctl->tasks_done, 1);
 }
 
-template <int VEC>
-__device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int item, double *smem) {
-    switch (t.op) {
-    case MTD_OP_POTRF: return op_potrf<VEC>(p, t, smem);
-    case MTD_OP_TRSM_RLT: return op_trsm_rlt<VEC>(p, t, item, smem);
-    case MTD_OP_SYRK_LN: return op_syrk_ln<VEC>(p, t, item, smem);
-    case MTD_OP_GEMM_NT: return op_gemm_nt<VEC>(p, t, item, smem);
-    case MTD_OP_GETRF: return op_getrf<VEC>(p, t, smem);
-    case MTD_OP_TRSM_LLNU: return op_trsm_llnu<VEC>(p, t, item, smem);
-    case MTD_OP_TRSM_RUN: return op_trsm_run<VEC>(p, t, item, smem);
-    case MTD_OP_GEMM_NN: return op_gemm_nn<VEC>(p, t, item, smem);
-    default:
-        if (threadIdx.x == 0) report_error(p.ctl, MTD_ERR_INVALID_ARG, 0);
-        return MTD_ERR_INVALID_ARG;
+// Element type of the matrix a run factors: double (the reference's FP64 arithmetic) or
+// float (low-precision Cholesky factor of the mixed-precision solver: SPLIT = 1 TF32
+// products, SPLIT = 3 FP32-accurate split-TF32 products).
+template <int VEC, typename T, int SPLIT = 1>
+__device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int item, void *smem) {
+    const MatCtx m = mat_ctx<T>(p, t);
+    if constexpr (sizeof(T) == 8) {
+        switch (t.op) {
+        case MTD_OP_POTRF: return op_potrf<T, VEC>(p, m, t, smem);
+        case MTD_OP_TRSM_RLT: return op_trsm_rlt<T, VEC>(p, m, t, item, smem);
+        case MTD_OP_SYRK_LN: return op_syrk_ln<T, VEC>(p, m, t, item, smem);
+        case MTD_OP_GEMM_NT: return op_gemm_nt<T, VEC>(p, m, t, item, smem);
+        case MTD_OP_GETRF: return op_getrf<VEC>(p, m, t, smem);
+        case MTD_OP_TRSM_LLNU: return op_trsm_llnu<VEC>(p, m, t, item, smem);
+        case MTD_OP_TRSM_RUN: return op_trsm_run<VEC>(p, m, t, item, smem);
+        case MTD_OP_GEMM_NN: return op_gemm_nn<VEC>(p, m, t, item, smem);
+        default: break;
+        }
+    } else {
+        switch (t.op) {
+        case MTD_OP_POTRF: return op_potrf<T, VEC, SPLIT>(p, m, t, smem);
+        case MTD_OP_TRSM_RLT: return op_trsm_rlt<T, VEC, SPLIT>(p, m, t, item, smem);
+        case MTD_OP_SYRK_LN: return op_syrk_ln<T, VEC, SPLIT>(p, m, t, item, smem);
+        case MTD_OP_GEMM_NT: return op_gemm_nt<T, VEC, SPLIT>(p, m, t, item, smem);
+        default: break;
+        }
     }
+    if (threadIdx.x == 0) report_error(p.ctl, MTD_ERR_INVALID_ARG, 0);
+    return MTD_ERR_INVALID_ARG;
 }
 
-template <int VEC>
+template <int VEC, typename T, int SPLIT = 1>
 __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const RunArgs p) {
     extern __shared__ __align__(128) double smem[];
     __shared__ int s_cmd, s_task, s_item;
+    if (threadIdx.x == 0) atomicMin(&p.ctl->start_ns, global_ns());
     while (true) {
         if (threadIdx.x == 0) {
             int tk = 0, it = 0;
@@ -167,7 +184,7 @@ __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const RunArgs p
 #pragma unroll
             for (int w = 0; w < int(sizeof(DevTask) / sizeof(int4)); ++w) dst[w] = __ldg(src + w);
         }
-        const int st = dispatch<VEC>(p, t, item, smem);
+        const int st = dispatch<VEC, T, SPLIT>(p, t, item, smem);
         __syncthreads();
         if (threadIdx.x == 0) {
             if (st == 0) complete_item(p, task);
@@ -188,12 +205,12 @@ __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const RunArgs p
 // One task as an ordinary launch (grid = its work items): the node kernel of the
 // host-launched CUDA-graph executor, the reference's --tiled mode
 // (mustard/mustard.h:155-159, cholesky_mustard.cu:498-513).
-template <int VEC>
+template <int VEC, typename T>
 __global__ void __launch_bounds__(kThreads, 1) task_kernel(const RunArgs p, int task) {
     extern __shared__ __align__(128) double smem[];
     if (ld_volatile(&p.ctl->abort)) return;
     const DevTask t = p.tasks[task];
-    if (t.n_items > 0) dispatch<VEC>(p, t, static_cast<int>(blockIdx.x), smem);
+    if (t.n_items > 0) dispatch<VEC, T>(p, t, static_cast<int>(blockIdx.x), smem);
 }
 
 __global__ void reset_ctl_kernel(const RunArgs p) {
@@ -203,6 +220,7 @@ __global__ void reset_ctl_kernel(const RunArgs p) {
         p.ctl->info = 0x7fffffff;
         p.ctl->abort = 0;
         p.ctl->items_done = 0;
+        p.ctl->start_ns = ~0ull;
     }
 }
 
@@ -226,6 +244,7 @@ __global__ void reset_kernel(const RunArgs p, const int *deps_init) {
         p.ctl->info = 0x7fffffff;
         p.ctl->abort = 0;
         p.ctl->items_done = 0;
+        p.ctl->start_ns = ~0ull;
     }
 }
 

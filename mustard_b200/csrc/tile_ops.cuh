@@ -1,13 +1,18 @@
-// FP64 tile operations executed by one persistent CTA per work item.
+// Tile operations executed by one persistent CTA per work item.
 //
 // Each operation replaces one captured cuBLAS / cuSOLVER call of the reference
 // (mustard/cholesky_mustard.cu:238-387, mustard/lu_mustard.cu:361-522).  The dense
-// updates are tensor-core DMMA block products (mma.cuh).  The diagonal factorisations
-// are left-looking blocked algorithms with kNB-wide diagonal blocks factored in shared
+// updates are tensor-core block products (mma.cuh).  The diagonal factorisations are
+// left-looking blocked algorithms with kNB-wide diagonal blocks factored in shared
 // memory; while a block is in shared memory its triangular inverse is formed and left in
 // the inverse workspace (indexed by the block's first matrix row), so every triangular
 // solve -- inside the diagonal task and in the TRSM tasks that follow it -- becomes a
 // block product as well.  Block geometry comes from the task (DevTask), in elements.
+//
+// The Cholesky operations are templated on the element type: double (FP64 DMMA, the
+// reference's arithmetic) or float (FP32 storage, TF32 tensor-core products with FP32
+// accumulation, FP32 diagonal blocks) for the low-precision factor of the mixed-precision
+// solver.  The LU operations are FP64 only.
 #pragma once
 
 #include "device_types.hpp"
@@ -39,17 +44,44 @@ constexpr int kGemmWarpsM = MTD_GEMM_WARPS_M;
 constexpr int kGemmWarpsN = kThreads / 32 / kGemmWarpsM;
 constexpr int kPanelWarpsM = MTD_PANEL_WARPS_M;
 constexpr int kPanelWarpsN = kThreads / 32 / kPanelWarpsM;
-template <int BL, int VEC>
-using GemmMma = BlockMma<kGemmTile, kGemmTile, kGemmWarpsM, kGemmWarpsN, BL, VEC, MTD_GEMM_STAGES, MTD_GEMM_BK>;
-template <int BL, int VEC>
-using PanelMma = BlockMma<64, 64, kPanelWarpsM, kPanelWarpsN, BL, VEC>;
+template <int BL, int VEC, typename T = double, int SPLIT = 1>
+using GemmMma =
+    BlockMmaT<T, kGemmTile, kGemmTile, kGemmWarpsM, kGemmWarpsN, BL, VEC, MTD_GEMM_STAGES, MTD_GEMM_BK, SPLIT>;
+template <int BL, int VEC, typename T = double, int SPLIT = 1>
+using PanelMma = BlockMmaT<T, 64, 64, kPanelWarpsM, kPanelWarpsN, BL, VEC, 3, 16, SPLIT>;
 
 __device__ __forceinline__ void block_fence_sync() {
     __threadfence_block();
     __syncthreads();
 }
 
-__device__ __forceinline__ double *at(const RunArgs &p, int r, int c) { return p.a + r + int64_t(c) * p.lda; }
+// The matrix one task works on: the run's matrix, or in a batched run the task's own
+// matrix (DevTask::mat), with its inverse workspace.
+struct MatCtx {
+    void *a;
+    int64_t lda;
+    void *wsl;
+    void *wsu;
+    int64_t wsld;
+    int mat;  // -1 for a single-matrix run
+};
+
+template <typename T>
+__device__ __forceinline__ MatCtx mat_ctx(const RunArgs &p, const DevTask &t) {
+    if (p.mats == nullptr) return MatCtx{p.a, p.lda, p.ws_lower, p.ws_upper, p.ws_ld, -1};
+    const BatchMat &bm = p.mats[t.mat];
+    return MatCtx{bm.a, bm.lda, static_cast<T *>(p.ws_lower) + bm.ws_off,
+                  p.ws_upper ? static_cast<T *>(p.ws_upper) + bm.ws_off : nullptr, bm.ws_ld, t.mat};
+}
+
+template <typename T>
+__device__ __forceinline__ T *at(const MatCtx &m, int r, int c) {
+    return static_cast<T *>(m.a) + r + int64_t(c) * m.lda;
+}
+template <typename T>
+__device__ __forceinline__ T *ws_lo(const MatCtx &m) { return static_cast<T *>(m.wsl); }
+template <typename T>
+__device__ __forceinline__ T *ws_up(const MatCtx &m) { return static_cast<T *>(m.wsu); }
 
 __device__ __forceinline__ void report_error(RunCtl *ctl, int code, int info) {
     if (info > 0) atomicMin(&ctl->info, info);
@@ -58,23 +90,37 @@ __device__ __forceinline__ void report_error(RunCtl *ctl, int code, int info) {
     atomicExch(&ctl->abort, 1);
 }
 
+// A diagonal factorisation met a bad pivot (thread 0 reports).  A single-matrix run stops
+// with the error; a batched run records LAPACK-style info for that matrix only and lets
+// the task complete, so the other matrices of the batch finish (the failed matrix's
+// factor is left partial, as LAPACK's batched routines leave it).  Returns the status the
+// task ends with.
+__device__ __forceinline__ int diag_failure(const RunArgs &p, const MatCtx &m, int code, int info) {
+    if (m.mat < 0) {
+        if (threadIdx.x == 0) report_error(p.ctl, code, info);
+        return code;
+    }
+    if (threadIdx.x == 0) atomicMin(p.mat_info + m.mat, info);
+    return 0;
+}
+
 // X = T^-1 for a jn x jn lower-triangular T read through tl(i, l) (i >= l); unit
-// diagonal when UNIT.  Four lanes per column, 64 columns per CTA; rows swept top-down.
-template <bool UNIT, typename TL>
-__device__ __forceinline__ void lower_inverse(int jn, TL tl, double *X) {
+// diagonal when UNIT.  Four lanes per column (64 columns); rows swept top-down.
+template <bool UNIT, typename E, typename TL>
+__device__ __forceinline__ void lower_inverse(int jn, TL tl, E *X) {
     const int c = threadIdx.x >> 2;
     const int q = threadIdx.x & 3;
     for (int i = 0; i < jn; ++i) {
-        double part = 0.0;
+        E part = E(0);
         if (c < i)
             for (int l = c + q; l < i; l += 4) part += tl(i, l) * X[l + c * kDiagLd];
         part += __shfl_xor_sync(0xffffffffu, part, 1);
         part += __shfl_xor_sync(0xffffffffu, part, 2);
         if (q == 0 && c < jn) {
-            double v;
-            if (c > i) v = 0.0;
-            else if (UNIT) v = (c == i) ? 1.0 : -part;
-            else v = (c == i) ? 1.0 / tl(i, i) : -part / tl(i, i);
+            E v;
+            if (c > i) v = E(0);
+            else if (UNIT) v = (c == i) ? E(1) : -part;
+            else v = (c == i) ? E(1) / tl(i, i) : -part / tl(i, i);
             X[i + c * kDiagLd] = v;
         }
         __syncwarp();
@@ -84,39 +130,38 @@ __device__ __forceinline__ void lower_inverse(int jn, TL tl, double *X) {
 
 // Cholesky of the jn x jn diagonal block at Ad (lower), in shared memory.  Writes L back
 // (lower triangle only; the strict upper triangle is never touched, as with LAPACK's
-// uplo = 'L') and L^-1 to Wd (ld = p.ws_ld, full block with zeros above).
-__device__ __forceinline__ int factor_chol_diag(const RunArgs &p, double *Ad, int jn, double *Wd,
-                                                double *smem, int info_base) {
+// uplo = 'L') and L^-1 to Wd (ld = m.wsld, full block with zeros above).
+template <typename T>
+__device__ __forceinline__ int factor_chol_diag(const RunArgs &p, const MatCtx &m, T *Ad, int jn, T *Wd, void *smem_raw,
+                                                int info_base) {
     const int tid = threadIdx.x;
-    double *D = smem;
-    double *X = smem + kNB * kDiagLd;
-    const int64_t lda = p.lda;
+    T *D = static_cast<T *>(smem_raw);
+    T *X = D + kNB * kDiagLd;
+    const int64_t lda = m.lda;
     for (int e = tid; e < jn * jn; e += kThreads) {
         const int r = e % jn, c = e / jn;
-        D[r + c * kDiagLd] = (r >= c) ? ld_cg(Ad + r + int64_t(c) * lda) : 0.0;
+        D[r + c * kDiagLd] = (r >= c) ? ld_cg(Ad + r + int64_t(c) * lda) : T(0);
     }
     __syncthreads();
     for (int j = 0; j < jn; ++j) {
-        const double djj = D[j + j * kDiagLd];
-        if (!(djj > 0.0)) {  // also catches NaN
-            if (tid == 0) report_error(p.ctl, MTD_ERR_NOT_POSITIVE_DEFINITE, info_base + j + 1);
-            return MTD_ERR_NOT_POSITIVE_DEFINITE;
-        }
-        const double s = sqrt(djj);
-        const double rs = 1.0 / s;
+        const T djj = D[j + j * kDiagLd];
+        if (!(djj > T(0)))  // also catches NaN
+            return diag_failure(p, m, MTD_ERR_NOT_POSITIVE_DEFINITE, info_base + j + 1);
+        const T s = sqrt(djj);
+        const T rs = T(1) / s;
         __syncthreads();
         for (int r = j + 1 + tid; r < jn; r += kThreads) D[r + j * kDiagLd] *= rs;
         if (tid == 0) D[j + j * kDiagLd] = s;
         __syncthreads();
-        const int m = jn - j - 1;
-        for (int e = tid; e < m * m; e += kThreads) {
-            const int r = j + 1 + e % m, c = j + 1 + e / m;
+        const int rest = jn - j - 1;
+        for (int e = tid; e < rest * rest; e += kThreads) {
+            const int r = j + 1 + e % rest, c = j + 1 + e / rest;
             if (r >= c) D[r + c * kDiagLd] -= D[r + j * kDiagLd] * D[c + j * kDiagLd];
         }
         __syncthreads();
     }
     lower_inverse<false>(jn, [&](int i, int l) { return D[i + l * kDiagLd]; }, X);
-    const int64_t ldw = p.ws_ld;
+    const int64_t ldw = m.wsld;
     for (int e = tid; e < jn * jn; e += kThreads) {
         const int r = e % jn, c = e / jn;
         if (r >= c) Ad[r + int64_t(c) * lda] = D[r + c * kDiagLd];
@@ -128,13 +173,13 @@ __device__ __forceinline__ int factor_chol_diag(const RunArgs &p, double *Ad, in
 // No-pivot LU of the jn x jn diagonal block at Ad, in shared memory (what
 // cusolverDnDgetrf computes with ipiv = NULL).  Writes L\U back, L^-1 (unit lower) to
 // WLd and U^-1 (upper) to WUd.
-__device__ __forceinline__ int factor_lu_diag(const RunArgs &p, double *Ad, int jn, double *WLd, double *WUd,
-                                              double *smem, int info_base) {
+__device__ __forceinline__ int factor_lu_diag(const RunArgs &p, const MatCtx &m, double *Ad, int jn, double *WLd, double *WUd,
+                                              void *smem_raw, int info_base) {
     const int tid = threadIdx.x;
-    double *D = smem;
-    double *XL = smem + kNB * kDiagLd;
-    double *XU = smem + 2 * kNB * kDiagLd;
-    const int64_t lda = p.lda;
+    double *D = static_cast<double *>(smem_raw);
+    double *XL = D + kNB * kDiagLd;
+    double *XU = D + 2 * kNB * kDiagLd;
+    const int64_t lda = m.lda;
     for (int e = tid; e < jn * jn; e += kThreads) {
         const int r = e % jn, c = e / jn;
         D[r + c * kDiagLd] = ld_cg(Ad + r + int64_t(c) * lda);
@@ -142,16 +187,13 @@ __device__ __forceinline__ int factor_lu_diag(const RunArgs &p, double *Ad, int 
     __syncthreads();
     for (int j = 0; j < jn; ++j) {
         const double piv = D[j + j * kDiagLd];
-        if (piv == 0.0) {
-            if (tid == 0) report_error(p.ctl, MTD_ERR_SINGULAR, info_base + j + 1);
-            return MTD_ERR_SINGULAR;
-        }
+        if (piv == 0.0) return diag_failure(p, m, MTD_ERR_SINGULAR, info_base + j + 1);
         const double rp = 1.0 / piv;
         for (int r = j + 1 + tid; r < jn; r += kThreads) D[r + j * kDiagLd] *= rp;
         __syncthreads();
-        const int m = jn - j - 1;
-        for (int e = tid; e < m * m; e += kThreads) {
-            const int r = j + 1 + e % m, c = j + 1 + e / m;
+        const int rest = jn - j - 1;
+        for (int e = tid; e < rest * rest; e += kThreads) {
+            const int r = j + 1 + e % rest, c = j + 1 + e / rest;
             D[r + c * kDiagLd] -= D[r + j * kDiagLd] * D[j + c * kDiagLd];
         }
         __syncthreads();
@@ -159,7 +201,7 @@ __device__ __forceinline__ int factor_lu_diag(const RunArgs &p, double *Ad, int 
     lower_inverse<true>(jn, [&](int i, int l) { return D[i + l * kDiagLd]; }, XL);
     // U^-1 = ((U^T)^-1)^T, and U^T is lower triangular.
     lower_inverse<false>(jn, [&](int i, int l) { return D[l + i * kDiagLd]; }, XU);
-    const int64_t ldw = p.ws_ld;
+    const int64_t ldw = m.wsld;
     for (int e = tid; e < jn * jn; e += kThreads) {
         const int r = e % jn, c = e / jn;
         Ad[r + int64_t(c) * lda] = D[r + c * kDiagLd];
@@ -172,36 +214,36 @@ __device__ __forceinline__ int factor_lu_diag(const RunArgs &p, double *Ad, int 
 // ---------------------------------------------------------------------------------
 // POTRF: left-looking blocked Cholesky of the m x m diagonal block at (cr, cc), one CTA.
 // ---------------------------------------------------------------------------------
-template <int VEC>
-__device__ int op_potrf(const RunArgs &p, const DevTask &t, double *smem) {
-    using Mn = PanelMma<kBNContig, VEC>;
+template <typename T, int VEC, int SPLIT = 1>
+__device__ int op_potrf(const RunArgs &p, const MatCtx &m, const DevTask &t, void *smem) {
+    using Mn = PanelMma<kBNContig, VEC, T, SPLIT>;
     const int n = t.m;
-    double *A = at(p, t.cr, t.cc);
-    double *W = p.ws_lower + t.cr;
-    const int64_t lda = p.lda, ldw = p.ws_ld;
+    T *A = at<T>(m, t.cr, t.cc);
+    T *W = ws_lo<T>(m) + t.cr;
+    const int64_t lda = m.lda, ldw = m.wsld;
     for (int jb = 0; jb < n; jb += kNB) {
         const int jn = min(kNB, n - jb);
         if (jb > 0) {
             // A[jb:n, jb:jb+jn] -= A[jb:n, 0:jb] * A[jb:jb+jn, 0:jb]^T (lower part of the block)
             for (int r0 = jb; r0 < n; r0 += 64) {
                 const int mm = min(64, n - r0);
-                Mn m;
-                m.zero();
-                m.run(smem, A + r0, lda, A + jb, lda, mm, jn, jb);
-                m.sub_from(A + r0 + int64_t(jb) * lda, lda, mm, jn, r0 == jb, 0, 0);
+                Mn e;
+                e.zero();
+                e.run(smem, A + r0, lda, A + jb, lda, mm, jn, jb);
+                e.sub_from(A + r0 + int64_t(jb) * lda, lda, mm, jn, r0 == jb, 0, 0);
             }
             block_fence_sync();
         }
-        const int st = factor_chol_diag(p, A + jb + int64_t(jb) * lda, jn, W + jb, smem, t.cc + jb);
+        const int st = factor_chol_diag<T>(p, m, A + jb + int64_t(jb) * lda, jn, W + jb, smem, t.cc + jb);
         if (st) return st;
         block_fence_sync();
         // A[jb+jn:n, jb:jb+jn] = A[jb+jn:n, jb:jb+jn] * L_jj^-T
         for (int r0 = jb + jn; r0 < n; r0 += 64) {
             const int mm = min(64, n - r0);
-            Mn m;
-            m.zero();
-            m.run(smem, A + r0 + int64_t(jb) * lda, lda, W + jb, ldw, mm, jn, jn);
-            m.store_to(A + r0 + int64_t(jb) * lda, lda, mm, jn);
+            Mn e;
+            e.zero();
+            e.run(smem, A + r0 + int64_t(jb) * lda, lda, W + jb, ldw, mm, jn, jn);
+            e.store_to(A + r0 + int64_t(jb) * lda, lda, mm, jn);
         }
         block_fence_sync();
     }
@@ -212,52 +254,52 @@ __device__ int op_potrf(const RunArgs &p, const DevTask &t, double *smem) {
 // GETRF without pivoting: left-looking (Crout) blocked LU of the m x m block, one CTA.
 // ---------------------------------------------------------------------------------
 template <int VEC>
-__device__ int op_getrf(const RunArgs &p, const DevTask &t, double *smem) {
+__device__ int op_getrf(const RunArgs &p, const MatCtx &m, const DevTask &t, void *smem) {
     using Mk = PanelMma<kBKContig, VEC>;
     const int n = t.m;
-    double *A = at(p, t.cr, t.cc);
-    double *WL = p.ws_lower + t.cr;
-    double *WU = p.ws_upper + t.cr;
-    const int64_t lda = p.lda, ldw = p.ws_ld;
+    double *A = at<double>(m, t.cr, t.cc);
+    double *WL = ws_lo<double>(m) + t.cr;
+    double *WU = ws_up<double>(m) + t.cr;
+    const int64_t lda = m.lda, ldw = m.wsld;
     for (int jb = 0; jb < n; jb += kNB) {
         const int jn = min(kNB, n - jb);
         if (jb > 0) {
             // block column: A[jb:n, jb:jb+jn] -= A[jb:n, 0:jb] * A[0:jb, jb:jb+jn]
             for (int r0 = jb; r0 < n; r0 += 64) {
                 const int mm = min(64, n - r0);
-                Mk m;
-                m.zero();
-                m.run(smem, A + r0, lda, A + int64_t(jb) * lda, lda, mm, jn, jb);
-                m.sub_from(A + r0 + int64_t(jb) * lda, lda, mm, jn);
+                Mk e;
+                e.zero();
+                e.run(smem, A + r0, lda, A + int64_t(jb) * lda, lda, mm, jn, jb);
+                e.sub_from(A + r0 + int64_t(jb) * lda, lda, mm, jn);
             }
             // block row: A[jb:jb+jn, jb+jn:n] -= A[jb:jb+jn, 0:jb] * A[0:jb, jb+jn:n]
             for (int c0 = jb + jn; c0 < n; c0 += 64) {
                 const int nn = min(64, n - c0);
-                Mk m;
-                m.zero();
-                m.run(smem, A + jb, lda, A + int64_t(c0) * lda, lda, jn, nn, jb);
-                m.sub_from(A + jb + int64_t(c0) * lda, lda, jn, nn);
+                Mk e;
+                e.zero();
+                e.run(smem, A + jb, lda, A + int64_t(c0) * lda, lda, jn, nn, jb);
+                e.sub_from(A + jb + int64_t(c0) * lda, lda, jn, nn);
             }
             block_fence_sync();
         }
-        const int st = factor_lu_diag(p, A + jb + int64_t(jb) * lda, jn, WL + jb, WU + jb, smem, t.cc + jb);
+        const int st = factor_lu_diag(p, m, A + jb + int64_t(jb) * lda, jn, WL + jb, WU + jb, smem, t.cc + jb);
         if (st) return st;
         block_fence_sync();
         // L panel: A[jb+jn:n, jb:jb+jn] = A[...] * U_jj^-1
         for (int r0 = jb + jn; r0 < n; r0 += 64) {
             const int mm = min(64, n - r0);
-            Mk m;
-            m.zero();
-            m.run(smem, A + r0 + int64_t(jb) * lda, lda, WU + jb, ldw, mm, jn, jn);
-            m.store_to(A + r0 + int64_t(jb) * lda, lda, mm, jn);
+            Mk e;
+            e.zero();
+            e.run(smem, A + r0 + int64_t(jb) * lda, lda, WU + jb, ldw, mm, jn, jn);
+            e.store_to(A + r0 + int64_t(jb) * lda, lda, mm, jn);
         }
         // U row: A[jb:jb+jn, jb+jn:n] = L_jj^-1 * A[...]
         for (int c0 = jb + jn; c0 < n; c0 += 64) {
             const int nn = min(64, n - c0);
-            Mk m;
-            m.zero();
-            m.run(smem, WL + jb, ldw, A + jb + int64_t(c0) * lda, lda, jn, nn, jn);
-            m.store_to(A + jb + int64_t(c0) * lda, lda, jn, nn);
+            Mk e;
+            e.zero();
+            e.run(smem, WL + jb, ldw, A + jb + int64_t(c0) * lda, lda, jn, nn, jn);
+            e.store_to(A + jb + int64_t(c0) * lda, lda, jn, nn);
         }
         block_fence_sync();
     }
@@ -270,29 +312,29 @@ __device__ int op_getrf(const RunArgs &p, const DevTask &t, double *smem) {
 // ---------------------------------------------------------------------------------
 
 // X = X * L^-T   (cublasDtrsm R, L, T, NonUnit; cholesky_mustard.cu:281)
-template <int VEC>
-__device__ int op_trsm_rlt(const RunArgs &p, const DevTask &t, int item, double *smem) {
-    using Mn = PanelMma<kBNContig, VEC>;
+template <typename T, int VEC, int SPLIT = 1>
+__device__ int op_trsm_rlt(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
+    using Mn = PanelMma<kBNContig, VEC, T, SPLIT>;
     const int r0 = item * kPanelRows;
     const int mm = min(kPanelRows, t.m - r0);
     const int nk = t.n;
-    const int64_t lda = p.lda, ldw = p.ws_ld;
-    double *X = at(p, t.cr + r0, t.cc);
-    const double *L = at(p, t.ar, t.ac);
-    const double *W = p.ws_lower + t.ar;
+    const int64_t lda = m.lda, ldw = m.wsld;
+    T *X = at<T>(m, t.cr + r0, t.cc);
+    const T *L = at<T>(m, t.ar, t.ac);
+    const T *W = ws_lo<T>(m) + t.ar;
     for (int jb = 0; jb < nk; jb += kNB) {
         const int jn = min(kNB, nk - jb);
         if (jb > 0) {
-            Mn m;
-            m.zero();
-            m.run(smem, X, lda, L + jb, lda, mm, jn, jb);
-            m.sub_from(X + int64_t(jb) * lda, lda, mm, jn);
+            Mn e;
+            e.zero();
+            e.run(smem, X, lda, L + jb, lda, mm, jn, jb);
+            e.sub_from(X + int64_t(jb) * lda, lda, mm, jn);
             block_fence_sync();
         }
-        Mn m;
-        m.zero();
-        m.run(smem, X + int64_t(jb) * lda, lda, W + jb, ldw, mm, jn, jn);
-        m.store_to(X + int64_t(jb) * lda, lda, mm, jn);
+        Mn e;
+        e.zero();
+        e.run(smem, X + int64_t(jb) * lda, lda, W + jb, ldw, mm, jn, jn);
+        e.store_to(X + int64_t(jb) * lda, lda, mm, jn);
         block_fence_sync();
     }
     return 0;
@@ -300,28 +342,28 @@ __device__ int op_trsm_rlt(const RunArgs &p, const DevTask &t, int item, double 
 
 // X = X * U^-1   (cublasDtrsm R, U, N, NonUnit; lu_mustard.cu:459)
 template <int VEC>
-__device__ int op_trsm_run(const RunArgs &p, const DevTask &t, int item, double *smem) {
+__device__ int op_trsm_run(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
     using Mk = PanelMma<kBKContig, VEC>;
     const int r0 = item * kPanelRows;
     const int mm = min(kPanelRows, t.m - r0);
     const int nk = t.n;
-    const int64_t lda = p.lda, ldw = p.ws_ld;
-    double *X = at(p, t.cr + r0, t.cc);
-    const double *U = at(p, t.ar, t.ac);
-    const double *W = p.ws_upper + t.ar;
+    const int64_t lda = m.lda, ldw = m.wsld;
+    double *X = at<double>(m, t.cr + r0, t.cc);
+    const double *U = at<double>(m, t.ar, t.ac);
+    const double *W = ws_up<double>(m) + t.ar;
     for (int jb = 0; jb < nk; jb += kNB) {
         const int jn = min(kNB, nk - jb);
         if (jb > 0) {
-            Mk m;
-            m.zero();
-            m.run(smem, X, lda, U + int64_t(jb) * lda, lda, mm, jn, jb);
-            m.sub_from(X + int64_t(jb) * lda, lda, mm, jn);
+            Mk e;
+            e.zero();
+            e.run(smem, X, lda, U + int64_t(jb) * lda, lda, mm, jn, jb);
+            e.sub_from(X + int64_t(jb) * lda, lda, mm, jn);
             block_fence_sync();
         }
-        Mk m;
-        m.zero();
-        m.run(smem, X + int64_t(jb) * lda, lda, W + jb, ldw, mm, jn, jn);
-        m.store_to(X + int64_t(jb) * lda, lda, mm, jn);
+        Mk e;
+        e.zero();
+        e.run(smem, X + int64_t(jb) * lda, lda, W + jb, ldw, mm, jn, jn);
+        e.store_to(X + int64_t(jb) * lda, lda, mm, jn);
         block_fence_sync();
     }
     return 0;
@@ -329,28 +371,28 @@ __device__ int op_trsm_run(const RunArgs &p, const DevTask &t, int item, double 
 
 // X = L^-1 * X, unit diagonal   (cublasDtrsm L, L, N, Unit; lu_mustard.cu:413)
 template <int VEC>
-__device__ int op_trsm_llnu(const RunArgs &p, const DevTask &t, int item, double *smem) {
+__device__ int op_trsm_llnu(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
     using Mk = PanelMma<kBKContig, VEC>;
     const int c0 = item * kPanelRows;
     const int nc = min(kPanelRows, t.n - c0);
     const int nk = t.m;
-    const int64_t lda = p.lda, ldw = p.ws_ld;
-    double *X = at(p, t.cr, t.cc + c0);
-    const double *L = at(p, t.ar, t.ac);
-    const double *W = p.ws_lower + t.ar;
+    const int64_t lda = m.lda, ldw = m.wsld;
+    double *X = at<double>(m, t.cr, t.cc + c0);
+    const double *L = at<double>(m, t.ar, t.ac);
+    const double *W = ws_lo<double>(m) + t.ar;
     for (int jb = 0; jb < nk; jb += kNB) {
         const int jn = min(kNB, nk - jb);
         if (jb > 0) {
-            Mk m;
-            m.zero();
-            m.run(smem, L + jb, lda, X, lda, jn, nc, jb);
-            m.sub_from(X + jb, lda, jn, nc);
+            Mk e;
+            e.zero();
+            e.run(smem, L + jb, lda, X, lda, jn, nc, jb);
+            e.sub_from(X + jb, lda, jn, nc);
             block_fence_sync();
         }
-        Mk m;
-        m.zero();
-        m.run(smem, W + jb, ldw, X + jb, lda, jn, nc, jn);
-        m.store_to(X + jb, lda, jn, nc);
+        Mk e;
+        e.zero();
+        e.run(smem, W + jb, ldw, X + jb, lda, jn, nc, jn);
+        e.store_to(X + jb, lda, jn, nc);
         block_fence_sync();
     }
     return 0;
@@ -361,56 +403,56 @@ __device__ int op_trsm_llnu(const RunArgs &p, const DevTask &t, int item, double
 // ---------------------------------------------------------------------------------
 
 // C -= A B^T   (cublasGemmEx N, T; cholesky_mustard.cu:376)
-template <int VEC>
-__device__ int op_gemm_nt(const RunArgs &p, const DevTask &t, int item, double *smem) {
-    using Mg = GemmMma<kBNContig, VEC>;
+template <typename T, int VEC, int SPLIT = 1>
+__device__ int op_gemm_nt(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
+    using Mg = GemmMma<kBNContig, VEC, T, SPLIT>;
     const int nbn = (t.n + kGemmTile - 1) / kGemmTile;
     const int r0 = (item / nbn) * kGemmTile, c0 = (item % nbn) * kGemmTile;
     const int mm = min(kGemmTile, t.m - r0), nn = min(kGemmTile, t.n - c0);
-    Mg m;
-    m.zero();
-    m.run(smem, at(p, t.ar + r0, t.ac), p.lda, at(p, t.br + c0, t.bc), p.lda, mm, nn, t.k);
-    m.sub_from(at(p, t.cr + r0, t.cc + c0), p.lda, mm, nn);
+    Mg e;
+    e.zero();
+    e.run(smem, at<T>(m, t.ar + r0, t.ac), m.lda, at<T>(m, t.br + c0, t.bc), m.lda, mm, nn, t.k);
+    e.sub_from(at<T>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn);
     return 0;
 }
 
 // C -= A B   (cublasGemmEx N, N; lu_mustard.cu:511)
 template <int VEC>
-__device__ int op_gemm_nn(const RunArgs &p, const DevTask &t, int item, double *smem) {
+__device__ int op_gemm_nn(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
     using Mg = GemmMma<kBKContig, VEC>;
     const int nbn = (t.n + kGemmTile - 1) / kGemmTile;
     const int r0 = (item / nbn) * kGemmTile, c0 = (item % nbn) * kGemmTile;
     const int mm = min(kGemmTile, t.m - r0), nn = min(kGemmTile, t.n - c0);
-    Mg m;
-    m.zero();
-    m.run(smem, at(p, t.ar + r0, t.ac), p.lda, at(p, t.br, t.bc + c0), p.lda, mm, nn, t.k);
-    m.sub_from(at(p, t.cr + r0, t.cc + c0), p.lda, mm, nn);
+    Mg e;
+    e.zero();
+    e.run(smem, at<double>(m, t.ar + r0, t.ac), m.lda, at<double>(m, t.br, t.bc + c0), m.lda, mm, nn, t.k);
+    e.sub_from(at<double>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn);
     return 0;
 }
 
 // C -= A A^T, lower triangle only   (cublasDsyrk L, N; cholesky_mustard.cu:327)
-template <int VEC>
-__device__ int op_syrk_ln(const RunArgs &p, const DevTask &t, int item, double *smem) {
-    using Mg = GemmMma<kBNContig, VEC>;
+template <typename T, int VEC, int SPLIT = 1>
+__device__ int op_syrk_ln(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
+    using Mg = GemmMma<kBNContig, VEC, T, SPLIT>;
     int pb = 0;
     while ((pb + 1) * (pb + 2) / 2 <= item) ++pb;
     const int qb = item - pb * (pb + 1) / 2;
     const int r0 = pb * kGemmTile, c0 = qb * kGemmTile;
     const int mm = min(kGemmTile, t.m - r0), nn = min(kGemmTile, t.m - c0);
-    Mg m;
-    m.zero();
-    m.run(smem, at(p, t.ar + r0, t.ac), p.lda, at(p, t.ar + c0, t.ac), p.lda, mm, nn, t.k);
-    m.sub_from(at(p, t.cr + r0, t.cc + c0), p.lda, mm, nn, pb == qb, 0, 0);
+    Mg e;
+    e.zero();
+    e.run(smem, at<T>(m, t.ar + r0, t.ac), m.lda, at<T>(m, t.ar + c0, t.ac), m.lda, mm, nn, t.k);
+    e.sub_from(at<T>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn, pb == qb, 0, 0);
     return 0;
 }
 
 // Shared memory (bytes) the largest operation needs.
 constexpr int kOpSmemBytes() {
-    constexpr int g1 = GemmMma<kBNContig, 2>::SMEM_DOUBLES;
-    constexpr int g2 = GemmMma<kBKContig, 2>::SMEM_DOUBLES;
-    constexpr int diag = 3 * kNB * kDiagLd;
+    constexpr int g1 = GemmMma<kBNContig, 2>::SMEM_BYTES;
+    constexpr int g2 = GemmMma<kBKContig, 2>::SMEM_BYTES;
+    constexpr int diag = 3 * kNB * kDiagLd * 8;
     constexpr int m = g1 > g2 ? g1 : g2;
-    return 8 * (m > diag ? m : diag);
+    return m > diag ? m : diag;
 }
 
 }  // namespace mtd

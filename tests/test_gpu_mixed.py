@@ -1,0 +1,117 @@
+"""Mixed-precision solver (no reference counterpart): TF32 tiled Cholesky on the task
+scheduler plus FP64 iterative refinement / GMRES-IR, against an FP64 LAPACK oracle.
+Bars: backward error <= 1e-13 (normwise, infinity norms, FP64) when converged; forward
+error within cond(A) * 1e-13 of the FP64 oracle's solution."""
+import numpy as np
+import pytest
+
+from oracle import gen, mixed, tiled
+from tests.gpu_util import from_dev, rel_diff, to_dev
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev_rect(x):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(np.asarray(x).T)).cuda().t()
+
+
+def _host_rect(t):
+    return np.asfortranarray(t.t().contiguous().cpu().numpy().T)
+
+
+def test_tf32_factor_close_to_fp64(mtd):
+    import torch
+    n, tile = 1536, 512
+    a = gen.spd_input(n, 3)
+    g = mtd.TaskGraph(mtd.KIND_CHOLESKY, n, tile).build_tiled().set_precision(mtd.PREC_TF32).finalize()
+    d = torch.from_numpy(np.ascontiguousarray(a.T).astype(np.float32)).cuda().t()
+    assert g.run_f32(d) == 0
+    l32 = np.tril(np.asfortranarray(d.t().contiguous().cpu().numpy().T).astype(np.float64))
+    ref = np.tril(tiled.cholesky_lapack(a))
+    err = rel_diff(l32, ref)
+    assert 1e-7 < err < 5e-3  # TF32 products (unit roundoff 2^-11), FP32 accumulation
+    # FP64 graphs refuse float runs and the other way round
+    with pytest.raises(mtd.MtdError):
+        g.run(to_dev(a))
+    g.close()
+
+
+@pytest.mark.parametrize("nrhs", [1, 16])
+def test_ir_reaches_fp64_accuracy_kappa_1e2(mtd, nrhs):
+    n, tile = 2048, 512
+    a = mixed.spd_kappa(n, 1e2, 5)
+    b = mixed.rhs(n, nrhs, 6)
+    s = mtd.SpdSolver(n, tile, mtd.PREC_TF32)
+    assert s.factor(to_dev(a)) == 0
+    xd = _dev_rect(np.zeros((n, nrhs)))
+    st = s.solve(_dev_rect(b), xd, method=mtd.REFINE_IR, tol=1e-13, max_iter=40)
+    x = _host_rect(xd)
+    assert st["converged"] and st["backward_error"] <= 1e-13
+    assert 1 < st["iterations"] <= 40
+    assert mixed.backward_error(a, x, b) <= 2e-13  # recomputed on the host in FP64
+    assert mixed.forward_error(x, mixed.solve_fp64(a, b)) <= 1e2 * 1e-12
+    s.close()
+
+
+def test_fp64_solver_one_solve(mtd):
+    n, tile = 2048, 512
+    a = mixed.spd_kappa(n, 1e2, 8)
+    b = mixed.rhs(n, 4, 9)
+    s = mtd.SpdSolver(n, tile, mtd.PREC_FP64)
+    assert s.factor(to_dev(a)) == 0
+    xd = _dev_rect(np.zeros((n, 4)))
+    st = s.solve(_dev_rect(b), xd, method=mtd.REFINE_NONE, tol=1e-13)
+    x = _host_rect(xd)
+    assert st["backward_error"] <= 1e-14
+    assert mixed.forward_error(x, mixed.solve_fp64(a, b)) <= 1e-12
+    s.close()
+
+
+def test_gmres_ir_kappa_1e5(mtd):
+    n, tile = 2048, 512
+    a = mixed.spd_kappa(n, 1e5, 10)
+    b = mixed.rhs(n, 1, 11)
+    s = mtd.SpdSolver(n, tile, mtd.PREC_TF32)
+    assert s.factor(to_dev(a)) == 0
+    xd = _dev_rect(np.zeros((n, 1)))
+    st = s.solve(_dev_rect(b), xd, method=mtd.REFINE_GMRES_IR, tol=1e-13, max_iter=20)
+    x = _host_rect(xd)
+    assert st["converged"] and st["backward_error"] <= 1e-13, st
+    assert mixed.backward_error(a, x, b) <= 2e-13
+    assert mixed.forward_error(x, mixed.solve_fp64(a, b)) <= 1e5 * 1e-12
+    s.close()
+
+
+def test_plain_ir_reports_non_convergence_honestly(mtd):
+    # kappa 1e5 with a TF32 factor: kappa * u_TF32 >> 1, plain IR cannot converge; the
+    # solver must say so rather than claim the tolerance.  The unshifted TF32
+    # factorisation may break down (non-positive pivot, reported with its column); a
+    # diagonal shift of a few TF32 roundoffs times ||A|| keeps it positive definite.
+    n, tile = 1024, 512
+    a = mixed.spd_kappa(n, 1e5, 12)
+    b = mixed.rhs(n, 1, 13)
+    s = mtd.SpdSolver(n, tile, mtd.PREC_TF32)
+    try:
+        s.factor(to_dev(a))
+    except mtd.MtdError as e:
+        assert e.status == 5 and 1 <= e.info <= n
+    shift = 4 * 2.0 ** -11 * np.abs(a).sum(axis=1).max()
+    assert s.factor(to_dev(a), shift=shift) == 0
+    xd = _dev_rect(np.zeros((n, 1)))
+    st = s.solve(_dev_rect(b), xd, method=mtd.REFINE_IR, tol=1e-13, max_iter=8)
+    x = _host_rect(xd)
+    assert st["converged"] == (st["backward_error"] <= 1e-13)
+    assert abs(mixed.backward_error(a, x, b) - st["backward_error"]) <= 0.05 * st["backward_error"] + 1e-15
+    s.close()
+
+
+def test_solver_argument_checks(mtd):
+    with pytest.raises(mtd.MtdError):
+        mtd.SpdSolver(1000, 100, mtd.PREC_TF32)  # tile must be a multiple of 64
+    s = mtd.SpdSolver(512, 128, mtd.PREC_TF32)
+    xd = _dev_rect(np.zeros((512, 1)))
+    with pytest.raises(mtd.MtdError) as e:
+        s.solve(xd, xd)  # not factored yet
+    assert e.value.status == 2
+    s.close()
