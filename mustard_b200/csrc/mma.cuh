@@ -71,10 +71,11 @@ __device__ __forceinline__ uint32_t to_tf32(float x) {
     return r;
 }
 
-// TF32 product with FP32 accumulation.  The FP32 operand bits go to the tensor core as they
-// are: it reads the TF32 part (sign, exponent, top 10 mantissa bits), i.e. truncates.  A
-// cvt.rna per fragment element would round to nearest instead, but costs six instructions
-// per MMA and made the FP32-storage GEMM issue-bound at a third of the TF32 peak.
+// TF32 product with FP32 accumulation.  The operand bits go to the tensor core as they are:
+// it reads the TF32 part (sign, exponent, top 10 mantissa bits).  The engine rounds each
+// fragment element to nearest once, when it is read from shared memory (frag_round), so a
+// fragment reused by several MMAs is converted once; rounding inside every MMA cost six
+// conversions per MMA and left the FP32-storage GEMM issue-bound at a third of the peak.
 __device__ __forceinline__ void mma_16x8x8(float (&d)[4], const float (&a)[4], const float (&b)[2]) {
     asm volatile(
         "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
@@ -113,6 +114,19 @@ __device__ __forceinline__ void mma_16x8x8_x3(float (&d)[4], const float (&a)[4]
         "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
         : "r"(ah[0]), "r"(ah[1]), "r"(ah[2]), "r"(ah[3]), "r"(bh[0]), "r"(bh[1]));
+}
+
+// Fragment element as the tensor core should see it: FP64 unchanged; single TF32 products
+// round to nearest TF32 (a truncated operand biases every product towards zero, and those
+// errors add up linearly along a long update chain); the split mode keeps all FP32 bits.
+template <int SPLIT>
+__device__ __forceinline__ double frag_round(double x) {
+    return x;
+}
+template <int SPLIT>
+__device__ __forceinline__ float frag_round(float x) {
+    if constexpr (SPLIT == 3) return x;
+    else return __uint_as_float(to_tf32(x));
 }
 
 template <int SPLIT>
@@ -250,21 +264,21 @@ struct BlockMmaT {
             for (int j = 0; j < FN; ++j) {
                 const int n = wn0 + j * 8 + g;
                 if (BL == kBNContig) {
-                    bf[j][0] = Bs[(ks + t) * LDB + n];
-                    bf[j][1] = Bs[(ks + t + 4) * LDB + n];
+                    bf[j][0] = frag_round<SPLIT>(Bs[(ks + t) * LDB + n]);
+                    bf[j][1] = frag_round<SPLIT>(Bs[(ks + t + 4) * LDB + n]);
                 } else {
-                    bf[j][0] = Bs[n * LDB + ks + t];
-                    bf[j][1] = Bs[n * LDB + ks + t + 4];
+                    bf[j][0] = frag_round<SPLIT>(Bs[n * LDB + ks + t]);
+                    bf[j][1] = frag_round<SPLIT>(Bs[n * LDB + ks + t + 4]);
                 }
             }
 #pragma unroll
             for (int i = 0; i < FM; ++i) {
                 const int m = wm0 + i * 16 + g;
                 T af[4];
-                af[0] = As[(ks + t) * LDA + m];
-                af[1] = As[(ks + t) * LDA + m + 8];
-                af[2] = As[(ks + t + 4) * LDA + m];
-                af[3] = As[(ks + t + 4) * LDA + m + 8];
+                af[0] = frag_round<SPLIT>(As[(ks + t) * LDA + m]);
+                af[1] = frag_round<SPLIT>(As[(ks + t) * LDA + m + 8]);
+                af[2] = frag_round<SPLIT>(As[(ks + t + 4) * LDA + m]);
+                af[3] = frag_round<SPLIT>(As[(ks + t + 4) * LDA + m + 8]);
 #pragma unroll
                 for (int j = 0; j < FN; ++j) mma_op<SPLIT>(acc[i][j], af, bf[j]);
             }

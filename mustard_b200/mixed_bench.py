@@ -96,7 +96,7 @@ DEFAULT_VARIANTS = [
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=32768)
-    ap.add_argument("--tile", type=int, default=1024)
+    ap.add_argument("--tile", type=int, default=1536)
     ap.add_argument("--kappas", default="1e2,1e5,1e8")
     ap.add_argument("--nrhs", default="1,16")
     ap.add_argument("--tol", type=float, default=1e-13)

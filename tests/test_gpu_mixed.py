@@ -54,6 +54,33 @@ def test_ir_reaches_fp64_accuracy_kappa_1e2(mtd, nrhs):
     s.close()
 
 
+@pytest.mark.parametrize("prec,n,nrhs", [("fp64", 1000, 3), ("tf32", 1000, 1), ("fp32", 1217, 7)])
+def test_ragged_sizes_and_rhs_groups(mtd, prec, n, nrhs):
+    """n not a multiple of the 64-row solve blocks (partial last block in the triangular
+    solves and the symmetric residual product) and right-hand-side counts in each group."""
+    p = {"fp64": mtd.PREC_FP64, "tf32": mtd.PREC_TF32, "fp32": mtd.PREC_FP32}[prec]
+    a = mixed.spd_kappa(n, 1e2, 21)
+    b = mixed.rhs(n, nrhs, 22)
+    s = mtd.SpdSolver(n, 256, p)
+    assert s.factor(to_dev(a)) == 0
+    xd = _dev_rect(np.zeros((n, nrhs)))
+    method = mtd.REFINE_NONE if prec == "fp64" else mtd.REFINE_IR
+    st = s.solve(_dev_rect(b), xd, method=method, tol=1e-13, max_iter=40)
+    x = _host_rect(xd)
+    bound = 1e-14 if prec == "fp64" else 1e-13
+    assert st["backward_error"] <= bound, st
+    assert mixed.backward_error(a, x, b) <= 2 * bound
+    assert mixed.forward_error(x, mixed.solve_fp64(a, b)) <= 1e2 * 1e-12
+    # factoring again reuses the buffers (whose upper triangle the solves use): same answer
+    # (to rounding: the FP64 residual sums with atomics, so its last bits vary run to run)
+    assert s.factor(to_dev(a)) == 0
+    xd2 = _dev_rect(np.zeros((n, nrhs)))
+    st2 = s.solve(_dev_rect(b), xd2, method=method, tol=1e-13, max_iter=40)
+    assert abs(st2["iterations"] - st["iterations"]) <= 1 and st2["backward_error"] <= bound
+    assert mixed.forward_error(_host_rect(xd2), x) <= 1e-12
+    s.close()
+
+
 def test_fp64_solver_one_solve(mtd):
     n, tile = 2048, 512
     a = mixed.spd_kappa(n, 1e2, 8)
