@@ -14,6 +14,9 @@ roofline    = the persistent kernel against the FP64 tensor-core (DMMA) peak mea
               reported beside it).
 cpu_baseline= the oracle's restatement of the reference's tiled algorithm (scipy /
               OpenBLAS tile calls on all host cores) on a bounded sample.
+mixed_ir    = time-to-solution of an FP64-accurate SPD solve at the same N (rank 0, after
+              the timed steps): plain FP64 Cholesky + solve against a TF32 tensor-core
+              factor + FP64 iterative refinement to normwise backward error 1e-13.
 
 `--impl reference` times that CPU implementation alone (rank 0; other ranks exit 0).
 Multi-GPU: the path does not shard, so `--gpus N` runs N independent replicas
@@ -171,6 +174,8 @@ def main():
     ap.add_argument("--cpu-tile", type=int, default=1000)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer measurement")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision + IR comparison")
+    ap.add_argument("--mixed-kappa", type=float, default=1e2)
     ap.add_argument("--trace", action="store_true", help="record per-item traces (adds busy fraction)")
     ap.add_argument("--only", choices=["lu", "chol"], default=None,
                     help="time one factorisation only (profiling runs; the metric needs both)")
@@ -335,6 +340,28 @@ def main():
                           f"({tlu:.1f} s + {tch:.1f} s): the oracle's restatement of the reference's "
                           "task list with scipy/OpenBLAS tile calls, all host cores")}
 
+    # FP64-accurate solve of A x = b at the same N: plain FP64 Cholesky + one solve against a
+    # TF32 factor + FP64 iterative refinement to backward error 1e-13 (wall time with the
+    # device synchronised on both sides; best of two; outside the timed region above).
+    mixed = None
+    if rank == 0 and not args.no_mixed:
+        from mustard_b200 import mixed_bench
+        recs = mixed_bench.run_case(n, args.tile_chol, args.mixed_kappa, 1, args.seed,
+                                    [(mtd.PREC_TF32, mtd.REFINE_IR, 0.0)], 1e-13, 30, 2)
+        fp64, lp = recs[0], recs[1]
+        mixed = {
+            "workload": f"SPD A = B B^T/N + alpha I (kappa {args.mixed_kappa:g}), N={n}, 1 RHS b ~ N(0,1), "
+                        f"tile {args.tile_chol}",
+            "unit": "TFLOP/s (FP64-equivalent: (N^3/3 + 2 N^2) / time-to-solution)",
+            "fp64": {"time_to_solution_ms": fp64["time_to_solution_ms"], "tflops": fp64["fp64_equiv_tflops"],
+                     "backward_error": fp64["backward_error"]},
+            "tf32_ir": {"time_to_solution_ms": lp.get("time_to_solution_ms"), "tflops": lp.get("fp64_equiv_tflops"),
+                        "iterations": lp.get("iterations"), "backward_error": lp.get("backward_error"),
+                        "forward_error_vs_fp64": lp.get("forward_error_vs_fp64"),
+                        "factor_ms": lp.get("factor_ms"), "solve_ms": lp.get("solve_ms")},
+            "ratio_vs_fp64": lp.get("ratio_vs_fp64"),
+        }
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
@@ -345,7 +372,7 @@ def main():
                        "lu_input": "U[-1,1) + N*I", "chol_input": "B B^T/N + I, B=U[-1,1)",
                        "parallelism": f"replicas{world}" if world > 1 else "1 GPU",
                        "l2": "inputs (4.6 GB each) larger than the 126 MB L2"},
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "mixed_ir": mixed,
             "clocks": clocks.summary(),
             "gpu_launches": args.steps * (1 if args.only else 2) * launches_per_run,
             "wall_s_timed": wall1 - wall0,

@@ -292,6 +292,31 @@ int mtd_batch_solve(mtd_batch *b, const double *const *dA, const int64_t *lda, v
                     const int *nrhs, int method, double tol, int max_iter, void *stream, mtd_batch_solve_stats *stats);
 int mtd_batch_destroy(mtd_batch *b);
 
+/* ---- Cholesky adjoint (no counterpart in the reference) ----
+ *
+ * Reverse-mode derivative of A = L L^T: given the factor L and Lbar = dLoss/dL (lower
+ * triangles), overwrite Lbar's lower triangle with Abar = dLoss/dA, the gradient with
+ * respect to the lower triangle of A (all a Cholesky factorisation reads; the symmetric
+ * gradient is (Abar + Abar^T) / 2 with the diagonal kept).  A reverse sweep over the tiled
+ * factorisation's block columns (tile 64 or 128) with its own TRSM / GEMM / diagonal-
+ * adjoint tasks, run by the persistent scheduler; many matrices of different sizes go in
+ * one merged task graph and one launch.  MTD_PREC_FP64: double matrices; MTD_PREC_FP32:
+ * float matrices with FP32-accurate (split-TF32) tensor-core products.  L is only read (the
+ * factor of a forward pass, or recomputed); the strict upper triangles are not touched. */
+typedef struct mtd_adjoint mtd_adjoint;
+
+int mtd_adjoint_create(mtd_adjoint **out, int count, const int64_t *n, int64_t tile, int prec);
+int mtd_adjoint_num_tasks(const mtd_adjoint *a);
+/* Stream-ordered; dL[m] and dLbar[m] are distinct device matrices of size n[m]. */
+int mtd_adjoint_run(mtd_adjoint *a, void *const *dL, const int64_t *ldl, void *const *dLbar, const int64_t *ldlb,
+                    void *stream);
+/* Wait for the last run; elapsed_ms (nullable) = its device time. */
+int mtd_adjoint_status(mtd_adjoint *a, double *elapsed_ms);
+int mtd_adjoint_destroy(mtd_adjoint *a);
+/* One matrix, synchronous. */
+int mtd_cholesky_adjoint(int prec, void *dL, int64_t ldl, void *dLbar, int64_t ldlb, int64_t n, int64_t tile,
+                         void *stream);
+
 /* ---- inputs: device generators (the reference builds its input on the host,
  *      include/gen.h:23-38; these make the seeded inputs of the benchmark shapes) ---- */
 int mtd_generate(double *dA, int64_t n, int64_t lda, int which, uint64_t seed, double alpha,

@@ -364,6 +364,60 @@ class Batch:
             pass
 
 
+class CholeskyAdjoint:
+    """Blocked Cholesky adjoint (mtd_adjoint_*): for factors L_m (lower) and Lbar_m =
+    dLoss/dL_m, overwrite each Lbar_m's lower triangle with Abar_m = dLoss/dA_m (gradient
+    with respect to the lower triangle of A_m).  Many matrices of different sizes run as
+    one merged reverse task graph in one persistent launch.  Matrices are column-major
+    CUDA tensors: float64 for PREC_FP64, float32 for PREC_FP32 (split-TF32 products)."""
+
+    def __init__(self, sizes, tile=128, prec=_capi.PREC_FP64):
+        self._lib = lib()
+        self.count = len(sizes)
+        n = (ctypes.c_int64 * self.count)(*sizes)
+        h = ctypes.c_void_p()
+        _capi.check(self._lib.mtd_adjoint_create(ctypes.byref(h), self.count, n, tile, prec))
+        self._h, self.sizes, self.tile, self.prec = h, list(sizes), tile, prec
+
+    def num_tasks(self):
+        return self._lib.mtd_adjoint_num_tasks(self._h)
+
+    def run(self, factors, lbars, stream=None):
+        """Stream-ordered; returns immediately (wait with status())."""
+        pl, ll = Batch._ptrs(factors)
+        pb, lb = Batch._ptrs(lbars)
+        self._keep = (factors, lbars)
+        _capi.check(self._lib.mtd_adjoint_run(self._h, pl, ll, pb, lb, _stream_handle(stream)))
+
+    def status(self):
+        """Wait for the last run; returns its device time in ms."""
+        ms = ctypes.c_double(0.0)
+        _capi.check(self._lib.mtd_adjoint_status(self._h, ctypes.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.mtd_adjoint_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def cholesky_adjoint(factor, lbar, tile=128, stream=None):
+    """One matrix, synchronous: ``lbar``'s lower triangle becomes dLoss/dA (see
+    CholeskyAdjoint).  Both column-major CUDA tensors of the same dtype."""
+    import torch
+    prec = _capi.PREC_FP64 if factor.dtype == torch.float64 else _capi.PREC_FP32
+    (pl,), (ll,) = Batch._ptrs([factor])
+    (pb,), (lb,) = Batch._ptrs([lbar])
+    _capi.check(lib().mtd_cholesky_adjoint(prec, ctypes.c_void_p(pl), ll, ctypes.c_void_p(pb), lb, factor.shape[0],
+                                           tile, _stream_handle(stream)))
+
+
 def _one_call(kind, a, tile, stream):
     ptr, n, ld = _matrix_ptr(a)
     info = ctypes.c_int(0)

@@ -57,6 +57,12 @@ SIGNATURES = {
     "mtd_batch_solve": (_i, [_vp, _pp, _pi64, _pp, _pi64, _pp, _pi64, _pp, _pi64, ctypes.POINTER(_i), _i, _d, _i, _vp,
                              ctypes.POINTER(BatchSolveStats)]),
     "mtd_batch_destroy": (_i, [_vp]),
+    "mtd_adjoint_create": (_i, [ctypes.POINTER(_vp), _i, _pi64, _i64, _i]),
+    "mtd_adjoint_num_tasks": (_i, [_vp]),
+    "mtd_adjoint_run": (_i, [_vp, _pp, _pi64, _pp, _pi64, _vp]),
+    "mtd_adjoint_status": (_i, [_vp, ctypes.POINTER(_d)]),
+    "mtd_adjoint_destroy": (_i, [_vp]),
+    "mtd_cholesky_adjoint": (_i, [_i, _vp, _i64, _vp, _i64, _i64, _i64, _vp]),
     "mtd_graph_set_precision": (_i, [_vp, _i]),
     "mtd_run_f32": (_i, [_vp, _vp, _i64, _vp, ctypes.POINTER(_i)]),
     "mtd_solver_create": (_i, [ctypes.POINTER(_vp), _i64, _i64, _i]),
@@ -103,7 +109,7 @@ def lib():
     if _lib is None:
         if not os.path.exists(_LIB_PATH):
             raise ImportError(f"mustard_b200 native library missing: {_LIB_PATH} "
-                              "(build it with `python -m mustard_b200.build`)")
+                              "(build it with `python mustard_b200/build.py`)")
         handle = ctypes.CDLL(_LIB_PATH)
         for name, (res, args) in SIGNATURES.items():
             fn = getattr(handle, name)

@@ -18,7 +18,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
                      "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]
 
-LIB_SOURCES = ["runtime.cu", "gen.cu", "dag.cpp", "solver.cu", "batch.cu"]
+LIB_SOURCES = ["runtime.cu", "gen.cu", "dag.cpp", "solver.cu", "batch.cu", "adjoint.cu"]
 CLI_PROGRAMS = {"lu_mustard": "lu_mustard.cpp", "cholesky_mustard": "cholesky_mustard.cpp"}
 
 

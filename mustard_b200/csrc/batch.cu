@@ -23,7 +23,7 @@
 
 namespace mtd {
 int launch_run(const RunArgs &a, const int *deps_init, const int *roots, int n_roots, long long total_items,
-               int prec, bool vec2, int grid, cudaStream_t s);
+               int prec, bool vec2, int grid, cudaStream_t s, bool adjoint);
 }
 using namespace mtd;
 
@@ -505,7 +505,7 @@ int mtd_batch_factor(mtd_batch *b, void *const *dA, const int64_t *lda, void *st
     a.mats = b->d_mats;
     a.mat_info = b->d_info;
     a.mat_done_ns = b->d_done;
-    int rc = launch_run(a, b->d_deps_init, b->d_roots, b->n_roots, b->total_items, b->prec, vec2, b->sms, s);
+    int rc = launch_run(a, b->d_deps_init, b->d_roots, b->n_roots, b->total_items, b->prec, vec2, b->sms, s, false);
     if (rc) return rc;
     if (cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, s) != cudaSuccess) return MTD_ERR_CUDA;
     b->last_stream = s;

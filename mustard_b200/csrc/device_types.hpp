@@ -18,6 +18,17 @@ constexpr int kNestTile = 128;  // default sub-tile edge of a nested diagonal fa
 // Device-side operation codes: the public mtd_op values plus a zero-work join.
 constexpr int kOpJoin = 100;
 
+// Cholesky adjoint operations (device tasks of the reverse sweep; see adjoint_ops.cuh).
+constexpr int kOpAdjTrsm = 20;    // C(m x n) := C * L^-1, L = n x n lower at (ar, ac) of the factor
+constexpr int kOpAdjGemmNN = 21;  // C(m x n) -= A(m x k) * B(k x n); A in the adjoint (pad 0) or Y (pad 2), B in L
+constexpr int kOpAdjGemmTN = 22;  // C(m x n) -= A^T * B, A stored k x m in the adjoint, B (k x n) in L;
+                                  // pad & 1: lower triangle of C only
+constexpr int kOpAdjPotrf = 23;   // diagonal tile (m x m) adjoint at (cr, cc); writes Y rows cr.., columns 0..m
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+constexpr bool is_adjoint_op(int op) { return op >= kOpAdjTrsm && op <= kOpAdjPotrf; }
+
 // One device task.  Geometry is in matrix elements (row, column origins of each block
 // inside the column-major matrix), so a task can cover a whole tile or a sub-tile of a
 // nested diagonal factorisation.

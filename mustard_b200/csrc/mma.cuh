@@ -146,8 +146,12 @@ struct SmemPad {
     static constexpr int a_mod = sizeof(T) == 8 ? 16 : 32;
 };
 
+// A operand layout: element (m, k) at A[m + k lda] (kAMContig, column-major A) or at
+// A[k + m lda] (kAKContig: the transpose of a column-major block, for C -= X^T Y).
+enum { kAMContig = 0, kAKContig = 1 };
+
 template <typename T, int BM, int BN, int WARPS_M, int WARPS_N, int BL, int VEC, int STAGES = 3, int BK_ = 16,
-          int SPLIT = 1>
+          int SPLIT = 1, int AL = kAMContig>
 struct BlockMmaT {
     static constexpr int BK = BK_;
     static constexpr int EPC = 16 / int(sizeof(T));  // elements per 16-byte copy
@@ -155,15 +159,17 @@ struct BlockMmaT {
     static constexpr int WN = BN / WARPS_N;
     static constexpr int FM = WM / 16;
     static constexpr int FN = WN / 8;
-    static constexpr int LDA = BM + SmemPad<T>::a;
+    // m-contiguous A is staged [k][m] (stride LDA); k-contiguous A is staged [m][k] with
+    // the k-contiguous B padding, which keeps its fragment reads conflict-free the same way
+    static constexpr int LDA = (AL == kAMContig) ? BM + SmemPad<T>::a : BK + SmemPad<T>::bk;
     static constexpr int LDB = (BL == kBNContig) ? BN + SmemPad<T>::a : BK + SmemPad<T>::bk;
-    static constexpr int A_STAGE = BK * LDA;
+    static constexpr int A_STAGE = (AL == kAMContig) ? BK * LDA : BM * LDA;
     static constexpr int B_STAGE = (BL == kBNContig) ? BK * LDB : BN * LDB;
     static constexpr int SMEM_ELEMS = STAGES * (A_STAGE + B_STAGE);
     static constexpr int SMEM_BYTES = SMEM_ELEMS * int(sizeof(T));
     static_assert(WARPS_M * WARPS_N * 32 == kThreads, "one warp tile per warp of the CTA");
     static_assert(FM >= 1 && FN >= 1 && WM % 16 == 0 && WN % 8 == 0, "warp tile");
-    static_assert(LDA % SmemPad<T>::a_mod == SmemPad<T>::a, "bank-conflict-free padding (A)");
+    static_assert(AL != kAMContig || LDA % SmemPad<T>::a_mod == SmemPad<T>::a, "bank-conflict-free padding (A)");
     static_assert((LDA * int(sizeof(T))) % 16 == 0 && (LDB * int(sizeof(T))) % 16 == 0, "16-byte rows");
     static_assert(BK % 8 == 0 && BM % EPC == 0 && BN % EPC == 0 && BK % EPC == 0, "copy granularity");
 
@@ -181,6 +187,29 @@ struct BlockMmaT {
     // ---- global -> shared stage loads ----
     __device__ __forceinline__ static void load_a(T *As, const T *A, int64_t lda, int M, int K, int k0) {
         const int tid = threadIdx.x;
+        if constexpr (AL == kAKContig) {
+            if (VEC == 2) {
+                constexpr int CH = BM * (BK / EPC);
+#pragma unroll
+                for (int c = tid; c < CH; c += kThreads) {
+                    const int m = c / (BK / EPC);
+                    const int k = EPC * (c % (BK / EPC));
+                    const int kk = k0 + k;
+                    const bool ok = m < M && kk < K;
+                    const T *src = ok ? A + kk + int64_t(m) * lda : A;
+                    cp_async16(As + m * LDA + k, src, ok);
+                }
+            } else {
+                constexpr int EL = BM * BK;
+                for (int e = tid; e < EL; e += kThreads) {
+                    const int m = e / BK;
+                    const int k = e % BK;
+                    const int kk = k0 + k;
+                    As[m * LDA + k] = (m < M && kk < K) ? ld_cg(A + kk + int64_t(m) * lda) : T(0);
+                }
+            }
+            return;
+        }
         if (VEC == 2) {
             constexpr int CH = BK * (BM / EPC);
 #pragma unroll
@@ -275,10 +304,17 @@ struct BlockMmaT {
             for (int i = 0; i < FM; ++i) {
                 const int m = wm0 + i * 16 + g;
                 T af[4];
-                af[0] = frag_round<SPLIT>(As[(ks + t) * LDA + m]);
-                af[1] = frag_round<SPLIT>(As[(ks + t) * LDA + m + 8]);
-                af[2] = frag_round<SPLIT>(As[(ks + t + 4) * LDA + m]);
-                af[3] = frag_round<SPLIT>(As[(ks + t + 4) * LDA + m + 8]);
+                if constexpr (AL == kAMContig) {
+                    af[0] = frag_round<SPLIT>(As[(ks + t) * LDA + m]);
+                    af[1] = frag_round<SPLIT>(As[(ks + t) * LDA + m + 8]);
+                    af[2] = frag_round<SPLIT>(As[(ks + t + 4) * LDA + m]);
+                    af[3] = frag_round<SPLIT>(As[(ks + t + 4) * LDA + m + 8]);
+                } else {
+                    af[0] = frag_round<SPLIT>(As[m * LDA + ks + t]);
+                    af[1] = frag_round<SPLIT>(As[(m + 8) * LDA + ks + t]);
+                    af[2] = frag_round<SPLIT>(As[m * LDA + ks + t + 4]);
+                    af[3] = frag_round<SPLIT>(As[(m + 8) * LDA + ks + t + 4]);
+                }
 #pragma unroll
                 for (int j = 0; j < FN; ++j) mma_op<SPLIT>(acc[i][j], af, bf[j]);
             }

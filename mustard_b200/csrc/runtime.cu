@@ -84,7 +84,11 @@ int smem_setup(int device) {
             cudaFuncSetAttribute(persistent_kernel<VEC, float, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  bytes) != cudaSuccess ||
             cudaFuncSetAttribute(task_kernel<VEC, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
-                cudaSuccess)
+                cudaSuccess ||
+            cudaFuncSetAttribute(persistent_kernel<VEC, double, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 bytes) != cudaSuccess ||
+            cudaFuncSetAttribute(persistent_kernel<VEC, float, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 bytes) != cudaSuccess)
             return MTD_ERR_CUDA;
         done[device] = true;
     }
@@ -396,7 +400,7 @@ namespace mtd {
 // Reset, seed and launch one persistent run (shared by graphs, batches and the
 // no-allocation entry point's sibling paths).  Stream-ordered; no host synchronisation.
 int launch_run(const RunArgs &a, const int *deps_init, const int *roots, int n_roots, long long total_items,
-               int prec, bool vec2, int grid, cudaStream_t s) {
+               int prec, bool vec2, int grid, cudaStream_t s, bool adjoint) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return MTD_ERR_NO_DEVICE;
     int rc = smem_setup<2>(dev);
@@ -409,6 +413,13 @@ int launch_run(const RunArgs &a, const int *deps_init, const int *roots, int n_r
     const int bytes = kOpSmemBytes();
     const bool fp64 = prec == MTD_PREC_FP64;
     const bool x3 = prec == MTD_PREC_FP32;
+    if (adjoint) {  // FP64, or FP32 with split-TF32 (FP32-accurate) products
+        if (fp64 && vec2) persistent_kernel<2, double, 1, true><<<grid, kThreads, bytes, s>>>(a);
+        else if (fp64) persistent_kernel<1, double, 1, true><<<grid, kThreads, bytes, s>>>(a);
+        else if (vec2) persistent_kernel<2, float, 3, true><<<grid, kThreads, bytes, s>>>(a);
+        else persistent_kernel<1, float, 3, true><<<grid, kThreads, bytes, s>>>(a);
+        return cudaGetLastError() == cudaSuccess ? MTD_OK : MTD_ERR_CUDA;
+    }
     if (fp64 && vec2) persistent_kernel<2, double><<<grid, kThreads, bytes, s>>>(a);
     else if (fp64) persistent_kernel<1, double><<<grid, kThreads, bytes, s>>>(a);
     else if (x3 && vec2) persistent_kernel<2, float, 3><<<grid, kThreads, bytes, s>>>(a);
@@ -432,7 +443,7 @@ static int run_persistent(mtd_graph *g, void *dA, int64_t lda, void *stream, int
     const int grid = g->num_sms;
     g->last_grid = grid;
     const int rc = launch_run(a, g->d_deps_init, g->d_roots, g->n_roots, g->total_items, g->prec,
-                              use_vec2(g, dA, lda), grid, s);
+                              use_vec2(g, dA, lda), grid, s, false);
     if (rc) return rc;
     if (cudaMemcpyAsync(g->h_ctl, g->d_ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, s) != cudaSuccess)
         return MTD_ERR_CUDA;

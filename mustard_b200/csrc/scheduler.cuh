@@ -18,6 +18,7 @@
 #pragma once
 
 #include "device_types.hpp"
+#include "adjoint_ops.cuh"
 #include "tile_ops.cuh"
 
 namespace mtd {
@@ -133,8 +134,11 @@ __device__ __forceinline__ void complete_item(const RunArgs &p, int task) {
 // Element type of the matrix a run factors: double (the reference's FP64 arithmetic) or
 // float (low-precision Cholesky factor of the mixed-precision solver: SPLIT = 1 TF32
 // products, SPLIT = 3 FP32-accurate split-TF32 products).
-template <int VEC, typename T, int SPLIT = 1>
+// ADJ: the kernel instance that runs the Cholesky adjoint's task graphs (its operations
+// only), so the factorisation kernels keep their own register allocation.
+template <int VEC, typename T, int SPLIT = 1, bool ADJ = false>
 __device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int item, void *smem) {
+    if constexpr (ADJ) return dispatch_adjoint<T, VEC, SPLIT>(p, t, item, smem);
     const MatCtx m = mat_ctx<T>(p, t);
     if constexpr (sizeof(T) == 8) {
         switch (t.op) {
@@ -161,7 +165,7 @@ __device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int 
     return MTD_ERR_INVALID_ARG;
 }
 
-template <int VEC, typename T, int SPLIT = 1>
+template <int VEC, typename T, int SPLIT = 1, bool ADJ = false>
 __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const RunArgs p) {
     extern __shared__ __align__(128) double smem[];
     __shared__ int s_cmd, s_task, s_item;
@@ -184,7 +188,7 @@ __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const RunArgs p
 #pragma unroll
             for (int w = 0; w < int(sizeof(DevTask) / sizeof(int4)); ++w) dst[w] = __ldg(src + w);
         }
-        const int st = dispatch<VEC, T, SPLIT>(p, t, item, smem);
+        const int st = dispatch<VEC, T, SPLIT, ADJ>(p, t, item, smem);
         __syncthreads();
         if (threadIdx.x == 0) {
             if (st == 0) complete_item(p, task);

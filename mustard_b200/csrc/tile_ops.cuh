@@ -450,8 +450,12 @@ __device__ int op_syrk_ln(const RunArgs &p, const MatCtx &m, const DevTask &t, i
 constexpr int kOpSmemBytes() {
     constexpr int g1 = GemmMma<kBNContig, 2>::SMEM_BYTES;
     constexpr int g2 = GemmMma<kBKContig, 2>::SMEM_BYTES;
-    constexpr int diag = 3 * kNB * kDiagLd * 8;
-    constexpr int m = g1 > g2 ? g1 : g2;
+    // C -= A^T B of the Cholesky adjoint: both operands staged k-contiguous
+    constexpr int g3 = BlockMmaT<double, kGemmTile, kGemmTile, kGemmWarpsM, kGemmWarpsN, kBKContig, 2, MTD_GEMM_STAGES,
+                                 MTD_GEMM_BK, 1, kAKContig>::SMEM_BYTES;
+    constexpr int diag = 5 * kNB * kDiagLd * 8;  // the adjoint's diagonal block: five 64 x 64 blocks
+    constexpr int m12 = g1 > g2 ? g1 : g2;
+    constexpr int m = m12 > g3 ? m12 : g3;
     return m > diag ? m : diag;
 }
 

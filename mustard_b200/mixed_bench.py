@@ -1,6 +1,6 @@
 """Mixed-precision factor + FP64 refinement against the plain FP64 solve (one B200).
 
-    python -m mustard_b200.mixed_bench [--n 32768] [--tile 1024] [--kappas 1e2,1e5,1e8]
+    python -m mustard_b200.mixed_bench [--n 32768] [--tile 1536] [--kappas 1e2,1e5,1e8]
                                        [--nrhs 1,16] [--out results.jsonl]
 
 For each condition number kappa: A = B B^T / n + alpha I (B = U[-1,1), alpha = (4/3)/(kappa-1),
