@@ -298,7 +298,7 @@ int mtd_batch_destroy(mtd_batch *b);
  * triangles), overwrite Lbar's lower triangle with Abar = dLoss/dA, the gradient with
  * respect to the lower triangle of A (all a Cholesky factorisation reads; the symmetric
  * gradient is (Abar + Abar^T) / 2 with the diagonal kept).  A reverse sweep over the tiled
- * factorisation's block columns (tile 64 or 128) with its own TRSM / GEMM / diagonal-
+ * factorisation's block columns (tile 64, 128 or 256) with its own TRSM / GEMM / diagonal-
  * adjoint tasks, run by the persistent scheduler; many matrices of different sizes go in
  * one merged task graph and one launch.  MTD_PREC_FP64: double matrices; MTD_PREC_FP32:
  * float matrices with FP32-accurate (split-TF32) tensor-core products.  L is only read (the
@@ -312,6 +312,12 @@ int mtd_adjoint_run(mtd_adjoint *a, void *const *dL, const int64_t *ldl, void *c
                     void *stream);
 /* Wait for the last run; elapsed_ms (nullable) = its device time. */
 int mtd_adjoint_status(mtd_adjoint *a, double *elapsed_ms);
+/* Per-work-item trace of the next runs (records as mtd_graph_copy_trace's: start ns, end
+ * ns, SM, task << 32 | item); mtd_adjoint_task_op gives a task's operation (internal code:
+ * 20 X L^-1, 21 C -= A B, 22 C -= A^T B, 23 diagonal-tile adjoint). */
+int mtd_adjoint_set_trace(mtd_adjoint *a, int enable);
+long long mtd_adjoint_copy_trace(mtd_adjoint *a, unsigned long long *out, long long cap_records);
+int mtd_adjoint_task_op(const mtd_adjoint *a, int task);
 int mtd_adjoint_destroy(mtd_adjoint *a);
 /* One matrix, synchronous. */
 int mtd_cholesky_adjoint(int prec, void *dL, int64_t ldl, void *dLbar, int64_t ldlb, int64_t n, int64_t tile,

@@ -395,6 +395,29 @@ class CholeskyAdjoint:
         _capi.check(self._lib.mtd_adjoint_status(self._h, ctypes.byref(ms)))
         return ms.value
 
+    ADJOINT_OP_NAMES = {20: "X L^-1", 21: "C -= A B", 22: "C -= A^T B", 23: "diagonal adjoint"}
+
+    def set_trace(self, enable=True):
+        _capi.check(self._lib.mtd_adjoint_set_trace(self._h, int(enable)))
+        return self
+
+    def op_times(self):
+        """Per operation of the last traced run: items and summed / median item time (us)."""
+        import statistics
+        cap = 1 << 22
+        buf = (ctypes.c_ulonglong * (4 * cap))()
+        n = self._lib.mtd_adjoint_copy_trace(self._h, buf, cap)
+        if n < 0:
+            _capi.check(-n)
+        per = {}
+        for i in range(n):
+            s, e, task = buf[4 * i], buf[4 * i + 1], buf[4 * i + 3] >> 32
+            if e <= s:
+                continue
+            op = self._lib.mtd_adjoint_task_op(self._h, int(task))
+            per.setdefault(self.ADJOINT_OP_NAMES.get(op, op), []).append((e - s) * 1e-3)
+        return {k: {"items": len(v), "total_us": sum(v), "median_us": statistics.median(v)} for k, v in per.items()}
+
     def close(self):
         if getattr(self, "_h", None):
             self._lib.mtd_adjoint_destroy(self._h)

@@ -61,6 +61,9 @@ SIGNATURES = {
     "mtd_adjoint_num_tasks": (_i, [_vp]),
     "mtd_adjoint_run": (_i, [_vp, _pp, _pi64, _pp, _pi64, _vp]),
     "mtd_adjoint_status": (_i, [_vp, ctypes.POINTER(_d)]),
+    "mtd_adjoint_set_trace": (_i, [_vp, _i]),
+    "mtd_adjoint_copy_trace": (ctypes.c_longlong, [_vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_longlong]),
+    "mtd_adjoint_task_op": (_i, [_vp, _i]),
     "mtd_adjoint_destroy": (_i, [_vp]),
     "mtd_cholesky_adjoint": (_i, [_i, _vp, _i64, _vp, _i64, _i64, _i64, _vp]),
     "mtd_graph_set_precision": (_i, [_vp, _i]),

@@ -1,6 +1,6 @@
 """torch.autograd.Function over the scheduler's batched Cholesky and its blocked adjoint.
 
-    L = cholesky(A, tile=128, recompute=False)     # A: (n, n) or (B, n, n), SPD
+    L = cholesky(A, tile=256, recompute=False)     # A: (n, n) or (B, n, n), SPD
 
 Forward: one merged task graph factors every matrix of the batch (mtd_batch_*: FP64 for
 float64 input; FP32 storage with FP32-accurate split-TF32 products for float32).
@@ -45,7 +45,9 @@ def _stream():
 
 
 def _factor(a, tile):
-    """(B, n, n) SPD -> (B, n, n) lower factors (row-major), via one merged task graph."""
+    """(B, n, n) SPD -> (B, n, n) lower factors, via one merged task graph.  The result is a
+    transposed view of one contiguous buffer whose (column-major) storage is L itself, so
+    the adjoint reads it without a copy."""
     b, n = a.shape[0], a.shape[-1]
     prec = _prec(a.dtype)
     key = (b, n, tile, prec)
@@ -65,11 +67,14 @@ def _factor(a, tile):
     bad = [i for i in range(b) if info[i]]
     if bad:
         raise _capi.MtdError(_capi.ERR_NOT_POSITIVE_DEFINITE, info[bad[0]])
-    return w.transpose(-1, -2).tril()
+    L = w.transpose(-1, -2)
+    L.tril_()  # zero what is left of A above the diagonal, in w itself
+    return L
 
 
 def _adjoint(L, gl, tile):
-    """Abar (lower) for factors L and gradients gl, both (B, n, n) row-major."""
+    """Symmetric gradient dLoss/dA for factors L (as _factor returns them) and gradients
+    gl = dLoss/dL, both (B, n, n)."""
     b, n = L.shape[0], L.shape[-1]
     prec = _prec(L.dtype)
     key = (b, n, tile, prec)
@@ -79,13 +84,20 @@ def _adjoint(L, gl, tile):
         sizes = (ctypes.c_int64 * b)(*([n] * b))
         _capi.check(lib().mtd_adjoint_create(ctypes.byref(h), b, sizes, tile, prec))
         _adjoints[key] = h
-    lc = L.transpose(-1, -2).contiguous()           # column-major L
-    gc = gl.tril().transpose(-1, -2).contiguous()   # column-major Lbar, becomes Abar
+    lc = L.transpose(-1, -2)
+    if not lc.is_contiguous():
+        lc = lc.contiguous()
+    # gc's storage read column-major is tril(gl); the adjoint turns it into Abar, after which
+    # gc (row-major) is Abar^T with zeros below the diagonal
+    gc = gl.transpose(-1, -2).contiguous()
+    gc.triu_()
     pl, ll = _table(lc)
     pg, lg = _table(gc)
     _capi.check(lib().mtd_adjoint_run(h, pl, ll, pg, lg, _stream()))
     _capi.check(lib().mtd_adjoint_status(h, None))
-    return gc.transpose(-1, -2).tril()
+    grad = gc + gc.transpose(-1, -2)
+    grad.mul_(0.5)
+    return grad
 
 
 class CholeskyFunction(torch.autograd.Function):
@@ -103,12 +115,11 @@ class CholeskyFunction(torch.autograd.Function):
         (saved,) = ctx.saved_tensors
         L = _factor(saved, ctx.tile) if ctx.recompute else saved
         g3 = gl if ctx.batched else gl.unsqueeze(0)
-        abar = _adjoint(L, g3.to(L.dtype), ctx.tile)
-        grad = 0.5 * (abar + abar.transpose(-1, -2))
+        grad = _adjoint(L, g3.to(L.dtype), ctx.tile)
         return (grad if ctx.batched else grad[0]), None, None
 
 
-def cholesky(a, tile=128, recompute=False):
+def cholesky(a, tile=256, recompute=False):
     """Lower Cholesky factor of the SPD matrix (or stack) ``a`` on the task scheduler,
     differentiable through the blocked adjoint."""
     return CholeskyFunction.apply(a, tile, recompute)

@@ -48,6 +48,8 @@ struct mtd_adjoint {
     BatchMat *h_mats = nullptr;  // pinned staging
     int *d_info = nullptr;
     unsigned long long *d_done = nullptr;
+    unsigned long long *d_trace = nullptr;  // per-item records when tracing (4 words each)
+    std::vector<int> task_op;               // op of each device task (for trace readers)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaStream_t last_stream = nullptr;
     bool pending = false;
@@ -200,6 +202,7 @@ void release(mtd_adjoint *a) {
     cudaFree(a->d_mats);
     cudaFree(a->d_info);
     cudaFree(a->d_done);
+    cudaFree(a->d_trace);
     if (a->h_ctl) cudaFreeHost(a->h_ctl);
     if (a->h_mats) cudaFreeHost(a->h_mats);
     if (a->ev0) cudaEventDestroy(a->ev0);
@@ -213,7 +216,8 @@ extern "C" {
 int mtd_adjoint_create(mtd_adjoint **out, int count, const int64_t *n, int64_t tile, int prec) {
     if (!out) return MTD_ERR_INVALID_ARG;
     *out = nullptr;
-    if (count <= 0 || !n || (tile != 64 && tile != 128) || (prec != MTD_PREC_FP64 && prec != MTD_PREC_FP32))
+    if (count <= 0 || !n || (tile != 64 && tile != 128 && tile != 256) ||
+        (prec != MTD_PREC_FP64 && prec != MTD_PREC_FP32))
         return MTD_ERR_INVALID_ARG;
     int dev = 0, major = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return MTD_ERR_NO_DEVICE;
@@ -243,7 +247,15 @@ int mtd_adjoint_create(mtd_adjoint **out, int count, const int64_t *n, int64_t t
         a->y_ld.push_back(ld);
         y_total += ld * tile;
         a->max_blocks = std::max(a->max_blocks, cdiv(nm, kNB));
-        build_matrix(g, nm, tile, 3 * m);
+        GraphBuilder one;  // tile keys are per matrix: the matrices share no dependency
+        build_matrix(one, nm, tile, 3 * m);
+        const int base = static_cast<int>(g.tasks.size());
+        for (size_t t = 0; t < one.tasks.size(); ++t) {
+            g.tasks.push_back(one.tasks[t]);
+            std::vector<int> p = one.preds[t];
+            for (int &x : p) x += base;
+            g.preds.push_back(std::move(p));
+        }
     }
     const int nt = static_cast<int>(g.tasks.size());
     std::vector<int> succ, deps_init(nt), roots;
@@ -265,6 +277,7 @@ int mtd_adjoint_create(mtd_adjoint **out, int count, const int64_t *n, int64_t t
     a->n_dev = nt;
     a->n_roots = static_cast<int>(roots.size());
     a->total_items = a->qcap[0] + a->qcap[1];
+    for (const DevTask &d : g.tasks) a->task_op.push_back(d.op);
     if (!rc) rc = dalloc(&a->d_tasks, nt);
     if (!rc) rc = dalloc(&a->d_succ, succ.size());
     if (!rc) rc = dalloc(&a->d_deps_init, nt);
@@ -352,6 +365,8 @@ int mtd_adjoint_run(mtd_adjoint *a, void *const *dL, const int64_t *ldl, void *c
     r.mats = a->d_mats;
     r.mat_info = a->d_info;
     r.mat_done_ns = a->d_done;
+    r.trace = a->d_trace;
+    r.trace_cap = a->d_trace ? a->total_items : 0;
     int rc = launch_run(r, a->d_deps_init, a->d_roots, a->n_roots, a->total_items, a->prec, vec2, a->sms, s, true);
     if (rc) return rc;
     if (cudaEventRecord(a->ev1, s) != cudaSuccess ||
@@ -374,6 +389,29 @@ int mtd_adjoint_status(mtd_adjoint *a, double *elapsed_ms) {
     if (a->h_ctl->error) return a->h_ctl->error;
     if (a->h_ctl->tasks_done != a->n_dev) return MTD_ERR_TIMEOUT;
     return MTD_OK;
+}
+
+int mtd_adjoint_set_trace(mtd_adjoint *a, int enable) {
+    if (!a) return MTD_ERR_INVALID_ARG;
+    if (cudaDeviceSynchronize() != cudaSuccess) return MTD_ERR_CUDA;
+    cudaFree(a->d_trace);
+    a->d_trace = nullptr;
+    if (enable) return dalloc(&a->d_trace, size_t(4) * size_t(a->total_items));
+    return MTD_OK;
+}
+
+long long mtd_adjoint_copy_trace(mtd_adjoint *a, unsigned long long *out, long long cap_records) {
+    if (!a || !out || cap_records < 0) return -MTD_ERR_INVALID_ARG;
+    if (!a->d_trace) return -MTD_ERR_STATE;
+    const long long n = std::min<long long>(cap_records, a->total_items);
+    if (cudaMemcpy(out, a->d_trace, size_t(n) * 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return -MTD_ERR_CUDA;
+    return n;
+}
+
+int mtd_adjoint_task_op(const mtd_adjoint *a, int task) {
+    if (!a || task < 0 || task >= a->n_dev) return -MTD_ERR_INVALID_ARG;
+    return a->task_op[task];
 }
 
 int mtd_adjoint_destroy(mtd_adjoint *a) {

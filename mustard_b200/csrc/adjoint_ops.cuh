@@ -147,9 +147,10 @@ __device__ void adj_diag_block(const T *D, int64_t ldd, T *G, int64_t ldg, const
     }
 }
 
-// Adjoint of the m x m diagonal tile at (cr, cc) (m <= 128: one or two 64-blocks), the same
-// reverse sweep inside the tile over its 64-blocks; writes the tile's Sbar (lower) over
-// Dbar and Y = Sbar + Sbar^T (full m x m) to the Y workspace.
+// Adjoint of the m x m diagonal tile at (cr, cc) (m <= 256), the same reverse sweep inside
+// the tile over its 64-blocks; writes the tile's Sbar (lower) over Dbar and
+// Y = Sbar + Sbar^T (full m x m) to the Y workspace.  Products with the rows below a block
+// go in 64-row pieces (the engine's output edge).
 template <typename T, int VEC, int SPLIT>
 __device__ int op_adj_potrf(const RunArgs &p, const DevTask &t, void *smem) {
     using Mnn = PanelMma<kBKContig, VEC, T, SPLIT>;
@@ -165,11 +166,12 @@ __device__ int op_adj_potrf(const RunArgs &p, const DevTask &t, void *smem) {
     for (int b = s - 1; b >= 0; --b) {
         const int bo = b * kNB, bn = min(kNB, tn - bo), lo = bo + bn, below = tn - lo;
         if (below > 0) {
-            {  // X = G(below, b) W_b
+            for (int r0 = lo; r0 < tn; r0 += kNB) {  // X = G(below, b) W_b
+                const int mm = min(kNB, tn - r0);
                 Mnn e;
                 e.zero();
-                e.run(smem, G + lo + int64_t(bo) * ldg, ldg, W + bo, ldw, below, bn, bn);
-                e.store_to(G + lo + int64_t(bo) * ldg, ldg, below, bn);
+                e.run(smem, G + r0 + int64_t(bo) * ldg, ldg, W + bo, ldw, mm, bn, bn);
+                e.store_to(G + r0 + int64_t(bo) * ldg, ldg, mm, bn);
             }
             block_fence_sync();
             {  // Dbar_b -= tril(X^T D(below, b))
@@ -186,11 +188,12 @@ __device__ int op_adj_potrf(const RunArgs &p, const DevTask &t, void *smem) {
         for (int kb = 0; kb < bo; kb += kNB) {
             const int kn = min(kNB, bo - kb);
             if (below > 0) {
-                {  // G(below, k) -= X D(b, k)
+                for (int r0 = lo; r0 < tn; r0 += kNB) {  // G(below, k) -= X D(b, k)
+                    const int mm = min(kNB, tn - r0);
                     Mnn e;
                     e.zero();
-                    e.run(smem, G + lo + int64_t(bo) * ldg, ldg, D + bo + int64_t(kb) * ldd, ldd, below, kn, bn);
-                    e.sub_from(G + lo + int64_t(kb) * ldg, ldg, below, kn);
+                    e.run(smem, G + r0 + int64_t(bo) * ldg, ldg, D + bo + int64_t(kb) * ldd, ldd, mm, kn, bn);
+                    e.sub_from(G + r0 + int64_t(kb) * ldg, ldg, mm, kn);
                 }
                 block_fence_sync();
                 {  // G(b, k) -= X^T D(below, k)

@@ -60,7 +60,7 @@ def test_gp_loss_gradient_matches_finite_differences():
     assert np.max(np.abs(adjoint.symmetric(abar) - g)) <= 1e-10 * np.max(np.abs(g))
 
 
-@pytest.mark.parametrize("n,tile", [(64, 64), (128, 64), (200, 64), (256, 128), (300, 128), (77, 128)])
+@pytest.mark.parametrize("n,tile", [(64, 64), (128, 64), (200, 64), (256, 128), (300, 128), (77, 128), (600, 256)])
 def test_blocked_sweep_matches_closed_form(n, tile):
     a = _spd(n, 6 + n)
     L = np.linalg.cholesky(a)

@@ -33,7 +33,7 @@ def _rel(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
-@pytest.mark.parametrize("n,tile", [(64, 64), (100, 64), (128, 128), (300, 128), (513, 128), (1024, 128),
+@pytest.mark.parametrize("n,tile", [(64, 64), (100, 64), (128, 128), (300, 128), (513, 128), (1024, 128), (700, 256),
                                     (640, 64)])
 def test_adjoint_matches_oracle(mtd, n, tile):
     a = _spd(n, n)
