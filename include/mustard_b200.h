@@ -291,6 +291,12 @@ int mtd_batch_solve(mtd_batch *b, const double *const *dA, const int64_t *lda, v
                     const double *const *dB, const int64_t *ldb, double *const *dX, const int64_t *ldx,
                     const int *nrhs, int method, double tol, int max_iter, void *stream, mtd_batch_solve_stats *stats);
 int mtd_batch_destroy(mtd_batch *b);
+/* Autotuner: picks tile[m] and nest[m] for a batch of sizes n[m] by timing, for each
+ * distinct size, trial factorisations of that size's share of the batch (seeded SPD
+ * matrices on this GPU) with each candidate tile (n itself, 128, 256, 384, 512) and nested
+ * sub-tile (none, 64, 128), keeping the fastest.  trial_ms (nullable): wall time spent. */
+int mtd_batch_autotune(int count, const int64_t *n, int prec, int64_t *tile_out, int *nest_out, double *trial_ms,
+                       void *stream);
 
 /* ---- Cholesky adjoint (no counterpart in the reference) ----
  *

@@ -294,6 +294,17 @@ class SpdSolver:
             pass
 
 
+def batch_autotune(sizes, prec=_capi.PREC_FP64, stream=None):
+    """(tiles, nests, wall ms) chosen by mtd_batch_autotune for a batch of these sizes."""
+    c = len(sizes)
+    n = (ctypes.c_int64 * c)(*sizes)
+    t = (ctypes.c_int64 * c)()
+    k = (ctypes.c_int * c)()
+    ms = ctypes.c_double(0.0)
+    _capi.check(lib().mtd_batch_autotune(c, n, prec, t, k, ctypes.byref(ms), _stream_handle(stream)))
+    return list(t), list(k), ms.value
+
+
 class Batch:
     """Batched Cholesky factorisations and solves (mtd_batch_*): matrices of different sizes
     factored as one merged task graph in one persistent launch.

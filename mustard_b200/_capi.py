@@ -57,6 +57,7 @@ SIGNATURES = {
     "mtd_batch_solve": (_i, [_vp, _pp, _pi64, _pp, _pi64, _pp, _pi64, _pp, _pi64, ctypes.POINTER(_i), _i, _d, _i, _vp,
                              ctypes.POINTER(BatchSolveStats)]),
     "mtd_batch_destroy": (_i, [_vp]),
+    "mtd_batch_autotune": (_i, [_i, _pi64, _i, _pi64, ctypes.POINTER(_i), ctypes.POINTER(_d), _vp]),
     "mtd_adjoint_create": (_i, [ctypes.POINTER(_vp), _i, _pi64, _i64, _i]),
     "mtd_adjoint_num_tasks": (_i, [_vp]),
     "mtd_adjoint_run": (_i, [_vp, _pp, _pi64, _pp, _pi64, _vp]),

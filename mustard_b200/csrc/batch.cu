@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <map>
 #include <new>
 #include <vector>
 
@@ -665,6 +666,121 @@ int mtd_batch_destroy(mtd_batch *b) {
     cudaDeviceSynchronize();
     release(b);
     delete b;
+    return MTD_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+__global__ void to_float_kernel(const double *x, float *y, int64_t count) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += int64_t(gridDim.x) * blockDim.x)
+        y[i] = static_cast<float>(x[i]);
+}
+
+// Trial settings for matrices of size n: one tile (tile = n), or tiles of 128 .. 512
+// elements; each with no nesting or with 64- / 128-element nested diagonal factorisations.
+std::vector<std::pair<int64_t, int>> tune_candidates(int64_t n) {
+    std::vector<int64_t> tiles{n};
+    for (int64_t t : {128, 256, 384, 512})
+        if (t < n) tiles.push_back(t);
+    std::vector<std::pair<int64_t, int>> out;
+    for (int64_t t : tiles) {
+        out.push_back({t, 0});
+        for (int nest : {64, 128})
+            if (nest < t) out.push_back({t, nest});
+    }
+    return out;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mtd_batch_autotune(int count, const int64_t *n, int prec, int64_t *tile_out, int *nest_out, double *trial_ms,
+                       void *stream) {
+    if (count <= 0 || !n || !tile_out || !nest_out ||
+        (prec != MTD_PREC_FP64 && prec != MTD_PREC_TF32 && prec != MTD_PREC_FP32))
+        return MTD_ERR_INVALID_ARG;
+    for (int m = 0; m < count; ++m)
+        if (n[m] <= 0 || n[m] > (int64_t(1) << 20)) return MTD_ERR_INVALID_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const auto t0 = std::chrono::steady_clock::now();
+    std::map<int64_t, int> per_size;
+    for (int m = 0; m < count; ++m) ++per_size[n[m]];
+    const size_t es = prec == MTD_PREC_FP64 ? sizeof(double) : sizeof(float);
+    std::map<int64_t, std::pair<int64_t, int>> choice;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return MTD_ERR_CUDA;
+    int rc = MTD_OK;
+    for (const auto &kv : per_size) {
+        if (rc) break;
+        const int64_t sz = kv.first;
+        // a trial batch as large as this size's share of the batch (so the trial sees the
+        // parallelism the real batch offers), capped at ~2^38 / 3 flop so it stays milliseconds
+        const int k = std::max(1, std::min(kv.second, static_cast<int>(std::max<int64_t>(4, (int64_t(1) << 38) /
+                                                                                         (sz * sz * sz)))));
+        const size_t elems = size_t(k) * size_t(sz) * size_t(sz);
+        double *src = nullptr;
+        void *work = nullptr;
+        float *src32 = nullptr;
+        if (dalloc(&src, elems) || cudaMalloc(&work, std::max<size_t>(elems * es, 1)) != cudaSuccess ||
+            (prec != MTD_PREC_FP64 && dalloc(&src32, elems))) {
+            cudaFree(src);
+            cudaFree(work);
+            rc = MTD_ERR_OUT_OF_MEMORY;
+            break;
+        }
+        for (int i = 0; i < k && !rc; ++i)
+            rc = mtd_generate(src + size_t(i) * sz * sz, sz, sz, MTD_GEN_SPD, 0x5eed + uint64_t(i), 1.0, s);
+        if (!rc && src32) to_float_kernel<<<1024, 256, 0, s>>>(src, src32, static_cast<int64_t>(elems));
+        const void *pristine = src32 ? static_cast<const void *>(src32) : static_cast<const void *>(src);
+        std::vector<void *> ptrs(k);
+        std::vector<int64_t> lds(k, sz), sizes(k, sz), tiles(k);
+        std::vector<int> nests(k);
+        for (int i = 0; i < k; ++i) ptrs[i] = static_cast<unsigned char *>(work) + size_t(i) * sz * sz * es;
+        double best_ms = 1e300;
+        std::pair<int64_t, int> best{std::min<int64_t>(sz, 512), sz > kNestTile ? kNestTile : 0};
+        for (const auto &cand : tune_candidates(sz)) {
+            if (rc) break;
+            std::fill(tiles.begin(), tiles.end(), cand.first);
+            std::fill(nests.begin(), nests.end(), cand.second);
+            mtd_batch *b = nullptr;
+            rc = mtd_batch_create(&b, k, sizes.data(), tiles.data(), nests.data(), prec);
+            if (rc) break;
+            double ms_min = 1e300;
+            for (int rep = 0; rep < 2 && !rc; ++rep) {  // the first run warms up
+                if (cudaMemcpyAsync(work, pristine, elems * es, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+                    cudaEventRecord(e0, s) != cudaSuccess) {
+                    rc = MTD_ERR_CUDA;
+                    break;
+                }
+                rc = mtd_batch_factor(b, ptrs.data(), lds.data(), s);
+                if (!rc && cudaEventRecord(e1, s) != cudaSuccess) rc = MTD_ERR_CUDA;
+                if (!rc) rc = mtd_batch_status(b, nullptr, nullptr);
+                float ms = 0.f;
+                if (!rc && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) rc = MTD_ERR_CUDA;
+                if (!rc && rep > 0) ms_min = std::min(ms_min, double(ms));
+            }
+            mtd_batch_destroy(b);
+            if (!rc && ms_min < best_ms) {
+                best_ms = ms_min;
+                best = cand;
+            }
+        }
+        choice[sz] = best;
+        cudaFree(src);
+        cudaFree(work);
+        cudaFree(src32);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    for (int m = 0; m < count; ++m) {
+        tile_out[m] = choice[n[m]].first;
+        nest_out[m] = choice[n[m]].second;
+    }
+    if (trial_ms) *trial_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return MTD_OK;
 }
 
