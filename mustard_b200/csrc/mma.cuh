@@ -391,6 +391,13 @@ struct BlockMmaT {
     __device__ __forceinline__ void store_to(T *C, int64_t ldc, int M, int N) const {
         for_each(M, N, [&](int r, int c, T v) { C[r + int64_t(c) * ldc] = v; });
     }
+
+    // C(r, c) = acc(r, c) as the tensor cores of this mode read it: rounded to nearest TF32
+    // for single TF32 products (so later products that truncate their operands see the
+    // rounded value), unchanged for FP64 and split-TF32.
+    __device__ __forceinline__ void store_rounded_to(T *C, int64_t ldc, int M, int N) const {
+        for_each(M, N, [&](int r, int c, T v) { C[r + int64_t(c) * ldc] = frag_round<SPLIT>(v); });
+    }
 };
 
 template <int BM, int BN, int WARPS_M, int WARPS_N, int BL, int VEC, int STAGES = 3, int BK_ = 16>

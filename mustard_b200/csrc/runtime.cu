@@ -1,4 +1,6 @@
 // C ABI implementation: graph lifetime, device upload, runs, statistics.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -397,6 +399,35 @@ int mtd_graph_finalize(mtd_graph *g) {
 
 namespace mtd {
 
+// TMA tensor map of an FP32 n x n column-major matrix (ld elements) for the tcgen05 GEMM
+// items: boxes of 32 rows x 32 columns, 128-byte swizzle with 32-byte atoms (the layout the
+// TF32 MMA reads for MN-major operands), zero fill past the matrix.  The driver entry point
+// is looked up once; without it (or on an encoding error) the run keeps its cp.async path.
+void encode_tmap(RunArgs &a, void *dA, int64_t n, int64_t ld) {
+    static_assert(sizeof(CUtensorMap) == sizeof(a.tmap), "tensor map storage");
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void *fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    });
+    a.tma = 0;
+    if (!encode) return;
+    const cuuint64_t dims[2] = {cuuint64_t(n), cuuint64_t(n)};
+    const cuuint64_t strides[1] = {cuuint64_t(ld) * sizeof(float)};
+    const cuuint32_t box[2] = {32, 32}, elem[2] = {1, 1};
+    CUtensorMap map;
+    if (encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, dA, dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return;
+    std::memcpy(a.tmap, &map, sizeof(map));
+    a.tma = 1;
+}
+
 // Reset, seed and launch one persistent run (shared by graphs, batches and the
 // no-allocation entry point's sibling paths).  Stream-ordered; no host synchronisation.
 int launch_run(const RunArgs &a, const int *deps_init, const int *roots, int n_roots, long long total_items,
@@ -439,11 +470,16 @@ static int run_persistent(mtd_graph *g, void *dA, int64_t lda, void *stream, int
     if (cudaGetDevice(&dev) != cudaSuccess || dev != g->device) return MTD_ERR_STATE;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
 
-    const RunArgs a = make_args(g, dA, lda);
+    RunArgs a = make_args(g, dA, lda);
+    const bool vec2 = use_vec2(g, dA, lda);
+    // TF32 runs feed their tcgen05 GEMM items with TMA when every update's depth (the tile
+    // and nested sub-tile edges) is a whole number of 32-column stages
+    if (g->prec == MTD_PREC_TF32 && vec2 && g->dag.tile() % 32 == 0 && g->nest % 32 == 0)
+        mtd::encode_tmap(a, dA, g->dag.n(), lda);
     const int grid = g->num_sms;
     g->last_grid = grid;
-    const int rc = launch_run(a, g->d_deps_init, g->d_roots, g->n_roots, g->total_items, g->prec,
-                              use_vec2(g, dA, lda), grid, s, false);
+    const int rc = launch_run(a, g->d_deps_init, g->d_roots, g->n_roots, g->total_items, g->prec, vec2, grid, s,
+                              false);
     if (rc) return rc;
     if (cudaMemcpyAsync(g->h_ctl, g->d_ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, s) != cudaSuccess)
         return MTD_ERR_CUDA;

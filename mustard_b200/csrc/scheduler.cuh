@@ -19,6 +19,7 @@
 
 #include "device_types.hpp"
 #include "adjoint_ops.cuh"
+#include "tcgen05.cuh"
 #include "tile_ops.cuh"
 
 namespace mtd {
@@ -136,10 +137,64 @@ __device__ __forceinline__ void complete_item(const RunArgs &p, int task) {
 // products, SPLIT = 3 FP32-accurate split-TF32 products).
 // ADJ: the kernel instance that runs the Cholesky adjoint's task graphs (its operations
 // only), so the factorisation kernels keep their own register allocation.
+// The TF32 factorisation with 16-byte aligned operands runs its GEMM and SYRK items on the
+// fifth-generation tensor cores (tcgen05, accumulator in TMEM); everything else on mma.sync.
+template <int VEC, typename T, int SPLIT, bool ADJ>
+constexpr bool uses_tcgen05() {
+    return VEC == 2 && sizeof(T) == 4 && SPLIT == 1 && !ADJ;
+}
+
+// C -= A B^T (GEMM_NT) or the lower part of C -= A A^T (SYRK_LN), one 128 x 128 output tile
+// per item, on tcgen05.
+__device__ __forceinline__ int op_update_tc(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem,
+                                            tc::State *tcs, const void *tmap) {
+    int r0, c0, mm, nn, brow;
+    bool lower = false;
+    const float *B;
+    if (t.op == MTD_OP_SYRK_LN) {
+        int pb = 0;
+        while ((pb + 1) * (pb + 2) / 2 <= item) ++pb;
+        const int qb = item - pb * (pb + 1) / 2;
+        r0 = pb * kGemmTile;
+        c0 = qb * kGemmTile;
+        mm = min(kGemmTile, t.m - r0);
+        nn = min(kGemmTile, t.m - c0);
+        lower = pb == qb;
+        B = at<float>(m, t.ar + c0, t.ac);
+        brow = t.ar + c0;
+    } else {
+        const int nbn = (t.n + kGemmTile - 1) / kGemmTile;
+        r0 = (item / nbn) * kGemmTile;
+        c0 = (item % nbn) * kGemmTile;
+        mm = min(kGemmTile, t.m - r0);
+        nn = min(kGemmTile, t.n - c0);
+        B = at<float>(m, t.br + c0, t.bc);
+        brow = t.br + c0;
+    }
+    // the swizzled operand layout wants 1024-byte aligned stage buffers
+    uint8_t *s = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem) + 1023) & ~uintptr_t(1023));
+    float *C = at<float>(m, t.cr + r0, t.cc + c0);
+    // SYRK's B panel starts in the same column as A; GEMM_NT's may not
+    const int bcol = t.op == MTD_OP_SYRK_LN ? t.ac : t.bc;
+    const bool ok = (tmap && t.k % tc::kBK == 0 && t.ac == bcol)
+                        ? tc::gemm_nt_tma<kThreads>(tcs, s, tmap, t.ar + r0, brow, t.ac, t.k, mm, nn, C, m.lda, lower,
+                                                    0, 0, p.timeout_ns)
+                        : tc::gemm_nt<kThreads>(tcs, s, at<float>(m, t.ar + r0, t.ac), m.lda, B, m.lda, mm, nn, t.k, C,
+                                                m.lda, lower, 0, 0, p.timeout_ns);
+    if (!ok) {
+        if (threadIdx.x == 0) report_error(p.ctl, MTD_ERR_TIMEOUT, 0);
+        return MTD_ERR_TIMEOUT;
+    }
+    return 0;
+}
+
 template <int VEC, typename T, int SPLIT = 1, bool ADJ = false>
-__device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int item, void *smem) {
+__device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int item, void *smem,
+                                        tc::State *tcs = nullptr, const void *tmap = nullptr) {
     if constexpr (ADJ) return dispatch_adjoint<T, VEC, SPLIT>(p, t, item, smem);
     const MatCtx m = mat_ctx<T>(p, t);
+    if constexpr (uses_tcgen05<VEC, T, SPLIT, ADJ>())
+        if (t.op == MTD_OP_GEMM_NT || t.op == MTD_OP_SYRK_LN) return op_update_tc(p, m, t, item, smem, tcs, tmap);
     if constexpr (sizeof(T) == 8) {
         switch (t.op) {
         case MTD_OP_POTRF: return op_potrf<T, VEC>(p, m, t, smem);
@@ -166,9 +221,12 @@ __device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int 
 }
 
 template <int VEC, typename T, int SPLIT = 1, bool ADJ = false>
-__global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const RunArgs p) {
+__global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const __grid_constant__ RunArgs p) {
     extern __shared__ __align__(128) double smem[];
     __shared__ int s_cmd, s_task, s_item;
+    __shared__ tc::State tcs;
+    constexpr bool kTc = uses_tcgen05<VEC, T, SPLIT, ADJ>();
+    if constexpr (kTc) tc::init(&tcs);  // TMEM accumulator and barriers, held for the whole run
     if (threadIdx.x == 0) atomicMin(&p.ctl->start_ns, global_ns());
     while (true) {
         if (threadIdx.x == 0) {
@@ -188,7 +246,8 @@ __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const RunArgs p
 #pragma unroll
             for (int w = 0; w < int(sizeof(DevTask) / sizeof(int4)); ++w) dst[w] = __ldg(src + w);
         }
-        const int st = dispatch<VEC, T, SPLIT, ADJ>(p, t, item, smem);
+        // the tensor map's address is taken here, on the kernel parameter itself
+        const int st = dispatch<VEC, T, SPLIT, ADJ>(p, t, item, smem, &tcs, p.tma ? p.tmap : nullptr);
         __syncthreads();
         if (threadIdx.x == 0) {
             if (st == 0) complete_item(p, task);
@@ -204,6 +263,7 @@ __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const RunArgs p
             }
         }
     }
+    if constexpr (kTc) tc::release(&tcs);
 }
 
 // One task as an ordinary launch (grid = its work items): the node kernel of the

@@ -1,0 +1,347 @@
+// Fifth-generation tensor cores (tcgen05) for the TF32 GEMM items of the low-precision
+// factorisation: C(M x N) -= A(M x K) * B(N x K)^T with M, N <= 128, FP32 operands in HBM
+// (column-major, A and B both MN-contiguous), FP32 accumulation in tensor memory (TMEM).
+//
+// Operands are staged by 16-byte cp.async pieces straight into the MN-major layout that
+// 32-bit operands need (the "128-byte swizzle with 32-byte atoms" mode; with no swizzle a
+// TF32 MN-major MMA reads zeros): atoms of 4 K-rows x 128 bytes (32 FP32 along MN), the
+// 32-byte chunks of row r stored at chunk index (c ^ r); MN-adjacent atoms kAtomMN = 512
+// bytes apart, K-adjacent atoms kAtomK = 2 KB apart.  Each piece is rounded to nearest TF32 in
+// shared memory before the MMAs read it (the tensor core reads the TF32 part of each FP32
+// bit pattern).  One thread issues tcgen05.mma (M = N = 128, K = 8 per instruction) for a
+// stage and commits the group to that stage's mbarrier; the stage's buffer is refilled only
+// after the barrier says the MMAs that read it are done.  The epilogue reads the accumulator
+// with tcgen05.ld (warp w: TMEM lanes 32 (w % 4) .., columns 32 (w / 4) ..) and updates C.
+//
+// Every mbarrier wait is bounded by a %globaltimer deadline; on expiry the caller's error
+// word is set and the item ends (its result is then not used: the run reports the error).
+#pragma once
+
+#include <cstdint>
+
+#include "device_types.hpp"
+
+namespace mtd {
+namespace tc {
+
+constexpr int kM = 128, kN = 128;     // MMA shape (one CTA)
+constexpr int kBK = 32;               // K per stage (4 MMAs of K = 8)
+constexpr int kStages = 6;            // up to 5 stages (160 KB) in flight: items are bandwidth-bound
+constexpr int kAtomMN = 512;          // bytes between MN-adjacent atoms (4 x 128-byte rows)
+constexpr int kAtomK = 4 * kAtomMN;   // bytes between K-adjacent atoms (4 MN atoms cover 128)
+constexpr int kOperandBytes = (kBK / 4) * kAtomK;    // 128 x 32 FP32 = 16 KB
+constexpr int kStageBytes = 2 * kOperandBytes;       // A and B
+constexpr int kSmemBytes = kStages * kStageBytes;    // 192 KB
+constexpr uint32_t kTmemCols = 128;
+
+// Instruction descriptor: F32 accumulator, TF32 A and B, both MN-major, M = 128, N = 128.
+constexpr uint32_t kIdescTf32 = (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | (1u << 16) |
+                                (uint32_t(kN >> 3) << 17) | (uint32_t(kM >> 4) << 24);
+
+struct State {
+    uint64_t mbar[kStages];  // MMAs reading stage s are done (tcgen05.commit)
+    uint64_t full[kStages];  // stage s is loaded (TMA complete_tx)
+    uint32_t taddr;          // TMEM base address (lane 0, first allocated column)
+    uint32_t phases;         // bit s: parity of the next completion of mbar[s]
+    uint32_t fphases;        // bit s: parity of the next completion of full[s]
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor for the swizzled MN-major layout: start address, leading
+// byte offset (between MN atoms) and stride byte offset (between K atoms) in 16-byte units,
+// descriptor version 1, layout type 1 (128-byte swizzle, 32-byte atoms).
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr) {
+    return uint64_t((saddr >> 4) & 0x3fff) | (uint64_t((kAtomMN >> 4) & 0x3fff) << 16) |
+           (uint64_t((kAtomK >> 4) & 0x3fff) << 32) | (1ull << 46) | (1ull << 61);
+}
+
+// Byte offset in an operand stage of the 16-byte piece holding elements (mn .. mn+3, k):
+// atom (mn / 32, k / 4), row k % 4, 32-byte chunk (mn % 32) / 8 swizzled with the row.
+__device__ __forceinline__ int piece_offset(int mn, int k) {
+    const int row = k & 3, cb = (mn & 31) * 4;  // byte column inside the 128-byte row
+    const int chunk = ((cb >> 5) ^ row) & 3;
+    return (mn >> 5) * kAtomMN + (k >> 2) * kAtomK + row * 128 + (chunk << 5) + (cb & 16);
+}
+
+__device__ __forceinline__ unsigned long long now_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Once per CTA, all threads: TMEM for the accumulator and the stage barriers.
+__device__ __forceinline__ void init(State *st) {
+    if (threadIdx.x < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&st->taddr)),
+                     "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&st->mbar[s])), "r"(1));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&st->full[s])), "r"(1));
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        st->phases = 0;
+        st->fphases = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// Once per CTA, all threads, after the last use.
+__device__ __forceinline__ void release(State *st) {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (threadIdx.x < 32)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(st->taddr), "r"(kTmemCols));
+}
+
+// Wait for the completion of parity `parity` of the barrier; false on timeout.
+__device__ __forceinline__ bool wait_bar(uint64_t *bar, uint32_t parity, unsigned long long deadline) {
+    const uint32_t a = smem_addr(bar);
+    for (unsigned it = 0;; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((it & 255) == 255 && now_ns() > deadline) return false;
+    }
+}
+
+__device__ __forceinline__ void cp16(uint32_t dst, const void *src, int bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+
+// Pieces of a stage: e -> (operand, K atom, MN atom, row, piece in row); 32 consecutive e
+// fill one 512-byte atom (conflict-free) from four 128-byte runs of consecutive columns.
+constexpr int kPieces = 2 * (kBK / 4) * 4 * 4 * 8;  // operands x K atoms x MN atoms x rows x pieces
+__device__ __forceinline__ void piece_of(int e, int &op, int &mn, int &k) {
+    const int p8 = e & 7, r4 = (e >> 3) & 3, am = (e >> 5) & 3, ka = (e >> 7) & 7;
+    op = e >> 10;
+    mn = am * 32 + p8 * 4;
+    k = ka * 4 + r4;
+}
+
+// Stage k-slice k0 of A (rows m < M) and B (rows n < N), thread-owned pieces e = tid + 512 i.
+template <int THREADS>
+__device__ __forceinline__ void load_stage(uint8_t *stage, const float *A, int64_t lda, const float *B, int64_t ldb,
+                                           int M, int N, int K, int k0) {
+    for (int e = threadIdx.x; e < kPieces; e += THREADS) {
+        int op, r, kl;
+        piece_of(e, op, r, kl);
+        const int kk = k0 + kl;
+        const int lim = op ? N : M;
+        const int rows = kk < K ? min(4, max(0, lim - r)) : 0;
+        const float *src = op ? B + r + int64_t(kk) * ldb : A + r + int64_t(kk) * lda;
+        cp16(smem_addr(stage + op * kOperandBytes + piece_offset(r, kl)), rows ? src : (op ? B : A), rows * 4);
+    }
+}
+
+// Round this thread's pieces of the stage to nearest TF32, in place.
+template <int THREADS>
+__device__ __forceinline__ void round_stage(uint8_t *stage) {
+    for (int e = threadIdx.x; e < kPieces; e += THREADS) {
+        int op, r, kl;
+        piece_of(e, op, r, kl);
+        float4 *p = reinterpret_cast<float4 *>(stage + op * kOperandBytes + piece_offset(r, kl));
+        float4 v = *p;
+        uint32_t x, y, z, w;
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(x) : "f"(v.x));
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(y) : "f"(v.y));
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(z) : "f"(v.z));
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(w) : "f"(v.w));
+        *p = make_float4(__uint_as_float(x), __uint_as_float(y), __uint_as_float(z), __uint_as_float(w));
+    }
+}
+
+// C -= accumulator (all threads; warp w reads TMEM lanes 32 (w % 4) .. and columns
+// 32 (w / 4) ..), then release the accumulator for the next item.
+__device__ __forceinline__ bool epilogue(State *st, bool ok, int M, int N, float *C, int64_t ldc, bool lower_only,
+                                         int r0, int c0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int row = (warp & 3) * 32 + lane, col0 = (warp >> 2) * 32;
+    uint32_t v[32];
+    const uint32_t taddr = st->taddr + (uint32_t((warp & 3) * 32) << 16) + uint32_t(col0);
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    if (ok && row < M) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            const int col = col0 + j;
+            if (col < N && (!lower_only || row + r0 >= col + c0)) {
+                float *p = C + row + int64_t(col) * ldc;
+                *p = __ldcg(p) - __uint_as_float(v[j]);
+            }
+        }
+    }
+    // the next item's MMAs overwrite the accumulator only after every warp has read it
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    return ok;
+}
+
+// C -= A B^T over K, M, N <= 128 (C(r, c) with r + r0 >= c + c0 only, when lower_only).
+// All THREADS threads of the CTA call it; `smem` holds kSmemBytes (1024-byte aligned).
+// Returns false if a wait timed out.
+template <int THREADS>
+__device__ bool gemm_nt(State *st, uint8_t *smem, const float *A, int64_t lda, const float *B, int64_t ldb, int M,
+                        int N, int K, float *C, int64_t ldc, bool lower_only, int r0, int c0,
+                        unsigned long long timeout_ns) {
+    static_assert(THREADS == 512, "epilogue: 16 warps cover 4 lane quarters x 4 column quarters of 128 x 128");
+    const unsigned long long deadline = now_ns() + timeout_ns;
+    const int nk = (K + kBK - 1) / kBK;
+    uint32_t phases = st->phases;
+    bool ok = true;
+#pragma unroll
+    for (int s = 0; s < kStages - 1; ++s) {
+        if (s < nk) load_stage<THREADS>(smem + s * kStageBytes, A, lda, B, ldb, M, N, K, s * kBK);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+    for (int kt = 0; kt < nk; ++kt) {
+        const int s = kt % kStages;
+        uint8_t *stage = smem + s * kStageBytes;
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 2) : "memory");
+        round_stage<THREADS>(stage);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = smem_addr(stage), b0 = a0 + kOperandBytes;
+#pragma unroll
+            for (int g = 0; g < kBK / 8; ++g) {
+                const uint64_t ad = make_desc(a0 + g * 2 * kAtomK), bd = make_desc(b0 + g * 2 * kAtomK);
+                const uint32_t acc = (kt > 0 || g > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+                    ::"r"(st->taddr), "l"(ad), "l"(bd), "r"(kIdescTf32), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_addr(&st->mbar[s]))
+                         : "memory");
+        }
+        // refill the stage used by k-slice kt - 1 once its MMAs are done
+        if (kt > 0) {
+            const int sp = (kt - 1) % kStages;
+            ok = ok && wait_bar(&st->mbar[sp], (phases >> sp) & 1u, deadline);
+            phases ^= 1u << sp;
+        }
+        const int nxt = kt + kStages - 1;
+        if (ok && nxt < nk) load_stage<THREADS>(smem + (nxt % kStages) * kStageBytes, A, lda, B, ldb, M, N, K, nxt * kBK);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+    {  // the accumulator is complete once the last k-slice's MMAs are
+        const int sl = (nk - 1) % kStages;
+        ok = ok && wait_bar(&st->mbar[sl], (phases >> sl) & 1u, deadline);
+        phases ^= 1u << sl;
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    if (threadIdx.x == 0) st->phases = phases;
+    return epilogue(st, ok, M, N, C, ldc, lower_only, r0, c0);
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const void *map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+// C -= A B^T as gemm_nt, with both operands fetched by TMA from the matrix `map` describes
+// (FP32, boxes of 32 rows x 32 columns, 128-byte swizzle with 32-byte atoms: box row k holds
+// 32 consecutive MN elements of column k, its 32-byte chunks at c ^ (k % 4)): A = rows
+// a_row .. a_row + 127, B = rows b_row .., columns k0 .. k0 + K - 1 (K a multiple of 32;
+// rows past the matrix read as zero).  One thread runs the whole pipeline: per stage one
+// expect_tx + 8 box loads on full[s], then, once the stage has landed, 4 MMAs committed to
+// mbar[s]; a stage is reloaded after its MMAs are done.  Operands must already be TF32
+// values (the tensor core truncates what it reads).
+template <int THREADS>
+__device__ bool gemm_nt_tma(State *st, uint8_t *smem, const void *map, int a_row, int b_row, int k0, int K, int M,
+                            int N, float *C, int64_t ldc, bool lower_only, int r0, int c0, unsigned long long timeout_ns) {
+    constexpr uint32_t kBoxBytes = 32 * 32 * 4;
+    bool ok = true;
+    if (threadIdx.x == 0) {
+        const unsigned long long deadline = now_ns() + timeout_ns;
+        const int nk = K / kBK;
+        uint32_t ph = st->phases, fph = st->fphases;
+        auto issue = [&](int s, int kt) {
+            const uint32_t bar = smem_addr(&st->full[s]), base = smem_addr(smem + s * kStageBytes);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(8 * kBoxBytes)
+                         : "memory");
+            for (int i = 0; i < 4; ++i) {
+                tma_load_2d(base + i * kBoxBytes, map, a_row + 32 * i, k0 + kt * kBK, bar);
+                tma_load_2d(base + kOperandBytes + i * kBoxBytes, map, b_row + 32 * i, k0 + kt * kBK, bar);
+            }
+        };
+        for (int s = 0; s < kStages && s < nk; ++s) issue(s, s);
+        for (int kt = 0; kt < nk && ok; ++kt) {
+            const int s = kt % kStages;
+            ok = wait_bar(&st->full[s], (fph >> s) & 1u, deadline);
+            fph ^= 1u << s;
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = smem_addr(smem + s * kStageBytes), b0 = a0 + kOperandBytes;
+#pragma unroll
+            for (int g = 0; g < kBK / 8; ++g) {
+                // boxes of 32 MN x 32 K: MN atoms one box apart, K atoms (4 rows) 512 bytes apart
+                const uint64_t lead = uint64_t(kBoxBytes >> 4) << 16, stride = uint64_t(512 >> 4) << 32;
+                const uint64_t ad = uint64_t(((a0 + g * 1024) >> 4) & 0x3fff) | lead | stride | (1ull << 46) | (1ull << 61);
+                const uint64_t bd = uint64_t(((b0 + g * 1024) >> 4) & 0x3fff) | lead | stride | (1ull << 46) | (1ull << 61);
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(st->taddr),
+                    "l"(ad), "l"(bd), "r"(kIdescTf32), "r"((kt > 0 || g > 0) ? 1u : 0u)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_addr(&st->mbar[s]))
+                         : "memory");
+            // reload the stage of k-slice kt - 1 once its MMAs are done
+            if (kt > 0 && kt - 1 + kStages < nk) {
+                const int sp = (kt - 1) % kStages;
+                ok = wait_bar(&st->mbar[sp], (ph >> sp) & 1u, deadline);
+                ph ^= 1u << sp;
+                if (ok) issue(sp, kt - 1 + kStages);
+            }
+        }
+        // consume the commits not waited above (the last kStages k-slices, in order), so the
+        // barriers' parities stay in step; the last one means the accumulator is complete
+        for (int kt = nk > kStages ? nk - kStages : 0; kt < nk && ok; ++kt) {
+            const int s = kt % kStages;
+            ok = wait_bar(&st->mbar[s], (ph >> s) & 1u, deadline);
+            ph ^= 1u << s;
+        }
+        st->phases = ph;
+        st->fphases = fph;
+    }
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) s_ok = ok ? 1 : 0;
+    __syncthreads();
+    return epilogue(st, s_ok != 0, M, N, C, ldc, lower_only, r0, c0);
+}
+
+}  // namespace tc
+}  // namespace mtd

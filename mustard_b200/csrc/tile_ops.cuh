@@ -334,7 +334,7 @@ __device__ int op_trsm_rlt(const RunArgs &p, const MatCtx &m, const DevTask &t, 
         Mn e;
         e.zero();
         e.run(smem, X + int64_t(jb) * lda, lda, W + jb, ldw, mm, jn, jn);
-        e.store_to(X + int64_t(jb) * lda, lda, mm, jn);
+        e.store_rounded_to(X + int64_t(jb) * lda, lda, mm, jn);  // panel of L: an operand of the updates
         block_fence_sync();
     }
     return 0;
