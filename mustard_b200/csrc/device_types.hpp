@@ -70,6 +70,8 @@ struct alignas(128) QueueCtl {
     char pad0[120];
     unsigned long long tail;   // slots reserved by producers
     char pad1[120];
+    long long avail;           // items pushed and not yet claimed (transiently low while a
+    char pad2[120];            // failed claim is being undone)
 };
 
 struct alignas(128) RunCtl {

@@ -376,15 +376,39 @@ struct BlockMmaT {
                 }
     }
 
-    // C(r, c) -= acc(r, c); with lower_only, only where (r + r0) >= (c + c0).
+    // C(r, c) -= acc(r, c); with lower_only, only where (r + r0) >= (c + c0).  The loads of
+    // one fragment row (FN x 4 elements) are issued together before any store, so their
+    // latencies overlap (interleaved load / store pairs would wait for each load in turn).
     __device__ __forceinline__ void sub_from(T *C, int64_t ldc, int M, int N, bool lower_only = false, int r0 = 0,
                                              int c0 = 0) const {
-        for_each(M, N, [&](int r, int c, T v) {
-            if (!lower_only || r + r0 >= c + c0) {
-                T *p = C + r + int64_t(c) * ldc;
-                *p = ld_cg(p) - v;
-            }
-        });
+        const int lane = threadIdx.x & 31;
+        const int warp = threadIdx.x >> 5;
+        const int wm0 = (warp / WARPS_N) * WM;
+        const int wn0 = (warp % WARPS_N) * WN;
+        const int g = lane >> 2;
+        const int t = lane & 3;
+#pragma unroll
+        for (int i = 0; i < FM; ++i) {
+            T cv[FN][4];
+#pragma unroll
+            for (int j = 0; j < FN; ++j)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int r = wm0 + i * 16 + g + ((v & 2) ? 8 : 0);
+                    const int c = wn0 + j * 8 + 2 * t + (v & 1);
+                    const bool in = r < M && c < N && (!lower_only || r + r0 >= c + c0);
+                    cv[j][v] = in ? ld_cg(C + r + int64_t(c) * ldc) : T(0);
+                }
+#pragma unroll
+            for (int j = 0; j < FN; ++j)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int r = wm0 + i * 16 + g + ((v & 2) ? 8 : 0);
+                    const int c = wn0 + j * 8 + 2 * t + (v & 1);
+                    if (r < M && c < N && (!lower_only || r + r0 >= c + c0))
+                        C[r + int64_t(c) * ldc] = cv[j][v] - acc[i][j][v];
+                }
+        }
     }
 
     // C(r, c) = acc(r, c).

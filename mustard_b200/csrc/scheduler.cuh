@@ -10,9 +10,14 @@
 //     148 SMs can share one tile operation;
 //   - the dependency decrement is fused into the epilogue of a task's last work item;
 //   - two ready queues (critical path first) replace the single FIFO ring;
-//   - a queue is a bounded array of 64-bit slots (task << 32 | item) claimed with a CAS
-//     on `head` only while head < tail, so a consumer never claims a slot nobody has
-//     reserved; every slot is written once per run (capacity = that queue's total items);
+//   - a queue is a bounded array of 64-bit slots (task << 32 | item); a producer reserves
+//     slots with a fetch-and-add on `tail`, writes them, then adds their number to `avail`;
+//     a consumer first takes one unit of `avail` (fetch-and-add, undone if it was not
+//     positive) and only then a slot index from `head` (fetch-and-add), so it never claims
+//     a slot nobody has reserved and no claim ever retries: with 148 CTAs popping short
+//     items a compare-and-swap on `head` admits about one claim per L2 round trip, which
+//     starved the tensor-core items; every slot is written once per run (capacity = that
+//     queue's total items);
 //   - every wait is bounded by a globaltimer deadline after which the CTA records
 //     MTD_ERR_TIMEOUT, raises the abort flag and returns.
 #pragma once
@@ -38,6 +43,12 @@ __device__ __forceinline__ unsigned long long ld_volatile(const unsigned long lo
 }
 __device__ __forceinline__ int ld_volatile(const int *p) { return *reinterpret_cast<const volatile int *>(p); }
 
+// Signed fetch-and-add on a queue's `avail` count (two's complement in 64 bits).
+__device__ __forceinline__ long long add_avail(long long *c, long long v) {
+    return static_cast<long long>(
+        atomicAdd(reinterpret_cast<unsigned long long *>(c), static_cast<unsigned long long>(v)));
+}
+
 // Thread 0 of a CTA: `task` has no predecessors left.  Push every work item of it; a
 // join (no work items) completes on the spot, releasing its own successors.
 __device__ __forceinline__ void release_task(const RunArgs &p, int task) {
@@ -58,6 +69,8 @@ __device__ __forceinline__ void release_task(const RunArgs &p, int task) {
             volatile unsigned long long *slots = p.queue[q];
             for (unsigned long long i = 0; i < n; ++i)
                 slots[base + i] = (static_cast<unsigned long long>(tk) << 32) | i;
+            __threadfence();  // the slots before the count that lets consumers claim them
+            add_avail(&p.qctl[q].avail, static_cast<long long>(n));
             continue;
         }
         const int sb = __ldg(&p.tasks[tk].succ_begin), sc = __ldg(&p.tasks[tk].succ_count);
@@ -76,22 +89,29 @@ __device__ __forceinline__ void release_task(const RunArgs &p, int task) {
     }
 }
 
-// Thread 0 of a CTA: claim one work item, waiting (bounded) while none is ready.
+// Thread 0 of a CTA: claim one work item, waiting (bounded) while none is ready.  The
+// exit flags and both queues' counts are read together (one round trip); a claim is then
+// two fetch-and-adds and the slot read.
 __device__ __forceinline__ int pop_item(const RunArgs &p, int *task, int *item) {
     const unsigned long long t0 = global_ns();
     unsigned int backoff = 32;
     while (true) {
-        if (ld_volatile(&p.ctl->abort)) return kCmdExit;
-        if (ld_volatile(&p.ctl->tasks_done) >= p.n_tasks) return kCmdExit;
-        bool retry = false;
+        const int abort = ld_volatile(&p.ctl->abort);
+        const int done = ld_volatile(&p.ctl->tasks_done);
+        long long avail[kNumQueues];
+#pragma unroll
+        for (int q = 0; q < kNumQueues; ++q)
+            avail[q] = static_cast<long long>(
+                ld_volatile(reinterpret_cast<const unsigned long long *>(&p.qctl[q].avail)));
+        if (abort || done >= p.n_tasks) return kCmdExit;
         for (int q = 0; q < kNumQueues; ++q) {
-            const unsigned long long h = ld_volatile(&p.qctl[q].head);
-            const unsigned long long tl = ld_volatile(&p.qctl[q].tail);
-            if (h >= tl) continue;
-            if (atomicCAS(&p.qctl[q].head, h, h + 1) != h) {
-                retry = true;  // lost the race for this slot: look again at once
-                break;
+            if (avail[q] <= 0) continue;
+            if (add_avail(&p.qctl[q].avail, -1) <= 0) {  // taken meanwhile: give the unit back
+                add_avail(&p.qctl[q].avail, 1);
+                continue;
             }
+            // one unit of avail = one pushed, unclaimed item, so this slot is reserved
+            const unsigned long long h = atomicAdd(&p.qctl[q].head, 1ull);
             const unsigned long long *slot = p.queue[q] + h;
             unsigned long long v;
             while ((v = ld_volatile(slot)) == kEmptySlot) {
@@ -106,7 +126,6 @@ __device__ __forceinline__ int pop_item(const RunArgs &p, int *task, int *item) 
             *item = static_cast<int>(v & 0xffffffffull);
             return kCmdWork;
         }
-        if (retry) continue;
         if (global_ns() - t0 > p.timeout_ns) {
             report_error(p.ctl, MTD_ERR_TIMEOUT, 0);
             return kCmdExit;
@@ -251,8 +270,12 @@ __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const __grid_co
         __syncthreads();
         if (threadIdx.x == 0) {
             if (st == 0) complete_item(p, task);
+            if (!p.trace) {
+                atomicAdd(&p.ctl->items_done, 1ull);  // result unused: no round trip
+                continue;
+            }
             const long long slot = static_cast<long long>(atomicAdd(&p.ctl->items_done, 1ull));
-            if (p.trace && slot < p.trace_cap) {
+            if (slot < p.trace_cap) {
                 unsigned int smid;
                 asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
                 unsigned long long *rec = p.trace + 4 * slot;
@@ -302,6 +325,7 @@ __global__ void reset_kernel(const RunArgs p, const int *deps_init) {
         for (int q = 0; q < kNumQueues; ++q) {
             p.qctl[q].head = 0;
             p.qctl[q].tail = 0;
+            p.qctl[q].avail = 0;
         }
         p.ctl->tasks_done = 0;
         p.ctl->error = 0;

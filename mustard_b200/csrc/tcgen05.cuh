@@ -165,31 +165,44 @@ __device__ __forceinline__ void round_stage(uint8_t *stage) {
     }
 }
 
-// C -= accumulator (all threads; warp w reads TMEM lanes 32 (w % 4) .. and columns
-// 32 (w / 4) ..), then release the accumulator for the next item.
-__device__ __forceinline__ bool epilogue(State *st, bool ok, int M, int N, float *C, int64_t ldc, bool lower_only,
-                                         int r0, int c0) {
+// This thread's 32 elements of C in the epilogue's layout (row 32 (w % 4) + lane, columns
+// 32 (w / 4) ..), loaded back to back so that their latencies overlap (elements outside
+// the block, or above the diagonal with lower_only, read as 0 and are not written back).
+__device__ __forceinline__ void load_c(float (&cv)[32], int M, int N, const float *C, int64_t ldc, bool lower_only,
+                                       int r0, int c0) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int row = (warp & 3) * 32 + lane, col0 = (warp >> 2) * 32;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        const int col = col0 + j;
+        const bool in = row < M && col < N && (!lower_only || row + r0 >= col + c0);
+        cv[j] = in ? __ldcg(C + row + int64_t(col) * ldc) : 0.f;
+    }
+}
+
+// C = cv - accumulator (all threads; warp w reads TMEM lanes 32 (w % 4) .. and columns
+// 32 (w / 4) ..; cv from load_c), then release the accumulator for the next item.
+__device__ __forceinline__ bool epilogue(State *st, bool ok, const float (&cv)[32], int M, int N, float *C,
+                                         int64_t ldc, bool lower_only, int r0, int c0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int row = (warp & 3) * 32 + lane, col0 = (warp >> 2) * 32;
-    uint32_t v[32];
     const uint32_t taddr = st->taddr + (uint32_t((warp & 3) * 32) << 16) + uint32_t(col0);
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
-          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
-          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    if (ok && row < M) {
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-            const int col = col0 + j;
-            if (col < N && (!lower_only || row + r0 >= col + c0)) {
-                float *p = C + row + int64_t(col) * ldc;
-                *p = __ldcg(p) - __uint_as_float(v[j]);
+    for (int h = 0; h < 2; ++h) {  // two halves of 16 columns: fewer live registers
+        uint32_t v[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(taddr + 16 * h));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (ok && row < M) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int col = col0 + 16 * h + j;
+                if (col < N && (!lower_only || row + r0 >= col + c0))
+                    C[row + int64_t(col) * ldc] = cv[16 * h + j] - __uint_as_float(v[j]);
             }
         }
     }
@@ -258,7 +271,9 @@ __device__ bool gemm_nt(State *st, uint8_t *smem, const float *A, int64_t lda, c
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     if (threadIdx.x == 0) st->phases = phases;
-    return epilogue(st, ok, M, N, C, ldc, lower_only, r0, c0);
+    float cv[32];
+    load_c(cv, M, N, C, ldc, lower_only, r0, c0);
+    return epilogue(st, ok, cv, M, N, C, ldc, lower_only, r0, c0);
 }
 
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const void *map, int x, int y, uint32_t bar) {
@@ -337,10 +352,13 @@ __device__ bool gemm_nt_tma(State *st, uint8_t *smem, const void *map, int a_row
         st->phases = ph;
         st->fphases = fph;
     }
+    // the other threads fetch their part of C while thread 0 runs the pipeline
+    float cv[32];
+    load_c(cv, M, N, C, ldc, lower_only, r0, c0);
     __shared__ int s_ok;
     if (threadIdx.x == 0) s_ok = ok ? 1 : 0;
     __syncthreads();
-    return epilogue(st, s_ok != 0, M, N, C, ldc, lower_only, r0, c0);
+    return epilogue(st, s_ok != 0, cv, M, N, C, ldc, lower_only, r0, c0);
 }
 
 }  // namespace tc

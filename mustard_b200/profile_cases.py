@@ -7,6 +7,9 @@
     python -m mustard_b200.profile_cases chol --n 6144 --tile 512
     python -m mustard_b200.profile_cases lu   --n 6144 --tile 512
         a whole tiled factorisation
+    python -m mustard_b200.profile_cases gemm --n 8192 --tile 1024 --prec tf32
+        the same cases on a float32 matrix with TF32 tensor-core products (tcgen05 GEMM /
+        SYRK items fed by TMA; Cholesky and the GEMM-only step only)
 
 Each case runs `--runs` launches (default 2: the first is the one to capture with
 `-c 1`), checks the run status, and prints the device time of the last launch.
@@ -26,7 +29,10 @@ def main():
     ap.add_argument("--n", type=int, default=6144)
     ap.add_argument("--tile", type=int, default=768)
     ap.add_argument("--runs", type=int, default=2)
+    ap.add_argument("--prec", choices=["fp64", "tf32"], default="fp64")
     args = ap.parse_args()
+    if args.prec == "tf32" and args.case == "lu":
+        ap.error("the TF32 path factors SPD matrices only (chol, gemm)")
     n, b = args.n, args.tile
     t = (n + b - 1) // b
     a = torch.empty((n, n), dtype=torch.float64, device="cuda").t()
@@ -47,6 +53,9 @@ def main():
             for j in range(i + 1, t):
                 g.add_task(mtd.OP_GEMM_NT, (j, i), [(j, i), (j, 0), (i, 0)])
                 flops += 2.0 * ext[j] * ext[i] * ext[0]
+    if args.prec == "tf32":
+        g.set_precision(mtd.PREC_TF32)
+        a = a.t().contiguous().float().t()
     g.finalize()
     src = a.clone()
     s = torch.cuda.current_stream()
@@ -55,14 +64,17 @@ def main():
         a.copy_(src)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(s)
-        g.run(a, stream=s, sync=False)
+        if args.prec == "tf32":
+            g.run_f32(a, stream=s, sync=False)
+        else:
+            g.run(a, stream=s, sync=False)
         e1.record(s)
         torch.cuda.synchronize()
         rc, info = g.status()
         if rc:
             raise mtd.MtdError(rc, info)
         ms = e0.elapsed_time(e1)
-    print(json.dumps({"case": args.case, "n": n, "tile": b, "tasks": g.num_tasks, "ms": ms,
+    print(json.dumps({"case": args.case, "prec": args.prec, "n": n, "tile": b, "tasks": g.num_tasks, "ms": ms,
                       "tflops": flops / (ms * 1e-3) / 1e12}))
     g.close()
 
