@@ -109,10 +109,11 @@ struct RunArgs {
     const BatchMat *mats;
     int *mat_info;
     unsigned long long *mat_done_ns;
-    // TF32 single-matrix runs: a TMA tensor map of the matrix (FP32, n x n, ld = lda; boxes of
-    // 32 x 32 with 128-byte / 32-byte-atom swizzle) for the tcgen05 GEMM items, when tma != 0.
-    // The kernel receives RunArgs as a __grid_constant__ parameter, so the map's address is
-    // a valid TMA descriptor address.
+    // TF32 single-matrix runs: a TMA tensor map of the matrix (FP32, ld = lda, 128-byte /
+    // 32-byte-atom swizzle) for the tcgen05 GEMM items; tma = 0 none, 1 a 2D map (box 32 x 64),
+    // 2 a 3D map (32 rows of an atom, columns, atoms; box 32 x 64 x 4).  The kernel receives
+    // RunArgs as a __grid_constant__ parameter, so the map's address is a valid TMA
+    // descriptor address.
     int tma;
     alignas(64) unsigned char tmap[128];
 };

@@ -399,9 +399,11 @@ int mtd_graph_finalize(mtd_graph *g) {
 
 namespace mtd {
 
-// TMA tensor map of an FP32 n x n column-major matrix (ld elements) for the tcgen05 GEMM
-// items: boxes of 32 rows x 32 columns, 128-byte swizzle with 32-byte atoms (the layout the
-// TF32 MMA reads for MN-major operands), zero fill past the matrix.  The driver entry point
+// TMA tensor map of an FP32 n x n column-major matrix (ld elements) for the tcgen05 GEMM /
+// SYRK items: 128-byte swizzle with 32-byte atoms (the layout the TF32 MMA reads for MN-major
+// operands), zero fill past the matrix.  With n a multiple of 32 the map is 3D (32 rows of an
+// atom, columns, atoms 128 bytes apart; box 32 x 64 x 4), so one load fetches a whole
+// 128-row operand slice; otherwise 2D (rows, columns; box 32 x 64).  The driver entry point
 // is looked up once; without it (or on an encoding error) the run keeps its cp.async path.
 void encode_tmap(RunArgs &a, void *dA, int64_t n, int64_t ld) {
     static_assert(sizeof(CUtensorMap) == sizeof(a.tmap), "tensor map storage");
@@ -414,18 +416,28 @@ void encode_tmap(RunArgs &a, void *dA, int64_t n, int64_t ld) {
             q == cudaDriverEntryPointSuccess)
             encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
     });
-    a.tma = 0;
+    a.tma = tc::kTmaNone;
     if (!encode) return;
-    const cuuint64_t dims[2] = {cuuint64_t(n), cuuint64_t(n)};
-    const cuuint64_t strides[1] = {cuuint64_t(ld) * sizeof(float)};
-    const cuuint32_t box[2] = {32, 32}, elem[2] = {1, 1};
     CUtensorMap map;
-    if (encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, dA, dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
-               CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-        return;
+    CUresult r;
+    if (n % 32 == 0) {
+        const cuuint64_t dims[3] = {32, cuuint64_t(n), cuuint64_t(n / 32)};
+        const cuuint64_t strides[2] = {cuuint64_t(ld) * sizeof(float), 32 * sizeof(float)};
+        const cuuint32_t box[3] = {32, tc::kTmaBK, 4}, elem[3] = {1, 1, 1};
+        r = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, dA, dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    } else {
+        const cuuint64_t dims[2] = {cuuint64_t(n), cuuint64_t(n)};
+        const cuuint64_t strides[1] = {cuuint64_t(ld) * sizeof(float)};
+        const cuuint32_t box[2] = {32, tc::kTmaBK}, elem[2] = {1, 1};
+        r = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, dA, dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    }
+    if (r != CUDA_SUCCESS) return;
     std::memcpy(a.tmap, &map, sizeof(map));
-    a.tma = 1;
+    a.tma = n % 32 == 0 ? tc::kTmaMap3D : tc::kTmaMap2D;
 }
 
 // Reset, seed and launch one persistent run (shared by graphs, batches and the
@@ -472,8 +484,9 @@ static int run_persistent(mtd_graph *g, void *dA, int64_t lda, void *stream, int
 
     RunArgs a = make_args(g, dA, lda);
     const bool vec2 = use_vec2(g, dA, lda);
-    // TF32 runs feed their tcgen05 GEMM items with TMA when every update's depth (the tile
-    // and nested sub-tile edges) is a whole number of 32-column stages
+    // TF32 runs feed their tcgen05 GEMM items with TMA when every item's rows start on a
+    // 32-row atom (tile and nested sub-tile edges multiples of 32); updates whose depth is
+    // not a whole number of 64-column stages use the cp.async path
     if (g->prec == MTD_PREC_TF32 && vec2 && g->dag.tile() % 32 == 0 && g->nest % 32 == 0)
         mtd::encode_tmap(a, dA, g->dag.n(), lda);
     const int grid = g->num_sms;

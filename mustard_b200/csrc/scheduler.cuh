@@ -195,9 +195,9 @@ __device__ __forceinline__ int op_update_tc(const RunArgs &p, const MatCtx &m, c
     float *C = at<float>(m, t.cr + r0, t.cc + c0);
     // SYRK's B panel starts in the same column as A; GEMM_NT's may not
     const int bcol = t.op == MTD_OP_SYRK_LN ? t.ac : t.bc;
-    const bool ok = (tmap && t.k % tc::kBK == 0 && t.ac == bcol)
-                        ? tc::gemm_nt_tma<kThreads>(tcs, s, tmap, t.ar + r0, brow, t.ac, t.k, mm, nn, C, m.lda, lower,
-                                                    0, 0, p.timeout_ns)
+    const bool ok = (tmap && t.k % tc::kTmaBK == 0 && t.ac == bcol)
+                        ? tc::gemm_nt_tma<kThreads>(tcs, s, tmap, p.tma, t.ar + r0, brow, t.ac, t.k, mm, nn, C, m.lda,
+                                                    lower, 0, 0, p.timeout_ns)
                         : tc::gemm_nt<kThreads>(tcs, s, at<float>(m, t.ar + r0, t.ac), m.lda, B, m.lda, mm, nn, t.k, C,
                                                 m.lda, lower, 0, 0, p.timeout_ns);
     if (!ok) {

@@ -284,44 +284,72 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const void *map, int x
         : "memory");
 }
 
-// C -= A B^T as gemm_nt, with both operands fetched by TMA from the matrix `map` describes
-// (FP32, boxes of 32 rows x 32 columns, 128-byte swizzle with 32-byte atoms: box row k holds
-// 32 consecutive MN elements of column k, its 32-byte chunks at c ^ (k % 4)): A = rows
-// a_row .. a_row + 127, B = rows b_row .., columns k0 .. k0 + K - 1 (K a multiple of 32;
-// rows past the matrix read as zero).  One thread runs the whole pipeline: per stage one
-// expect_tx + 8 box loads on full[s], then, once the stage has landed, 4 MMAs committed to
-// mbar[s]; a stage is reloaded after its MMAs are done.  Operands must already be TF32
-// values (the tensor core truncates what it reads).
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const void *map, int x, int y, int z, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+        : "memory");
+}
+
+// TMA pipeline geometry: 64-deep k-slices, 3 stages of 64 KB (A then B).  An operand slice is
+// 4 MN atoms of 32 rows, each atom 64 K-rows of 128 bytes (8 KB), K-rows 128 bytes apart.
+constexpr int kTmaBK = 64;
+constexpr int kTmaStages = 3;
+constexpr int kTmaAtomBytes = 32 * kTmaBK * 4;                // 8 KB
+constexpr int kTmaOperandBytes = 4 * kTmaAtomBytes;           // 32 KB
+constexpr int kTmaStageBytes = 2 * kTmaOperandBytes;          // 64 KB
+static_assert(kTmaStages * kTmaStageBytes <= kSmemBytes, "TMA stages fit the engine's shared memory");
+static_assert(kTmaStages <= kStages, "TMA stages use the engine's barriers");
+enum { kTmaNone = 0, kTmaMap2D = 1, kTmaMap3D = 2 };
+
+// C -= A B^T as gemm_nt, with both operands fetched by TMA from the FP32 matrix `map`
+// describes, 128-byte swizzle with 32-byte atoms (an atom row k holds 32 consecutive MN
+// elements of column k, its 32-byte chunks at c ^ (k % 4)).  A = rows a_row .. a_row + 127,
+// B = rows b_row .., columns k0 .. k0 + K - 1 (K a multiple of 64; a_row, b_row multiples of
+// 32; rows past the matrix read as zero).  map_kind kTmaMap3D: dims (32 rows of an atom,
+// columns, atoms), box 32 x 64 x 4, one load per operand and stage; kTmaMap2D: dims (rows,
+// columns), box 32 x 64, four loads per operand and stage (the number of TMA instructions,
+// not the bytes, limited the 32 x 32 boxes of the first design to ~25 GB/s per SM).  One
+// thread runs the pipeline: per stage one expect_tx and the loads on full[s], then, once the
+// stage has landed, 8 MMAs committed to mbar[s]; a stage is reloaded after its MMAs are done.
+// Operands must already be TF32 values (the tensor core truncates what it reads).
 template <int THREADS>
-__device__ bool gemm_nt_tma(State *st, uint8_t *smem, const void *map, int a_row, int b_row, int k0, int K, int M,
-                            int N, float *C, int64_t ldc, bool lower_only, int r0, int c0, unsigned long long timeout_ns) {
-    constexpr uint32_t kBoxBytes = 32 * 32 * 4;
+__device__ bool gemm_nt_tma(State *st, uint8_t *smem, const void *map, int map_kind, int a_row, int b_row, int k0,
+                            int K, int M, int N, float *C, int64_t ldc, bool lower_only, int r0, int c0,
+                            unsigned long long timeout_ns) {
     bool ok = true;
     if (threadIdx.x == 0) {
         const unsigned long long deadline = now_ns() + timeout_ns;
-        const int nk = K / kBK;
+        const int nk = K / kTmaBK;
         uint32_t ph = st->phases, fph = st->fphases;
         auto issue = [&](int s, int kt) {
-            const uint32_t bar = smem_addr(&st->full[s]), base = smem_addr(smem + s * kStageBytes);
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(8 * kBoxBytes)
+            const uint32_t bar = smem_addr(&st->full[s]), base = smem_addr(smem + s * kTmaStageBytes);
+            const int k = k0 + kt * kTmaBK;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kTmaStageBytes)
                          : "memory");
-            for (int i = 0; i < 4; ++i) {
-                tma_load_2d(base + i * kBoxBytes, map, a_row + 32 * i, k0 + kt * kBK, bar);
-                tma_load_2d(base + kOperandBytes + i * kBoxBytes, map, b_row + 32 * i, k0 + kt * kBK, bar);
+            if (map_kind == kTmaMap3D) {
+                tma_load_3d(base, map, 0, k, a_row >> 5, bar);
+                tma_load_3d(base + kTmaOperandBytes, map, 0, k, b_row >> 5, bar);
+            } else {
+                for (int i = 0; i < 4; ++i) {
+                    tma_load_2d(base + i * kTmaAtomBytes, map, a_row + 32 * i, k, bar);
+                    tma_load_2d(base + kTmaOperandBytes + i * kTmaAtomBytes, map, b_row + 32 * i, k, bar);
+                }
             }
         };
-        for (int s = 0; s < kStages && s < nk; ++s) issue(s, s);
+        for (int s = 0; s < kTmaStages && s < nk; ++s) issue(s, s);
         for (int kt = 0; kt < nk && ok; ++kt) {
-            const int s = kt % kStages;
+            const int s = kt % kTmaStages;
             ok = wait_bar(&st->full[s], (fph >> s) & 1u, deadline);
             fph ^= 1u << s;
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t a0 = smem_addr(smem + s * kStageBytes), b0 = a0 + kOperandBytes;
+            const uint32_t a0 = smem_addr(smem + s * kTmaStageBytes), b0 = a0 + kTmaOperandBytes;
 #pragma unroll
-            for (int g = 0; g < kBK / 8; ++g) {
-                // boxes of 32 MN x 32 K: MN atoms one box apart, K atoms (4 rows) 512 bytes apart
-                const uint64_t lead = uint64_t(kBoxBytes >> 4) << 16, stride = uint64_t(512 >> 4) << 32;
+            for (int g = 0; g < kTmaBK / 8; ++g) {
+                // MN atoms kTmaAtomBytes apart, groups of 4 K-rows 512 bytes apart
+                const uint64_t lead = uint64_t(kTmaAtomBytes >> 4) << 16, stride = uint64_t(512 >> 4) << 32;
                 const uint64_t ad = uint64_t(((a0 + g * 1024) >> 4) & 0x3fff) | lead | stride | (1ull << 46) | (1ull << 61);
                 const uint64_t bd = uint64_t(((b0 + g * 1024) >> 4) & 0x3fff) | lead | stride | (1ull << 46) | (1ull << 61);
                 asm volatile(
@@ -335,17 +363,17 @@ __device__ bool gemm_nt_tma(State *st, uint8_t *smem, const void *map, int a_row
                              smem_addr(&st->mbar[s]))
                          : "memory");
             // reload the stage of k-slice kt - 1 once its MMAs are done
-            if (kt > 0 && kt - 1 + kStages < nk) {
-                const int sp = (kt - 1) % kStages;
+            if (kt > 0 && kt - 1 + kTmaStages < nk) {
+                const int sp = (kt - 1) % kTmaStages;
                 ok = wait_bar(&st->mbar[sp], (ph >> sp) & 1u, deadline);
                 ph ^= 1u << sp;
-                if (ok) issue(sp, kt - 1 + kStages);
+                if (ok) issue(sp, kt - 1 + kTmaStages);
             }
         }
-        // consume the commits not waited above (the last kStages k-slices, in order), so the
-        // barriers' parities stay in step; the last one means the accumulator is complete
-        for (int kt = nk > kStages ? nk - kStages : 0; kt < nk && ok; ++kt) {
-            const int s = kt % kStages;
+        // consume the commits not waited above (the last kTmaStages k-slices, in order), so
+        // the barriers' parities stay in step; the last one means the accumulator is complete
+        for (int kt = nk > kTmaStages ? nk - kTmaStages : 0; kt < nk && ok; ++kt) {
+            const int s = kt % kTmaStages;
             ok = wait_bar(&st->mbar[s], (ph >> s) & 1u, deadline);
             ph ^= 1u << s;
         }
