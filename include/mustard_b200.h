@@ -126,6 +126,10 @@ int mtd_graph_num_device_tasks(const mtd_graph *g);
 /* Number of device work items task `task` is split into (0 before finalize). */
 int mtd_graph_task_items(const mtd_graph *g, int task);
 
+/* Operation (mtd_op; 100 for a zero-work join) of device task `task` after finalize, the
+ * task index the trace records carry; a negative status otherwise. */
+int mtd_graph_device_task_op(const mtd_graph *g, int task);
+
 /* Validate and upload the DAG: predecessor counts (the reference's h_dependencies,
  * cholesky_mustard.cu:422-425), successor lists (what insertDependencyKernel wires,
  * mustard/mustard.h:197-211), work items, priorities, queues and workspace.  Replaces

@@ -120,6 +120,13 @@ class TaskGraph:
     def items(self, task):
         return self._lib.mtd_graph_task_items(self._h, task)
 
+    def device_task_op(self, task):
+        """Operation (OP_*; 100 for a join) of device task ``task``, the index trace records carry."""
+        op = self._lib.mtd_graph_device_task_op(self._h, task)
+        if op < 0:
+            raise MtdError(-op)
+        return op
+
     @property
     def num_device_tasks(self):
         """Device tasks after finalize (nested diagonal factorisations expanded)."""

@@ -296,6 +296,11 @@ int mtd_graph_task_items(const mtd_graph *g, int task) {
     return g->finalized ? g->low.host_items[task] : 0;
 }
 
+int mtd_graph_device_task_op(const mtd_graph *g, int task) {
+    if (!g || !g->finalized || task < 0 || task >= static_cast<int>(g->low.tasks.size())) return -MTD_ERR_INVALID_ARG;
+    return g->low.tasks[task].op;
+}
+
 int mtd_graph_set_trace(mtd_graph *g, int enable) {
     if (!g) return MTD_ERR_INVALID_ARG;
     if (g->finalized) return MTD_ERR_STATE;

@@ -128,45 +128,266 @@ __device__ __forceinline__ void lower_inverse(int jn, TL tl, E *X) {
     __syncthreads();
 }
 
-// Cholesky of the jn x jn diagonal block at Ad (lower), in shared memory.  Writes L back
-// (lower triangle only; the strict upper triangle is never touched, as with LAPACK's
-// uplo = 'L') and L^-1 to Wd (ld = m.wsld, full block with zeros above).
+// Cholesky of the n x n diagonal block at Ad (n <= kSmallChol, lower; the strict upper
+// triangle is never touched, as with LAPACK's uplo = 'L'), and the inverses of its kNB-row
+// diagonal blocks to Wd (Wd[r + c * ldw], full kNB x kNB blocks with zeros above the
+// diagonal).  The block is held in shared memory and factored in panels of PW columns
+// (16 in FP64, 32 in FP32, so that a row of the panel fits in registers):
+//   - warp 0 factors the panel's PW x PW diagonal block in registers (lane r holds row r;
+//     column j is broadcast with shuffles: no block barrier inside the panel) with the
+//     arithmetic of LAPACK's dpotf2 (l(r, j) = d(r, j) * (1 / sqrt(d(j, j))), then the
+//     rank-1 update; the reciprocal square root is CUDA's rsqrt, within 1 ulp), and then
+//     its inverse (lane c forms column c by forward substitution);
+//   - the whole CTA computes the panel below it, P = A_panel X^T, and the trailing update
+//     A -= P P^T (lower), each followed by one barrier.
+// The kNB x kNB inverses are composed from the panel inverses by doubling:
+// inv([La 0; L21 Lb]) = [Xa 0; -Xb (L21 Xa) Xb].
+// (The first design synchronised the CTA three times per column and formed the inverse
+// row by row: ~170 us for a 128 x 128 block, which made the chain of nested diagonal
+// factorisations the critical path of the TF32 factor.)
+constexpr int kSmallChol = 128;
+constexpr int kSmallLd = kSmallChol + 1;
+constexpr int kInvLd = kNB + 1;
 template <typename T>
-__device__ __forceinline__ int factor_chol_diag(const RunArgs &p, const MatCtx &m, T *Ad, int jn, T *Wd, void *smem_raw,
-                                                int info_base) {
-    const int tid = threadIdx.x;
-    T *D = static_cast<T *>(smem_raw);
-    T *X = D + kNB * kDiagLd;
-    const int64_t lda = m.lda;
-    for (int e = tid; e < jn * jn; e += kThreads) {
-        const int r = e % jn, c = e / jn;
-        D[r + c * kDiagLd] = (r >= c) ? ld_cg(Ad + r + int64_t(c) * lda) : T(0);
+constexpr int chol_panel() {
+    return sizeof(T) == 8 ? 16 : 32;
+}
+template <typename T>
+constexpr int chol_small_smem_bytes() {
+    // the block, the inverses of its two kNB-row diagonal blocks, a 2 x 32 x 33 scratch
+    // product, 1 / L(r, r), the failure flag
+    return int(sizeof(T)) * (kSmallChol * kSmallLd + 2 * kNB * kInvLd + 2 * 32 * 33 + kSmallChol + 1);
+}
+
+// Warp 0: Cholesky of the pw x pw block at S(p0, p0) (pw <= PW) in registers, L written
+// back to S (lower part), 1 / L(r, r) to rdiag[r], and X = L^-1 to X (leading dimension
+// kInvLd, lower part).  Returns the 0-based column of the first non-positive pivot, or -1.
+template <typename T, int PW>
+__device__ __forceinline__ int warp_chol(T *S, int p0, int pw, T *rdiag, T *X) {
+    const int lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    T a[PW];
+#pragma unroll
+    for (int c = 0; c < PW; ++c)
+        a[c] = (lane < pw && c <= lane) ? S[(p0 + lane) + (p0 + c) * kSmallLd] : T(0);
+    T myd = T(1), myrs = T(1);
+    int bad = -1;
+#pragma unroll
+    for (int j = 0; j < PW; ++j) {
+        if (j < pw && bad < 0) {
+            const T d = __shfl_sync(full, a[j], j);
+            if (!(d > T(0))) {  // also catches NaN; the same value in every lane
+                bad = j;
+            } else {
+                const T rs = rsqrt(d);
+                if (lane == j) {
+                    myd = d;
+                    myrs = rs;
+                }
+                const T l = a[j] * rs;  // l(lane, j) for lane > j
+                a[j] = l;
+#pragma unroll
+                for (int c = j + 1; c < PW; ++c) {
+                    const T lc = __shfl_sync(full, l, c);
+                    a[c] -= l * lc;
+                }
+            }
+        }
     }
+    if (bad >= 0) return bad;
+    // L back to S (the diagonal as sqrt of the pivot, formed once here, off the chain)
+    if (lane < pw) {
+#pragma unroll
+        for (int c = 0; c < PW; ++c)
+            if (c < lane) S[(p0 + lane) + (p0 + c) * kSmallLd] = a[c];
+        S[(p0 + lane) + (p0 + lane) * kSmallLd] = sqrt(myd);
+        rdiag[lane] = myrs;
+    }
+    __syncwarp();
+    // X = L^-1: lane c forms column c, rows i >= c, by forward substitution in registers
+    // (fully unrolled: the loads of L do not wait on the recurrence, which carries one
+    // multiply-add per row: the newest x[i - 1] enters the sum last)
+    T x[PW];
+#pragma unroll
+    for (int i = 0; i < PW; ++i) {
+        if (i < pw) {
+            T s0 = (i == lane) ? T(1) : T(0), s1 = T(0);
+#pragma unroll
+            for (int l = 0; l + 1 < i; ++l) {
+                const T v = S[(p0 + i) + (p0 + l) * kSmallLd] * x[l];
+                if (l & 1) s1 -= v;
+                else s0 -= v;
+            }
+            if (i > 0) s0 -= S[(p0 + i) + (p0 + i - 1) * kSmallLd] * x[i - 1];
+            x[i] = (s0 + s1) * rdiag[i];
+        } else {
+            x[i] = T(0);
+        }
+    }
+    if (lane < pw) {
+#pragma unroll
+        for (int i = 0; i < PW; ++i)
+            if (i >= lane && i < pw) X[i + lane * kInvLd] = x[i];
+    }
+    return -1;
+}
+
+// Not inlined: its register-heavy phases are allocated on their own, so they do not raise
+// the register pressure (or cause spills) in the GEMM paths of the persistent kernel.
+template <typename T>
+__device__ __noinline__ int chol_small(const RunArgs &p, const MatCtx &m, T *Ad, int n, T *Wd, void *smem_raw,
+                                      int info_base) {
+    static_assert(kThreads == 512, "work split over 512 threads");
+    static_assert(kNB == 64, "two kNB-row inverse blocks per 128-row block");
+    constexpr int PW = chol_panel<T>();
+    const int tid = threadIdx.x;
+    T *S = static_cast<T *>(smem_raw);              // the block, then L (column-major, kSmallLd)
+    T *XI = S + kSmallChol * kSmallLd;              // inverses of the kNB-row diagonal blocks
+    T *T1 = XI + 2 * kNB * kInvLd;                  // scratch products of the composition
+    T *rdiag = T1 + 2 * 32 * 33;                    // 1 / L(r, r)
+    int *flag = reinterpret_cast<int *>(rdiag + kSmallChol);
+    const int64_t lda = m.lda;
+    // load the lower triangle: each batch of a thread's loads issues before its stores
+    {
+        constexpr int kPer = kSmallChol * kSmallChol / kThreads, kBatch = 8;  // 32 elements, 4 batches
+        const int r = tid & (kSmallChol - 1);
+#pragma unroll 1
+        for (int h = 0; h < kPer / kBatch; ++h) {
+            T v[kBatch];
+#pragma unroll
+            for (int i = 0; i < kBatch; ++i) {
+                const int c = (tid + (h * kBatch + i) * kThreads) >> 7;
+                v[i] = (r < n && c < n && r >= c) ? ld_cg(Ad + r + int64_t(c) * lda) : T(0);
+            }
+#pragma unroll
+            for (int i = 0; i < kBatch; ++i) S[r + ((tid + (h * kBatch + i) * kThreads) >> 7) * kSmallLd] = v[i];
+        }
+    }
+    if (tid == 0) *flag = -1;
     __syncthreads();
-    for (int j = 0; j < jn; ++j) {
-        const T djj = D[j + j * kDiagLd];
-        if (!(djj > T(0)))  // also catches NaN
-            return diag_failure(p, m, MTD_ERR_NOT_POSITIVE_DEFINITE, info_base + j + 1);
-        const T s = sqrt(djj);
-        const T rs = T(1) / s;
+    for (int p0 = 0; p0 < n; p0 += PW) {
+        const int pw = min(PW, n - p0);
+        T *X = XI + (p0 / kNB) * kNB * kInvLd + (p0 % kNB) * (1 + kInvLd);  // panel inverse, kInvLd
+        if (tid < 32) {
+            const int bad = warp_chol<T, PW>(S, p0, pw, rdiag + p0, X);
+            if (tid == 0 && bad >= 0) *flag = p0 + bad;
+        }
         __syncthreads();
-        for (int r = j + 1 + tid; r < jn; r += kThreads) D[r + j * kDiagLd] *= rs;
-        if (tid == 0) D[j + j * kDiagLd] = s;
+        const int bad = *flag;  // every thread reads the same flag
+        if (bad >= 0) return diag_failure(p, m, MTD_ERR_NOT_POSITIVE_DEFINITE, info_base + bad + 1);
+        const int q0 = p0 + pw, nr = n - q0;
+        if (nr <= 0) break;
+        // panel below: P(r, c) = sum_{l <= c} A(r, p0 + l) X(c, l), rows q0 .., four columns a unit
+        {
+            const int groups = (pw + 3) >> 2, units = nr * groups;
+            T out[2][4];
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int u = tid + k * kThreads;
+                if (u >= units) continue;
+                const int r = q0 + u % nr, c0 = 4 * (u / nr);
+                T acc[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll 2
+                for (int l = 0; l < PW; ++l) {
+                    if (l >= pw) break;
+                    const T av = S[r + (p0 + l) * kSmallLd];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (l <= c0 + q && c0 + q < pw) acc[q] += av * X[(c0 + q) + l * kInvLd];
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) out[k][q] = acc[q];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int u = tid + k * kThreads;
+                if (u >= units) continue;
+                const int r = q0 + u % nr, c0 = 4 * (u / nr);
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (c0 + q < pw) S[r + (p0 + c0 + q) * kSmallLd] = out[k][q];
+            }
+            __syncthreads();
+        }
+        // trailing update: A(r, c) -= sum_l P(r, l) P(c, l), r >= c >= q0, in 4 x 4 blocks
+        {
+            const int nb4 = (nr + 3) >> 2, blocks = nb4 * (nb4 + 1) / 2;
+            if (tid < blocks) {
+                int br = int((sqrtf(8.0f * float(tid) + 1.0f) - 1.0f) * 0.5f);
+                while ((br + 1) * (br + 2) / 2 <= tid) ++br;
+                while (br * (br + 1) / 2 > tid) --br;
+                const int r0 = q0 + 4 * br, c0 = q0 + 4 * (tid - br * (br + 1) / 2);
+                T acc[4][4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc[i][q] = T(0);
+#pragma unroll 2
+                for (int l = 0; l < PW; ++l) {
+                    if (l >= pw) break;
+                    T x[4], y[4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        x[i] = S[min(r0 + i, kSmallChol - 1) + (p0 + l) * kSmallLd];
+                        y[i] = S[min(c0 + i, kSmallChol - 1) + (p0 + l) * kSmallLd];
+                    }
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) acc[i][q] += x[i] * y[q];
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int r = r0 + i, c = c0 + q;
+                        if (r < n && c < n && r >= c) S[r + c * kSmallLd] -= acc[i][q];
+                    }
+            }
+            __syncthreads();
+        }
+    }
+    // L to the matrix
+    for (int e = tid; e < n * kSmallChol; e += kThreads) {
+        const int r = e & (kSmallChol - 1), c = e >> 7;
+        if (r < n && r >= c) Ad[r + int64_t(c) * lda] = S[r + c * kSmallLd];
+    }
+    // kNB-row inverses by doubling: for each pair of adjacent h-blocks (a above b) inside a
+    // kNB block, X21 = -Xb (L21 Xa); all pairs of a level at once, two barriers a level
+    for (int h = PW; h < kNB; h *= 2) {
+        const int pairs = kSmallChol / (2 * h);
+        // T1 = L21 Xa  (hb x h per pair; Xa lower)
+        for (int e = tid; e < pairs * h * h; e += kThreads) {
+            const int pr = e / (h * h), r = e % h, c = (e / h) % h;
+            const int g0 = pr * 2 * h, hb = min(h, n - g0 - h);  // rows of the lower half
+            if (hb <= 0 || r >= hb) continue;
+            const T *Xa = XI + (g0 / kNB) * kNB * kInvLd + (g0 % kNB) * (1 + kInvLd);
+            T acc = T(0);
+            for (int l = c; l < h; ++l) acc += S[(g0 + h + r) + (g0 + l) * kSmallLd] * Xa[l + c * kInvLd];
+            T1[pr * h * (h + 1) + r + c * (h + 1)] = acc;
+        }
         __syncthreads();
-        const int rest = jn - j - 1;
-        for (int e = tid; e < rest * rest; e += kThreads) {
-            const int r = j + 1 + e % rest, c = j + 1 + e / rest;
-            if (r >= c) D[r + c * kDiagLd] -= D[r + j * kDiagLd] * D[c + j * kDiagLd];
+        // X21 = -Xb T1  (Xb lower), into the composed inverse
+        for (int e = tid; e < pairs * h * h; e += kThreads) {
+            const int pr = e / (h * h), r = e % h, c = (e / h) % h;
+            const int g0 = pr * 2 * h, hb = min(h, n - g0 - h);
+            if (hb <= 0 || r >= hb) continue;
+            T *Xg = XI + (g0 / kNB) * kNB * kInvLd + (g0 % kNB) * (1 + kInvLd);  // the 2h block
+            const T *Xb = Xg + h * (1 + kInvLd);
+            T acc = T(0);
+            for (int l = 0; l <= r; ++l) acc += Xb[r + l * kInvLd] * T1[pr * h * (h + 1) + l + c * (h + 1)];
+            Xg[(h + r) + c * kInvLd] = -acc;
         }
         __syncthreads();
     }
-    lower_inverse<false>(jn, [&](int i, int l) { return D[i + l * kDiagLd]; }, X);
     const int64_t ldw = m.wsld;
-    for (int e = tid; e < jn * jn; e += kThreads) {
-        const int r = e % jn, c = e / jn;
-        if (r >= c) Ad[r + int64_t(c) * lda] = D[r + c * kDiagLd];
-        Wd[r + int64_t(c) * ldw] = X[r + c * kDiagLd];
+    for (int e = tid; e < n * kNB; e += kThreads) {
+        const int r = e % n, c = e / n;
+        const int b0 = (r / kNB) * kNB;
+        if (c < min(kNB, n - b0)) Wd[r + int64_t(c) * ldw] = (r - b0 >= c) ? XI[(b0 / kNB) * kNB * kInvLd + (r - b0) + c * kInvLd] : T(0);
     }
+    __syncthreads();
     return 0;
 }
 
@@ -221,6 +442,11 @@ __device__ int op_potrf(const RunArgs &p, const MatCtx &m, const DevTask &t, voi
     T *A = at<T>(m, t.cr, t.cc);
     T *W = ws_lo<T>(m) + t.cr;
     const int64_t lda = m.lda, ldw = m.wsld;
+    if (n <= kSmallChol) {  // the whole block in shared memory
+        const int st = chol_small<T>(p, m, A, n, W, smem, t.cc);
+        block_fence_sync();
+        return st;
+    }
     for (int jb = 0; jb < n; jb += kNB) {
         const int jn = min(kNB, n - jb);
         if (jb > 0) {
@@ -234,7 +460,7 @@ __device__ int op_potrf(const RunArgs &p, const MatCtx &m, const DevTask &t, voi
             }
             block_fence_sync();
         }
-        const int st = factor_chol_diag<T>(p, m, A + jb + int64_t(jb) * lda, jn, W + jb, smem, t.cc + jb);
+        const int st = chol_small<T>(p, m, A + jb + int64_t(jb) * lda, jn, W + jb, smem, t.cc + jb);
         if (st) return st;
         block_fence_sync();
         // A[jb+jn:n, jb:jb+jn] = A[jb+jn:n, jb:jb+jn] * L_jj^-T
@@ -454,9 +680,11 @@ constexpr int kOpSmemBytes() {
     constexpr int g3 = BlockMmaT<double, kGemmTile, kGemmTile, kGemmWarpsM, kGemmWarpsN, kBKContig, 2, MTD_GEMM_STAGES,
                                  MTD_GEMM_BK, 1, kAKContig>::SMEM_BYTES;
     constexpr int diag = 5 * kNB * kDiagLd * 8;  // the adjoint's diagonal block: five 64 x 64 blocks
+    constexpr int chol = chol_small_smem_bytes<double>();
     constexpr int m12 = g1 > g2 ? g1 : g2;
     constexpr int m = m12 > g3 ? m12 : g3;
-    return m > diag ? m : diag;
+    constexpr int d = diag > chol ? diag : chol;
+    return m > d ? m : d;
 }
 
 }  // namespace mtd

