@@ -17,6 +17,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
                      "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]
+# engine-shape overrides for tuning builds, e.g. MTD_NVCC_EXTRA="-DMTD_PANEL_STAGES=4"
+CUDA_FLAGS += os.environ.get("MTD_NVCC_EXTRA", "").split()
 
 LIB_SOURCES = ["runtime.cu", "gen.cu", "dag.cpp", "solver.cu", "batch.cu", "adjoint.cu"]
 CLI_PROGRAMS = {"lu_mustard": "lu_mustard.cpp", "cholesky_mustard": "cholesky_mustard.cpp"}

@@ -40,6 +40,16 @@ constexpr int kDiagLd = kNB + 1;  // shared-memory leading dimension of a diagon
 #ifndef MTD_PANEL_WARPS_M
 #define MTD_PANEL_WARPS_M 4
 #endif
+// Panel engine (64 x 64 blocks: TRSM strips, updates inside diagonal factorisations):
+// 4 stages of 32-deep k-slices.  Measured at N = 32768, tile 1536: TRSM item 598 -> 398 us
+// (TF32) and 957 -> 886 us (FP64) against 3 stages of 16, whose ~24 KB in flight left each
+// step waiting on L2 round trips; 5-6 stages or 64-deep slices gave nothing more.
+#ifndef MTD_PANEL_STAGES
+#define MTD_PANEL_STAGES 4
+#endif
+#ifndef MTD_PANEL_BK
+#define MTD_PANEL_BK 32
+#endif
 constexpr int kGemmWarpsM = MTD_GEMM_WARPS_M;
 constexpr int kGemmWarpsN = kThreads / 32 / kGemmWarpsM;
 constexpr int kPanelWarpsM = MTD_PANEL_WARPS_M;
@@ -48,7 +58,7 @@ template <int BL, int VEC, typename T = double, int SPLIT = 1>
 using GemmMma =
     BlockMmaT<T, kGemmTile, kGemmTile, kGemmWarpsM, kGemmWarpsN, BL, VEC, MTD_GEMM_STAGES, MTD_GEMM_BK, SPLIT>;
 template <int BL, int VEC, typename T = double, int SPLIT = 1>
-using PanelMma = BlockMmaT<T, 64, 64, kPanelWarpsM, kPanelWarpsN, BL, VEC, 3, 16, SPLIT>;
+using PanelMma = BlockMmaT<T, 64, 64, kPanelWarpsM, kPanelWarpsN, BL, VEC, MTD_PANEL_STAGES, MTD_PANEL_BK, SPLIT>;
 
 __device__ __forceinline__ void block_fence_sync() {
     __threadfence_block();
@@ -681,7 +691,11 @@ constexpr int kOpSmemBytes() {
                                  MTD_GEMM_BK, 1, kAKContig>::SMEM_BYTES;
     constexpr int diag = 5 * kNB * kDiagLd * 8;  // the adjoint's diagonal block: five 64 x 64 blocks
     constexpr int chol = chol_small_smem_bytes<double>();
-    constexpr int m12 = g1 > g2 ? g1 : g2;
+    constexpr int pn = PanelMma<kBNContig, 2>::SMEM_BYTES > PanelMma<kBKContig, 2>::SMEM_BYTES
+                           ? PanelMma<kBNContig, 2>::SMEM_BYTES
+                           : PanelMma<kBKContig, 2>::SMEM_BYTES;
+    static_assert(pn <= 227 * 1024, "panel engine stages fit shared memory");
+    constexpr int m12 = (g1 > g2 ? g1 : g2) > pn ? (g1 > g2 ? g1 : g2) : pn;
     constexpr int m = m12 > g3 ? m12 : g3;
     constexpr int d = diag > chol ? diag : chol;
     return m > d ? m : d;
