@@ -130,6 +130,10 @@ int mtd_graph_task_items(const mtd_graph *g, int task);
  * task index the trace records carry; a negative status otherwise. */
 int mtd_graph_device_task_op(const mtd_graph *g, int task);
 
+/* Copy device task `task`'s predecessor device tasks into out[0..cap) after finalize (for
+ * critical-path analysis of traces); returns the full count or a negative status. */
+int mtd_graph_device_task_deps(const mtd_graph *g, int task, int *out, int cap);
+
 /* Validate and upload the DAG: predecessor counts (the reference's h_dependencies,
  * cholesky_mustard.cu:422-425), successor lists (what insertDependencyKernel wires,
  * mustard/mustard.h:197-211), work items, priorities, queues and workspace.  Replaces

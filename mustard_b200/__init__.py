@@ -120,6 +120,15 @@ class TaskGraph:
     def items(self, task):
         return self._lib.mtd_graph_task_items(self._h, task)
 
+    def device_task_deps(self, task):
+        """Predecessor device tasks of device task ``task`` (after finalize)."""
+        cnt = self._lib.mtd_graph_device_task_deps(self._h, task, None, 0)
+        if cnt < 0:
+            raise MtdError(-cnt)
+        buf = (ctypes.c_int * max(cnt, 1))()
+        self._lib.mtd_graph_device_task_deps(self._h, task, buf, cnt)
+        return list(buf[:cnt])
+
     def device_task_op(self, task):
         """Operation (OP_*; 100 for a join) of device task ``task``, the index trace records carry."""
         op = self._lib.mtd_graph_device_task_op(self._h, task)
@@ -301,8 +310,7 @@ class SpdSolver:
             pass
 
 
-def batch_autotune(sizes, prec=_capi.PREC_FP64, stream=None):
-    """(tiles, nests, wall ms) chosen by mtd_batch_autotune for a batch of these sizes."""
+def _autotune_call(sizes, prec, stream):
     c = len(sizes)
     n = (ctypes.c_int64 * c)(*sizes)
     t = (ctypes.c_int64 * c)()
@@ -310,6 +318,35 @@ def batch_autotune(sizes, prec=_capi.PREC_FP64, stream=None):
     ms = ctypes.c_double(0.0)
     _capi.check(lib().mtd_batch_autotune(c, n, prec, t, k, ctypes.byref(ms), _stream_handle(stream)))
     return list(t), list(k), ms.value
+
+
+def batch_autotune(sizes, prec=_capi.PREC_FP64, stream=None, table=None):
+    """(tiles, nests, wall ms) chosen by mtd_batch_autotune for a batch of these sizes.
+
+    ``table``: path of a JSON file of earlier choices (mustard_b200.tune_table), kept per
+    device and precision.  Sizes it holds are not tuned again; the others are tuned with
+    their share of this batch (so the trial counts are the ones a full call would use), and
+    their choices are added to the file."""
+    if table is None:
+        return _autotune_call(sizes, prec, stream)
+    import torch
+    from . import tune_table
+    device = torch.cuda.get_device_name(torch.cuda.current_device())
+    tab = tune_table.load(table)
+    todo = tune_table.missing(tab, device, prec, sizes)
+    ms = 0.0
+    if todo:
+        sub = [sizes[i] for i in todo]
+        t, k, ms = _autotune_call(sub, prec, stream)
+        for n, ti, ki in zip(sub, t, k):
+            tune_table.record(tab, device, prec, n, ti, ki)
+        tune_table.save(tab, table)
+    tiles, nests = [], []
+    for n in sizes:
+        ti, ki = tune_table.lookup(tab, device, prec, n)
+        tiles.append(ti)
+        nests.append(ki)
+    return tiles, nests, ms
 
 
 class Batch:

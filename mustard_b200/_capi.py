@@ -80,6 +80,7 @@ SIGNATURES = {
     "mtd_graph_get_deps": (_i, [_vp, _i, ctypes.POINTER(_i), _i]),
     "mtd_graph_task_items": (_i, [_vp, _i]),
     "mtd_graph_device_task_op": (_i, [_vp, _i]),
+    "mtd_graph_device_task_deps": (_i, [_vp, _i, ctypes.POINTER(ctypes.c_int), _i]),
     "mtd_graph_num_device_tasks": (_i, [_vp]),
     "mtd_graph_finalize": (_i, [_vp]),
     "mtd_graph_set_trace": (_i, [_vp, _i]),

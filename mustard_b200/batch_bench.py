@@ -61,6 +61,8 @@ def main():
     ap.add_argument("--precs", default="fp64,fp32")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--tune-table", default=None,
+                    help="JSON table of autotuner choices to reuse and extend (mustard_b200.tune_table)")
     args = ap.parse_args()
     sizes, nrhs, groups, rhs = make_batch(args.count, args.seed)
     count = args.count
@@ -80,7 +82,7 @@ def main():
             for n, (idx, w) in work_groups.items():
                 w.copy_(pristine[n])
 
-        tiles, nests, tune_ms = mtd.batch_autotune(sizes, prec)
+        tiles, nests, tune_ms = mtd.batch_autotune(sizes, prec, table=args.tune_table)
         chosen = {n: (tiles[sizes.index(n)], nests[sizes.index(n)]) for n in sorted(set(sizes))}
         print(json.dumps(dict(base, prec=pname, step="autotune", wall_ms=tune_ms,
                               choice={str(n): list(v) for n, v in chosen.items()})), flush=True)

@@ -5,7 +5,10 @@
 
 namespace mtd {
 
-constexpr int kNumQueues = 2;   // 0: critical path (diagonal, panel, next-panel updates); 1: rest
+// Ready queues, popped in order: 0 critical path (diagonal factorisations, panel solves,
+// diagonal-tile updates, updates of the next panel column); 1 updates of the two panel
+// columns after it; 2 the other updates.
+constexpr int kNumQueues = 3;
 #ifndef MTD_THREADS
 #define MTD_THREADS 512
 #endif
@@ -43,7 +46,7 @@ constexpr bool is_adjoint_op(int op) { return op >= kOpAdjTrsm && op <= kOpAdjPo
 // diagonal block whose first row is r sits at ws[r + c * ws_ld], c < kNB.
 struct alignas(16) DevTask {
     int32_t op;
-    int32_t queue;       // 0 or 1
+    int32_t queue;       // ready queue, 0 .. kNumQueues - 1
     int32_t n_items;     // 0 for a join
     int32_t cr, cc;      // output block origin
     int32_t ar, ac;      // first operand (triangular block for TRSM)

@@ -301,6 +301,15 @@ int mtd_graph_device_task_op(const mtd_graph *g, int task) {
     return g->low.tasks[task].op;
 }
 
+int mtd_graph_device_task_deps(const mtd_graph *g, int task, int *out, int cap) {
+    if (!g || !g->finalized || task < 0 || task >= static_cast<int>(g->low.tasks.size()) || cap < 0 ||
+        (cap > 0 && !out))
+        return -MTD_ERR_INVALID_ARG;
+    const auto &d = g->low.preds[task];
+    for (int i = 0; i < cap && i < static_cast<int>(d.size()); ++i) out[i] = d[i];
+    return static_cast<int>(d.size());
+}
+
 int mtd_graph_set_trace(mtd_graph *g, int enable) {
     if (!g) return MTD_ERR_INVALID_ARG;
     if (g->finalized) return MTD_ERR_STATE;
@@ -697,7 +706,8 @@ extern "C" int mtd_factor_noalloc(int kind, double *dA, int64_t n, int64_t lda, 
     rc = dag.lower(kNestTile, low);
     if (rc) return rc;
     const int nt = static_cast<int>(low.tasks.size());
-    const long long items = low.queue_cap[0] + low.queue_cap[1];
+    long long items = 0;
+    for (int q = 0; q < kNumQueues; ++q) items += low.queue_cap[q];
     if (nt > kNoAllocMaxTasks || static_cast<long long>(low.succ.size()) > kNoAllocMaxEdges ||
         items > kNoAllocMaxItems)
         return MTD_ERR_TOO_LARGE;

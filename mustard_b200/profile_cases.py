@@ -14,8 +14,9 @@
 Each case runs `--runs` launches (default 2: the first is the one to capture with
 `-c 1`), checks the run status, and prints the device time of the last launch.  With
 `--trace` the runs record per-item timestamps and the line adds, per tile operation, the
-items, median and summed item time, and the busy fraction (summed item time over
-SMs x span).
+items, median and summed item time, the busy fraction (summed item time over SMs x span)
+and the critical path's composition (mustard_b200.trace_analysis); `--trace-out FILE`
+also writes the records, task spans and critical path as JSON.
 Inputs are the seeded generators of the benchmark (larger than L2 from n = 4096).
 """
 import argparse
@@ -59,6 +60,8 @@ def main():
     ap.add_argument("--runs", type=int, default=2)
     ap.add_argument("--prec", choices=["fp64", "tf32"], default="fp64")
     ap.add_argument("--trace", action="store_true", help="per-operation item-time breakdown")
+    ap.add_argument("--trace-out", default=None,
+                    help="also write the records, task spans and critical path to this JSON file")
     args = ap.parse_args()
     if args.prec == "tf32" and args.case == "lu":
         ap.error("the TF32 path factors SPD matrices only (chol, gemm)")
@@ -85,6 +88,8 @@ def main():
     if args.prec == "tf32":
         g.set_precision(mtd.PREC_TF32)
         a = a.t().contiguous().float().t()
+    if args.trace_out:
+        args.trace = True
     if args.trace:
         g.set_trace(True)
     g.finalize()
@@ -109,6 +114,10 @@ def main():
            "tflops": flops / (ms * 1e-3) / 1e12}
     if args.trace:
         rec.update(op_breakdown(g))
+        from mustard_b200 import trace_analysis
+        recs = g.trace()
+        rec["critical_path"] = (trace_analysis.dump_json(args.trace_out, g, recs) if args.trace_out
+                                else trace_analysis.summary(g, recs))["critical_path"]
     print(json.dumps(rec))
     g.close()
 

@@ -1,0 +1,89 @@
+"""Per-item device traces -> per-task spans, scheduler idle fraction, critical path, JSON.
+
+A traced run (``TaskGraph.set_trace(True)``) records, per work item, the %globaltimer times
+at which its CTA started and finished it, the SM and the device task.  From those records:
+
+- a task's span runs from its first item's start to its last item's end;
+- the busy fraction is the summed item time over (SMs x the run's span); the idle fraction
+  is the rest (queue waits, dependency stalls, the tail);
+- the critical path is walked back from the task that ended last, each time to the
+  predecessor (device task dependencies) that ended last; along it, ``wait`` is the time
+  from that predecessor's end to the task's first item start (the scheduler's hand-off
+  plus any wait for a free SM).
+
+``graph`` needs ``device_task_op(t)`` and ``device_task_deps(t)`` (a finalized TaskGraph).
+"""
+import json
+
+from ._capi import OP_NAMES
+
+
+def task_spans(graph, records):
+    """{task: {"op", "start", "end", "items", "item_ns"}} (times in ns)."""
+    spans = {}
+    for s, e, _sm, task, _item in records:
+        t = spans.get(task)
+        if t is None:
+            spans[task] = t = {"op": OP_NAMES.get(graph.device_task_op(task), "join"), "start": s, "end": e,
+                               "items": 0, "item_ns": 0}
+        t["start"] = min(t["start"], s)
+        t["end"] = max(t["end"], e)
+        t["items"] += 1
+        t["item_ns"] += e - s
+    return spans
+
+
+def busy_fraction(records):
+    if not records:
+        return 0.0
+    t0 = min(r[0] for r in records)
+    t1 = max(r[1] for r in records)
+    sms = len({r[2] for r in records})
+    return sum(e - s for s, e, _, _, _ in records) / (sms * (t1 - t0))
+
+
+def critical_path(graph, spans):
+    """Tasks on the critical path, first to last: dicts with task, op, start, end, wait (ns)."""
+    if not spans:
+        return []
+    task = max(spans, key=lambda t: spans[t]["end"])
+    path = []
+    while task is not None:
+        sp = spans[task]
+        preds = [p for p in graph.device_task_deps(task) if p in spans]
+        prev = max(preds, key=lambda p: spans[p]["end"]) if preds else None
+        wait = sp["start"] - spans[prev]["end"] if prev is not None else 0
+        path.append({"task": task, "op": sp["op"], "start": sp["start"], "end": sp["end"], "wait": wait})
+        task = prev
+    path.reverse()
+    return path
+
+
+def summary(graph, records):
+    """Busy fraction, span and the critical path's composition (per op: tasks, time in the
+    task, waits before it), in ms."""
+    spans = task_spans(graph, records)
+    path = critical_path(graph, spans)
+    t0 = min(r[0] for r in records)
+    t1 = max(r[1] for r in records)
+    per = {}
+    for step in path:
+        d = per.setdefault(step["op"], {"tasks": 0, "in_task_ms": 0.0, "wait_ms": 0.0})
+        d["tasks"] += 1
+        d["in_task_ms"] += (step["end"] - step["start"]) * 1e-6
+        d["wait_ms"] += step["wait"] * 1e-6
+    first = path[0]["start"] if path else t0
+    return {"span_ms": (t1 - t0) * 1e-6, "busy": busy_fraction(records),
+            "critical_path": {"tasks": len(path), "start_offset_ms": (first - t0) * 1e-6, "per_op": per}}
+
+
+def dump_json(path, graph, records):
+    """Write the records, the task spans and the critical path to ``path``."""
+    spans = task_spans(graph, records)
+    out = {"records": [list(r) for r in records],
+           "tasks": {str(k): v for k, v in sorted(spans.items())},
+           "critical_path": critical_path(graph, spans),
+           "summary": summary(graph, records)}
+    with open(path, "w") as f:
+        json.dump(out, f)
+    return out["summary"]

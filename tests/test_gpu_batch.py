@@ -125,3 +125,32 @@ def test_batched_factor_captured_in_a_cuda_graph(mtd):
             assert rel_diff(np.tril(from_dev(work[i])), np.tril(tiled.cholesky_lapack(a))) <= 1e-12
     del g
     b.close()
+
+
+def test_autotune_choices_factor_correctly_and_persist(mtd, tmp_path):
+    # the autotuner's per-size choices are valid tile / nested-tile edges for each size, a
+    # batch built with them factors correctly, and a JSON table makes a second tune of the
+    # same sizes free while a new size is tuned and added
+    import json
+    sizes = [96, 96, 300, 300, 520]
+    table = str(tmp_path / "tune.json")
+    tiles, nests, ms = mtd.batch_autotune(sizes, mtd.PREC_FP64, table=table)
+    assert ms > 0
+    for n, t, k in zip(sizes, tiles, nests):
+        assert 1 <= t <= n and (k == 0 or (k % 64 == 0 and k < t))
+    assert tiles[0] == tiles[1] and tiles[2] == tiles[3]  # one choice per size
+    mats = [gen.spd_input(n, 900 + i) for i, n in enumerate(sizes)]
+    b = mtd.Batch(sizes, tiles=tiles, nests=nests, prec=mtd.PREC_FP64)
+    work = [to_dev(a) for a in mats]
+    b.factor(work)
+    rc, info = b.status()
+    assert rc == 0 and all(v == 0 for v in info)
+    for i, a in enumerate(mats):
+        assert rel_diff(np.tril(from_dev(work[i])), np.tril(tiled.cholesky_lapack(a))) <= 1e-12
+    b.close()
+    t2, k2, ms2 = mtd.batch_autotune(sizes, mtd.PREC_FP64, table=table)
+    assert (t2, k2, ms2) == (tiles, nests, 0.0)
+    t3, k3, ms3 = mtd.batch_autotune(sizes + [160], mtd.PREC_FP64, table=table)
+    assert ms3 > 0 and t3[:5] == tiles and k3[:5] == nests
+    dev = json.load(open(table))["devices"]
+    assert sorted(int(n) for n in next(iter(dev.values()))["fp64"]) == [96, 160, 300, 520]

@@ -1,0 +1,42 @@
+"""Trace analysis on a synthetic trace (host logic, no GPU)."""
+import json
+
+from mustard_b200 import trace_analysis
+
+
+class FakeGraph:
+    # 0 POTRF -> 1 TRSM -> 3 GEMM ; 0 -> 2 TRSM -> 3 ; 3 -> 4 POTRF
+    ops = {0: 0, 1: 1, 2: 1, 3: 3, 4: 0}
+    deps = {0: [], 1: [0], 2: [0], 3: [1, 2], 4: [3]}
+
+    def device_task_op(self, t):
+        return self.ops[t]
+
+    def device_task_deps(self, t):
+        return self.deps[t]
+
+
+# (start, end, sm, task, item), ns
+RECORDS = [
+    (0, 100, 0, 0, 0),
+    (110, 200, 0, 1, 0), (110, 300, 1, 1, 1),   # task 1 ends at 300
+    (105, 250, 2, 2, 0),                         # task 2 ends at 250
+    (320, 400, 0, 3, 0), (330, 420, 1, 3, 1),
+    (450, 500, 2, 4, 0),
+]
+
+
+def test_spans_busy_and_critical_path(tmp_path):
+    g = FakeGraph()
+    spans = trace_analysis.task_spans(g, RECORDS)
+    assert spans[1] == {"op": "TRSM_RLT", "start": 110, "end": 300, "items": 2, "item_ns": 280}
+    path = trace_analysis.critical_path(g, spans)
+    assert [p["task"] for p in path] == [0, 1, 3, 4]  # through the later-ending TRSM
+    assert [p["wait"] for p in path] == [0, 10, 20, 30]
+    busy = trace_analysis.busy_fraction(RECORDS)
+    assert abs(busy - (100 + 90 + 190 + 145 + 80 + 90 + 50) / (3 * 500)) < 1e-12
+    s = trace_analysis.dump_json(str(tmp_path / "t.json"), g, RECORDS)
+    assert s["critical_path"]["tasks"] == 4
+    assert abs(s["critical_path"]["per_op"]["POTRF"]["in_task_ms"] - 150e-6) < 1e-15
+    out = json.load(open(tmp_path / "t.json"))
+    assert len(out["records"]) == len(RECORDS) and set(out["tasks"]) == {"0", "1", "2", "3", "4"}
