@@ -71,8 +71,12 @@ typedef enum mtd_precision {
     MTD_PREC_TF32 = 1,           /* FP32 matrix, TF32 tensor-core products with FP32           */
                                  /* accumulation, FP32 diagonal blocks (Cholesky only); the    */
                                  /* low-precision factor of the mixed-precision solver         */
-    MTD_PREC_FP32 = 2            /* FP32 matrix, FP32-accurate products from three TF32 MMAs   */
+    MTD_PREC_FP32 = 2,           /* FP32 matrix, FP32-accurate products from three TF32 MMAs   */
                                  /* per product (split operands: hi*hi + hi*lo + lo*hi)        */
+    MTD_PREC_BF16 = 3            /* FP32 matrix; the GEMM / SYRK updates take BF16 operands    */
+                                 /* (FP32 accumulation) from a BF16 copy of the panels that    */
+                                 /* the TRSMs write (the graph allocates it: 2 N^2 bytes);     */
+                                 /* diagonal and panel work as MTD_PREC_TF32 (Cholesky only)   */
 } mtd_precision;
 
 typedef enum mtd_generator {
@@ -250,8 +254,8 @@ typedef struct mtd_solve_stats {
 
 typedef struct mtd_solver mtd_solver;
 
-/* n x n systems; tile must be a multiple of 64; prec MTD_PREC_TF32, MTD_PREC_FP32 (low-
- * precision factors) or MTD_PREC_FP64 (the plain FP64 baseline). */
+/* n x n systems; tile must be a multiple of 64; prec MTD_PREC_TF32, MTD_PREC_FP32,
+ * MTD_PREC_BF16 (low-precision factors) or MTD_PREC_FP64 (the plain FP64 baseline). */
 int mtd_solver_create(mtd_solver **out, int64_t n, int64_t tile, int prec);
 /* Factor A + shift*I (shift >= 0; a diagonal shift keeps a low-precision factorisation of
  * an ill-conditioned matrix positive definite; refinement still solves with A itself). */

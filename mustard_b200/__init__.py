@@ -21,7 +21,7 @@ from . import _capi
 from ._capi import (  # noqa: F401  (re-exported constants)
     GEN_SPD, GEN_UNIFORM_DIAG, KIND_CHOLESKY, KIND_CUSTOM, KIND_LU, OP_GEMM_NN, OP_GEMM_NT,
     OP_GETRF, OP_NAMES, OP_POTRF, OP_SYRK_LN, OP_TRSM_LLNU, OP_TRSM_RLT, OP_TRSM_RUN,
-    PREC_FP32, PREC_FP64, PREC_TF32, REFINE_GMRES_IR, REFINE_IR, REFINE_NONE, STATUS_NAMES, MtdError,
+    PREC_BF16, PREC_FP32, PREC_FP64, PREC_TF32, REFINE_GMRES_IR, REFINE_IR, REFINE_NONE, STATUS_NAMES, MtdError,
     lib, lib_path)
 
 __all__ = [

@@ -32,7 +32,7 @@ class RunStats(ctypes.Structure):
                 ("busy_fraction", ctypes.c_double), ("span_ms", ctypes.c_double)]
 
 
-PREC_FP64, PREC_TF32, PREC_FP32 = 0, 1, 2
+PREC_FP64, PREC_TF32, PREC_FP32, PREC_BF16 = 0, 1, 2, 3
 REFINE_NONE, REFINE_IR, REFINE_GMRES_IR = 0, 1, 2
 
 

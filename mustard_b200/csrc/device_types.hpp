@@ -119,6 +119,14 @@ struct RunArgs {
     // descriptor address.
     int tma;
     alignas(64) unsigned char tmap[128];
+    // BF16-update runs (MTD_PREC_BF16): the BF16 copy of the panels (column-major, leading
+    // dimension bf16_ld, a multiple of 64) that TRSM items write and GEMM / SYRK items read,
+    // and its TMA tensor map (3D: 64 rows of an atom, columns, atoms; box 64 x 128 x 2,
+    // 128-byte swizzle) when tma_bf16 != 0.
+    void *bf16;
+    int64_t bf16_ld;
+    int tma_bf16;
+    alignas(64) unsigned char tmap_bf16[128];
 };
 
 }  // namespace mtd

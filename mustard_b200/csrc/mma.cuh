@@ -27,6 +27,8 @@
 // VEC == 1: element loads through registers, any shape.
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include <cstdint>
 
 #include "device_types.hpp"
@@ -414,6 +416,11 @@ struct BlockMmaT {
     // C(r, c) = acc(r, c).
     __device__ __forceinline__ void store_to(T *C, int64_t ldc, int M, int N) const {
         for_each(M, N, [&](int r, int c, T v) { C[r + int64_t(c) * ldc] = v; });
+    }
+
+    // C(r, c) = acc(r, c) rounded to nearest BF16 (the copy BF16 updates read).
+    __device__ __forceinline__ void store_bf16_to(__nv_bfloat16 *C, int64_t ldc, int M, int N) const {
+        for_each(M, N, [&](int r, int c, T v) { C[r + int64_t(c) * ldc] = __float2bfloat16_rn(float(v)); });
     }
 
     // C(r, c) = acc(r, c) as the tensor cores of this mode read it: rounded to nearest TF32

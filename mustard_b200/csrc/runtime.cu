@@ -36,6 +36,8 @@ struct mtd_graph {
     double timeout_s = 10.0;
     int nest = kNestTile;
     int prec = MTD_PREC_FP64;  // element type of the matrix runs factor
+    unsigned short *d_bf16 = nullptr;  // MTD_PREC_BF16: BF16 copy of the panels (bf16_ld x n)
+    int64_t bf16_ld = 0;
     Lowered low;   // device form, kept for the CUDA-graph executor and item queries
     int n_dev = 0;
 
@@ -132,6 +134,8 @@ RunArgs make_args(const mtd_graph *g, void *dA, int64_t lda) {
     a.trace = g->d_trace;
     a.trace_cap = g->trace_cap;
     a.timeout_ns = static_cast<unsigned long long>(g->timeout_s * 1e9);
+    a.bf16 = g->d_bf16;
+    a.bf16_ld = g->bf16_ld;
     return a;
 }
 
@@ -227,6 +231,8 @@ void release_device(mtd_graph *g) {
     cudaFree(g->d_ctl);
     if (g->h_ctl) cudaFreeHost(g->h_ctl);
     cudaFree(g->d_ws_lower);
+    cudaFree(g->d_bf16);
+    g->d_bf16 = nullptr;
     cudaFree(g->d_ws_upper);
     cudaFree(g->d_trace);
 }
@@ -380,6 +386,10 @@ int mtd_graph_finalize(mtd_graph *g) {
     rc = rc ? rc : dev_alloc(&g->d_ctl, 1);
     rc = rc ? rc : dev_alloc(&g->d_ws_lower, ws);
     if (needs_upper) rc = rc ? rc : dev_alloc(&g->d_ws_upper, ws);
+    if (g->prec == MTD_PREC_BF16) {
+        g->bf16_ld = (g->dag.n() + 63) & ~int64_t(63);
+        rc = rc ? rc : dev_alloc(&g->d_bf16, size_t(g->bf16_ld) * size_t(g->dag.n()));
+    }
     if (g->trace) rc = rc ? rc : dev_alloc(&g->d_trace, size_t(4 * g->trace_cap));
     if (!rc && cudaMallocHost(reinterpret_cast<void **>(&g->h_ctl), sizeof(RunCtl)) != cudaSuccess) {
         g->h_ctl = nullptr;
@@ -393,6 +403,10 @@ int mtd_graph_finalize(mtd_graph *g) {
         ok = ok && cudaMemcpy(g->d_roots, roots.data(), roots.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
         ok = ok && cudaMemset(g->d_ws_lower, 0, ws) == cudaSuccess;
         if (needs_upper) ok = ok && cudaMemset(g->d_ws_upper, 0, ws) == cudaSuccess;
+        // rows past n of the copy's last atom are read by TMA and multiplied into rows the
+        // epilogue never stores; keep them finite
+        if (g->d_bf16)
+            ok = ok && cudaMemset(g->d_bf16, 0, size_t(g->bf16_ld) * size_t(g->dag.n()) * 2) == cudaSuccess;
         ok = ok && cudaMemset(g->d_ctl, 0, sizeof(RunCtl)) == cudaSuccess;
         if (!ok) rc = MTD_ERR_CUDA;
     }
@@ -419,8 +433,8 @@ namespace mtd {
 // atom, columns, atoms 128 bytes apart; box 32 x 64 x 4), so one load fetches a whole
 // 128-row operand slice; otherwise 2D (rows, columns; box 32 x 64).  The driver entry point
 // is looked up once; without it (or on an encoding error) the run keeps its cp.async path.
-void encode_tmap(RunArgs &a, void *dA, int64_t n, int64_t ld) {
-    static_assert(sizeof(CUtensorMap) == sizeof(a.tmap), "tensor map storage");
+// The driver's tensor-map encoder, looked up once (nullptr if the driver has none).
+PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     static std::once_flag once;
     std::call_once(once, [] {
@@ -430,6 +444,12 @@ void encode_tmap(RunArgs &a, void *dA, int64_t n, int64_t ld) {
             q == cudaDriverEntryPointSuccess)
             encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
     });
+    return encode;
+}
+
+void encode_tmap(RunArgs &a, void *dA, int64_t n, int64_t ld) {
+    static_assert(sizeof(CUtensorMap) == sizeof(a.tmap), "tensor map storage");
+    const PFN_cuTensorMapEncodeTiled_v12000 encode = tmap_encoder();
     a.tma = tc::kTmaNone;
     if (!encode) return;
     CUtensorMap map;
@@ -452,6 +472,29 @@ void encode_tmap(RunArgs &a, void *dA, int64_t n, int64_t ld) {
     if (r != CUDA_SUCCESS) return;
     std::memcpy(a.tmap, &map, sizeof(map));
     a.tma = n % 32 == 0 ? tc::kTmaMap3D : tc::kTmaMap2D;
+}
+
+// TMA tensor map of the BF16 copy of the panels (column-major, leading dimension ld, a
+// multiple of 64) for the BF16 GEMM / SYRK items: 3D (64 rows of an atom, columns, atoms
+// 128 bytes apart), box 64 x 128 x 2 (a 128-row x 128-column operand slice per load),
+// 128-byte swizzle -- the MN-major layout tcgen05 kind::f16 reads with 64-element atoms.
+// Rows past n (the last atom's padding) hold zeros.  Without the encoder, or on an encoding
+// error, the run keeps the TF32 path for every update.
+void encode_tmap_bf16(RunArgs &a, void *d16, int64_t n, int64_t ld) {
+    static_assert(sizeof(CUtensorMap) == sizeof(a.tmap_bf16), "tensor map storage");
+    const PFN_cuTensorMapEncodeTiled_v12000 encode = tmap_encoder();
+    a.tma_bf16 = 0;
+    if (!encode || !d16 || ld % 64 != 0) return;
+    const cuuint64_t dims[3] = {64, cuuint64_t(n), cuuint64_t(ld / 64)};
+    const cuuint64_t strides[2] = {cuuint64_t(ld) * 2, 128};
+    const cuuint32_t box[3] = {64, tc::kBfBK, 2}, elem[3] = {1, 1, 1};
+    CUtensorMap map;
+    if (encode(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, d16, dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return;
+    std::memcpy(a.tmap_bf16, &map, sizeof(map));
+    a.tma_bf16 = 1;
 }
 
 // Reset, seed and launch one persistent run (shared by graphs, batches and the
@@ -501,8 +544,12 @@ static int run_persistent(mtd_graph *g, void *dA, int64_t lda, void *stream, int
     // TF32 runs feed their tcgen05 GEMM items with TMA when every item's rows start on a
     // 32-row atom (tile and nested sub-tile edges multiples of 32); updates whose depth is
     // not a whole number of 64-column stages use the cp.async path
-    if (g->prec == MTD_PREC_TF32 && vec2 && g->dag.tile() % 32 == 0 && g->nest % 32 == 0)
-        mtd::encode_tmap(a, dA, g->dag.n(), lda);
+    const bool tf32_items = g->prec == MTD_PREC_TF32 || g->prec == MTD_PREC_BF16;
+    if (tf32_items && vec2 && g->dag.tile() % 32 == 0 && g->nest % 32 == 0) mtd::encode_tmap(a, dA, g->dag.n(), lda);
+    // BF16 updates read the BF16 copy by TMA when every item's rows start on a 64-row atom;
+    // the others keep the TF32 path on the FP32 matrix
+    if (g->prec == MTD_PREC_BF16 && vec2 && g->dag.tile() % 64 == 0 && g->nest % 64 == 0)
+        mtd::encode_tmap_bf16(a, g->d_bf16, g->dag.n(), g->bf16_ld);
     const int grid = g->num_sms;
     g->last_grid = grid;
     const int rc = launch_run(a, g->d_deps_init, g->d_roots, g->n_roots, g->total_items, g->prec, vec2, grid, s,
@@ -530,7 +577,8 @@ int mtd_run_f32(mtd_graph *g, float *dA, int64_t lda, void *stream, int *info_ou
 }
 
 int mtd_graph_set_precision(mtd_graph *g, int prec) {
-    if (!g || (prec != MTD_PREC_FP64 && prec != MTD_PREC_TF32 && prec != MTD_PREC_FP32)) return MTD_ERR_INVALID_ARG;
+    if (!g || (prec != MTD_PREC_FP64 && prec != MTD_PREC_TF32 && prec != MTD_PREC_FP32 && prec != MTD_PREC_BF16))
+        return MTD_ERR_INVALID_ARG;
     if (g->finalized) return MTD_ERR_STATE;
     g->prec = prec;
     return MTD_OK;

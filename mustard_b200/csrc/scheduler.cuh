@@ -9,7 +9,8 @@
 //   - a task is split into independent work items (output sub-tiles / row strips) so all
 //     148 SMs can share one tile operation;
 //   - the dependency decrement is fused into the epilogue of a task's last work item;
-//   - two ready queues (critical path first) replace the single FIFO ring;
+//   - three ready queues (critical path first, then by distance to the panel) replace the
+//     single FIFO ring;
 //   - a queue is a bounded array of 64-bit slots (task << 32 | item); a producer reserves
 //     slots with a fetch-and-add on `tail`, writes them, then adds their number to `avail`;
 //     a consumer first takes one unit of `avail` (fetch-and-add, undone if it was not
@@ -90,7 +91,7 @@ __device__ __forceinline__ void release_task(const RunArgs &p, int task) {
 }
 
 // Thread 0 of a CTA: claim one work item, waiting (bounded) while none is ready.  The
-// exit flags and both queues' counts are read together (one round trip); a claim is then
+// exit flags and every queue's count are read together (one round trip); a claim is then
 // two fetch-and-adds and the slot read.
 __device__ __forceinline__ int pop_item(const RunArgs &p, int *task, int *item) {
     const unsigned long long t0 = global_ns();
@@ -195,7 +196,12 @@ __device__ __forceinline__ int op_update_tc(const RunArgs &p, const MatCtx &m, c
     float *C = at<float>(m, t.cr + r0, t.cc + c0);
     // SYRK's B panel starts in the same column as A; GEMM_NT's may not
     const int bcol = t.op == MTD_OP_SYRK_LN ? t.ac : t.bc;
-    const bool ok = (tmap && t.k % tc::kTmaBK == 0 && t.ac == bcol)
+    // BF16 updates (operands from the BF16 copy of the panels, same coordinates) when the
+    // depth is whole 128-column stages and both operand slices start on 64-row atoms
+    const bool bf16 = p.tma_bf16 && t.k % tc::kBfBK == 0 && t.ac == bcol && (t.ar + r0) % 64 == 0 && brow % 64 == 0;
+    const bool ok = bf16 ? tc::gemm_nt_tma_bf16<kThreads>(tcs, s, p.tmap_bf16, t.ar + r0, brow, t.ac, t.k, mm, nn, C,
+                                                          m.lda, lower, 0, 0, p.timeout_ns)
+                    : (tmap && t.k % tc::kTmaBK == 0 && t.ac == bcol)
                         ? tc::gemm_nt_tma<kThreads>(tcs, s, tmap, p.tma, t.ar + r0, brow, t.ac, t.k, mm, nn, C, m.lda,
                                                     lower, 0, 0, p.timeout_ns)
                         : tc::gemm_nt<kThreads>(tcs, s, at<float>(m, t.ar + r0, t.ac), m.lda, B, m.lda, mm, nn, t.k, C,

@@ -939,7 +939,8 @@ int mtd_solver_create(mtd_solver **out, int64_t n, int64_t tile, int prec) {
     if (!out) return MTD_ERR_INVALID_ARG;
     *out = nullptr;
     if (n <= 0 || tile <= 0 || tile > n || tile % kSB != 0 || n > (int64_t(1) << 30)) return MTD_ERR_INVALID_ARG;
-    if (prec != MTD_PREC_FP64 && prec != MTD_PREC_TF32 && prec != MTD_PREC_FP32) return MTD_ERR_INVALID_ARG;
+    if (prec != MTD_PREC_FP64 && prec != MTD_PREC_TF32 && prec != MTD_PREC_FP32 && prec != MTD_PREC_BF16)
+        return MTD_ERR_INVALID_ARG;
     mtd_solver *s = new (std::nothrow) mtd_solver();
     if (!s) return MTD_ERR_OUT_OF_MEMORY;
     s->n = n;

@@ -323,6 +323,9 @@ __device__ bool gemm_nt_tma(State *st, uint8_t *smem, const void *map, int map_k
         const unsigned long long deadline = now_ns() + timeout_ns;
         const int nk = K / kTmaBK;
         uint32_t ph = st->phases, fph = st->fphases;
+        // the operands were written by other CTAs with generic stores (released and acquired
+        // through the scheduler's counters): order them before this thread's async-proxy loads
+        asm volatile("fence.proxy.async.global;" ::: "memory");
         auto issue = [&](int s, int kt) {
             const uint32_t bar = smem_addr(&st->full[s]), base = smem_addr(smem + s * kTmaStageBytes);
             const int k = k0 + kt * kTmaBK;
@@ -387,6 +390,87 @@ __device__ bool gemm_nt_tma(State *st, uint8_t *smem, const void *map, int map_k
     if (threadIdx.x == 0) s_ok = ok ? 1 : 0;
     __syncthreads();
     return epilogue(st, s_ok != 0, cv, M, N, C, ldc, lower_only, r0, c0);
+}
+
+// BF16 updates: C -= A B^T with BF16 operands read by TMA from the BF16 copy of the panels
+// (`map`: 3D, 64-row atoms, box 64 x kBfBK x 2, 128-byte swizzle), tcgen05.mma kind::f16
+// (BF16 x BF16, FP32 accumulation in TMEM, M = N = 128, K = 16 per instruction).  A stage is
+// 128 MN rows x kBfBK columns per operand: two atoms of kBfBK rows x 128 bytes, 16 KB apart
+// (LBO), 8-row groups 1 KB apart (SBO), layout type 2 (128-byte swizzle); this layout was
+// checked bit-exact against a host product of the same BF16 values.  a_row, b_row multiples
+// of 64, K a multiple of kBfBK; otherwise as gemm_nt_tma.
+constexpr int kBfBK = 128;
+constexpr int kBfStages = 3;
+constexpr int kBfAtomBytes = kBfBK * 128;                   // 64 BF16 x kBfBK rows: 16 KB
+constexpr int kBfOperandBytes = 2 * kBfAtomBytes;           // 32 KB
+constexpr int kBfStageBytes = 2 * kBfOperandBytes;          // 64 KB
+static_assert(kBfStages * kBfStageBytes <= kSmemBytes, "BF16 stages fit the engine's shared memory");
+static_assert(kBfStages <= kStages, "BF16 stages use the engine's barriers");
+constexpr uint32_t kIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
+                                (uint32_t(kN >> 3) << 17) | (uint32_t(kM >> 4) << 24);
+
+template <int THREADS>
+__device__ bool gemm_nt_tma_bf16(State *st, uint8_t *smem, const void *map, int a_row, int b_row, int k0, int K, int M,
+                                 int N, float *C, int64_t ldc, bool lower_only, int r0, int c0,
+                                 unsigned long long timeout_ns) {
+    bool ok = true;
+    if (threadIdx.x == 0) {
+        const unsigned long long deadline = now_ns() + timeout_ns;
+        const int nk = K / kBfBK;
+        uint32_t ph = st->phases, fph = st->fphases;
+        asm volatile("fence.proxy.async.global;" ::: "memory");  // see gemm_nt_tma
+        auto issue = [&](int s, int kt) {
+            const uint32_t bar = smem_addr(&st->full[s]), base = smem_addr(smem + s * kBfStageBytes);
+            const int k = k0 + kt * kBfBK;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kBfStageBytes)
+                         : "memory");
+            tma_load_3d(base, map, 0, k, a_row >> 6, bar);
+            tma_load_3d(base + kBfOperandBytes, map, 0, k, b_row >> 6, bar);
+        };
+        for (int s = 0; s < kBfStages && s < nk; ++s) issue(s, s);
+        for (int kt = 0; kt < nk && ok; ++kt) {
+            const int s = kt % kBfStages;
+            ok = wait_bar(&st->full[s], (fph >> s) & 1u, deadline);
+            fph ^= 1u << s;
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = smem_addr(smem + s * kBfStageBytes), b0 = a0 + kBfOperandBytes;
+#pragma unroll
+            for (int g = 0; g < kBfBK / 16; ++g) {
+                const uint64_t lead = uint64_t(kBfAtomBytes >> 4) << 16, stride = uint64_t(1024 >> 4) << 32;
+                const uint64_t ad = uint64_t(((a0 + g * 2048) >> 4) & 0x3fff) | lead | stride | (1ull << 46) | (2ull << 61);
+                const uint64_t bd = uint64_t(((b0 + g * 2048) >> 4) & 0x3fff) | lead | stride | (1ull << 46) | (2ull << 61);
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(st->taddr),
+                    "l"(ad), "l"(bd), "r"(kIdescBf16), "r"((kt > 0 || g > 0) ? 1u : 0u)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_addr(&st->mbar[s]))
+                         : "memory");
+            if (kt > 0 && kt - 1 + kBfStages < nk) {
+                const int sp = (kt - 1) % kBfStages;
+                ok = wait_bar(&st->mbar[sp], (ph >> sp) & 1u, deadline);
+                ph ^= 1u << sp;
+                if (ok) issue(sp, kt - 1 + kBfStages);
+            }
+        }
+        for (int kt = nk > kBfStages ? nk - kBfStages : 0; kt < nk && ok; ++kt) {
+            const int s = kt % kBfStages;
+            ok = wait_bar(&st->mbar[s], (ph >> s) & 1u, deadline);
+            ph ^= 1u << s;
+        }
+        st->phases = ph;
+        st->fphases = fph;
+    }
+    float cv[32];
+    load_c(cv, M, N, C, ldc, lower_only, r0, c0);
+    __shared__ int s_ok_bf;
+    if (threadIdx.x == 0) s_ok_bf = ok ? 1 : 0;
+    __syncthreads();
+    return epilogue(st, s_ok_bf != 0, cv, M, N, C, ldc, lower_only, r0, c0);
 }
 
 }  // namespace tc

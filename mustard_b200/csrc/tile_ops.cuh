@@ -571,6 +571,10 @@ __device__ int op_trsm_rlt(const RunArgs &p, const MatCtx &m, const DevTask &t, 
         e.zero();
         e.run(smem, X + int64_t(jb) * lda, lda, W + jb, ldw, mm, jn, jn);
         e.store_rounded_to(X + int64_t(jb) * lda, lda, mm, jn);  // panel of L: an operand of the updates
+        if constexpr (sizeof(T) == 4)
+            if (p.bf16)  // BF16-update runs: the updates read the panel from its BF16 copy
+                e.store_bf16_to(static_cast<__nv_bfloat16 *>(p.bf16) + (t.cr + r0) + int64_t(t.cc + jb) * p.bf16_ld,
+                                p.bf16_ld, mm, jn);
         block_fence_sync();
     }
     return 0;

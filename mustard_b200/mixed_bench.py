@@ -6,7 +6,8 @@
 For each condition number kappa: A = B B^T / n + alpha I (B = U[-1,1), alpha = (4/3)/(kappa-1),
 built on the device by the seeded generator), right-hand sides i.i.d. N(0,1).  The plain FP64
 time-to-solution (FP64 tiled Cholesky + one FP64 solve) is compared with each
-low-precision variant: TF32 or FP32-accurate (split TF32) factor of A + shift*I followed by
+low-precision variant: TF32, BF16-update (tcgen05 kind::f16 updates, TF32 panels) or
+FP32-accurate (split TF32) factor of A + shift*I followed by
 IR or GMRES-IR to a normwise backward error of 1e-13.  One JSON line per run: iterations,
 backward error (FP64, on the device), forward error against the FP64 solution, times, and
 the FP64-equivalent rate (n^3/3 + 2 n^2 nrhs) / time-to-solution.
@@ -19,9 +20,9 @@ import torch
 
 import mustard_b200 as mtd
 
-PREC_NAMES = {mtd.PREC_FP64: "fp64", mtd.PREC_TF32: "tf32", mtd.PREC_FP32: "fp32(3xtf32)"}
+PREC_NAMES = {mtd.PREC_FP64: "fp64", mtd.PREC_TF32: "tf32", mtd.PREC_FP32: "fp32(3xtf32)", mtd.PREC_BF16: "bf16"}
 METHOD_NAMES = {mtd.REFINE_NONE: "none", mtd.REFINE_IR: "ir", mtd.REFINE_GMRES_IR: "gmres-ir"}
-UNIT_ROUNDOFF = {mtd.PREC_TF32: 2.0 ** -11, mtd.PREC_FP32: 2.0 ** -24}
+UNIT_ROUNDOFF = {mtd.PREC_TF32: 2.0 ** -11, mtd.PREC_FP32: 2.0 ** -24, mtd.PREC_BF16: 2.0 ** -8}
 
 
 def colmajor(n, k):
@@ -88,6 +89,8 @@ def run_case(n, tile, kappa, nrhs, seed, variants, tol, max_iter, reps):
 DEFAULT_VARIANTS = [
     (mtd.PREC_TF32, mtd.REFINE_IR, 0.0),
     (mtd.PREC_TF32, mtd.REFINE_GMRES_IR, 0.0),
+    (mtd.PREC_BF16, mtd.REFINE_IR, 0.0),
+    (mtd.PREC_BF16, mtd.REFINE_GMRES_IR, 0.0),
     (mtd.PREC_FP32, mtd.REFINE_IR, 0.0),
     (mtd.PREC_FP32, mtd.REFINE_GMRES_IR, 2.0),
 ]

@@ -58,13 +58,13 @@ def main():
     ap.add_argument("--n", type=int, default=6144)
     ap.add_argument("--tile", type=int, default=768)
     ap.add_argument("--runs", type=int, default=2)
-    ap.add_argument("--prec", choices=["fp64", "tf32"], default="fp64")
+    ap.add_argument("--prec", choices=["fp64", "tf32", "bf16"], default="fp64")
     ap.add_argument("--trace", action="store_true", help="per-operation item-time breakdown")
     ap.add_argument("--trace-out", default=None,
                     help="also write the records, task spans and critical path to this JSON file")
     args = ap.parse_args()
-    if args.prec == "tf32" and args.case == "lu":
-        ap.error("the TF32 path factors SPD matrices only (chol, gemm)")
+    if args.prec != "fp64" and args.case == "lu":
+        ap.error("the low-precision paths factor SPD matrices only (chol, gemm)")
     n, b = args.n, args.tile
     t = (n + b - 1) // b
     a = torch.empty((n, n), dtype=torch.float64, device="cuda").t()
@@ -85,8 +85,8 @@ def main():
             for j in range(i + 1, t):
                 g.add_task(mtd.OP_GEMM_NT, (j, i), [(j, i), (j, 0), (i, 0)])
                 flops += 2.0 * ext[j] * ext[i] * ext[0]
-    if args.prec == "tf32":
-        g.set_precision(mtd.PREC_TF32)
+    if args.prec != "fp64":
+        g.set_precision(mtd.PREC_TF32 if args.prec == "tf32" else mtd.PREC_BF16)
         a = a.t().contiguous().float().t()
     if args.trace_out:
         args.trace = True
@@ -100,7 +100,7 @@ def main():
         a.copy_(src)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(s)
-        if args.prec == "tf32":
+        if args.prec != "fp64":
             g.run_f32(a, stream=s, sync=False)
         else:
             g.run(a, stream=s, sync=False)

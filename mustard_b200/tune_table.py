@@ -18,7 +18,7 @@ import os
 import tempfile
 
 VERSION = 1
-PREC_KEYS = {0: "fp64", 1: "tf32", 2: "fp32"}  # mtd_precision values
+PREC_KEYS = {0: "fp64", 1: "tf32", 2: "fp32", 3: "bf16"}  # mtd_precision values
 
 
 def empty():

@@ -149,3 +149,47 @@ def test_solver_argument_checks(mtd):
         s.solve(xd, xd)  # not factored yet
     assert e.value.status == 2
     s.close()
+
+
+def _low_factor(mtd, a, tile, prec):
+    import torch
+    n = a.shape[0]
+    g = mtd.TaskGraph(mtd.KIND_CHOLESKY, n, tile).build_tiled().set_precision(prec).finalize()
+    d = torch.from_numpy(np.ascontiguousarray(a.T).astype(np.float32)).cuda().t()
+    assert g.run_f32(d) == 0
+    g.close()
+    return np.tril(np.asfortranarray(d.t().contiguous().cpu().numpy().T).astype(np.float64))
+
+
+@pytest.mark.parametrize("n,tile,ratio", [(2048, 512, 2.0), (1024, 320, 1.0)])
+def test_bf16_update_factor_accuracy(mtd, n, tile, ratio):
+    # GEMM / SYRK updates with BF16 operands (tcgen05 kind::f16 from the BF16 copy of the
+    # panels): at tile 512 every update is a BF16 one and the factor is accurate to about
+    # BF16 roundoff, clearly coarser than the TF32 factor (7 against 10 mantissa bits); at
+    # tile 320 the 320-deep outer updates (most of the work) take the TF32 path and only the
+    # nested 128-deep ones the BF16 path.  Either way far from a wrong factor.
+    a = mixed.spd_kappa(n, 1e2, 31)
+    err = {}
+    for prec in (mtd.PREC_TF32, mtd.PREC_BF16):
+        l = _low_factor(mtd, a, tile, prec)
+        err[prec] = np.linalg.norm(l @ l.T - a) / np.linalg.norm(a)
+    assert err[mtd.PREC_TF32] < 2e-3
+    assert ratio * err[mtd.PREC_TF32] < err[mtd.PREC_BF16] < 2e-2, err
+
+
+@pytest.mark.parametrize("method", ["ir", "gmres-ir"])
+def test_bf16_factor_refines_to_fp64_accuracy(mtd, method):
+    n, tile = 2048, 512
+    a = mixed.spd_kappa(n, 1e2, 32)
+    k = 2 if method == "ir" else 1  # GMRES-IR solves one right-hand side at a time
+    b = mixed.rhs(n, k, 33)
+    m = mtd.REFINE_IR if method == "ir" else mtd.REFINE_GMRES_IR
+    s = mtd.SpdSolver(n, tile, mtd.PREC_BF16)
+    assert s.factor(to_dev(a)) == 0
+    xd = _dev_rect(np.zeros((n, k)))
+    st = s.solve(_dev_rect(b), xd, method=m, tol=1e-13, max_iter=60)
+    x = _host_rect(xd)
+    assert st["converged"] and st["backward_error"] <= 1e-13, st
+    assert mixed.backward_error(a, x, b) <= 2e-13
+    assert mixed.forward_error(x, mixed.solve_fp64(a, b)) <= 1e2 * 1e-12
+    s.close()
