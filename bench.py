@@ -355,9 +355,16 @@ def main():
 
     peak_meas = mtd.probe_fp64_peak()
     achieved = flops_step / (dev_ms * 1e-3) / 1e12
+    # DRAM bytes (read + write) of the two launches of one step, from one ncu capture of
+    # dram__bytes_read.sum / dram__bytes_write.sum (a single-pass metric pair) on exactly this
+    # workload: profiles/dram_traffic_bench_n24000_t1536.md.  Other workloads report null.
+    measured = n == 24000 and args.tile_lu == 1536 and args.tile_chol == 1536 and args.only is None
+    traffic = (76424422400 + 35419470336 + 39205473280 + 17637506560) if measured else None
     roofline = {
         "bound": "tensor", "achieved": achieved, "peak": peak_meas, "unit": "TFLOP/s",
-        "frac": achieved / peak_meas if peak_meas else None, "traffic": None,
+        "frac": achieved / peak_meas if peak_meas else None, "traffic": traffic,
+        "traffic_unit": "bytes per step (LU launch + Cholesky launch)",
+        "traffic_bytes_per_flop": traffic / flops_step if traffic else None,
         "kernel": "mtd::persistent_kernel<2> (scheduler + all FP64 tile operations)",
         "peak_source": "measured: register-only mma.sync.m16n8k8.f64 probe on this GPU",
         "frac_of_datasheet_37": achieved / DATASHEET_FP64_TFLOPS,
