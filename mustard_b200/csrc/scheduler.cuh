@@ -31,7 +31,7 @@
 namespace mtd {
 
 constexpr unsigned long long kEmptySlot = ~0ull;
-enum { kCmdWork = 0, kCmdExit = 1 };
+enum { kCmdWork = 0, kCmdExit = 1, kCmdNone = 2 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -50,7 +50,7 @@ __device__ __forceinline__ long long add_avail(long long *c, long long v) {
         atomicAdd(reinterpret_cast<unsigned long long *>(c), static_cast<unsigned long long>(v)));
 }
 
-// Thread 0 of a CTA: `task` has no predecessors left.  Push every work item of it; a
+// One thread of a CTA: `task` has no predecessors left.  Push every work item of it; a
 // join (no work items) completes on the spot, releasing its own successors.
 __device__ __forceinline__ void release_task(const RunArgs &p, int task) {
     int stack[8];
@@ -90,43 +90,49 @@ __device__ __forceinline__ void release_task(const RunArgs &p, int task) {
     }
 }
 
-// Thread 0 of a CTA: claim one work item, waiting (bounded) while none is ready.  The
-// exit flags and every queue's count are read together (one round trip); a claim is then
-// two fetch-and-adds and the slot read.
+// One thread of a CTA: one attempt to claim a work item.  The exit flags and every queue's
+// count are read together (one round trip); a claim is then two fetch-and-adds and the slot
+// read.  kCmdNone: nothing is ready right now.
+__device__ __forceinline__ int claim_item(const RunArgs &p, int *task, int *item, unsigned long long t0) {
+    const int abort = ld_volatile(&p.ctl->abort);
+    const int done = ld_volatile(&p.ctl->tasks_done);
+    long long avail[kNumQueues];
+#pragma unroll
+    for (int q = 0; q < kNumQueues; ++q)
+        avail[q] = static_cast<long long>(ld_volatile(reinterpret_cast<const unsigned long long *>(&p.qctl[q].avail)));
+    if (abort || done >= p.n_tasks) return kCmdExit;
+    for (int q = 0; q < kNumQueues; ++q) {
+        if (avail[q] <= 0) continue;
+        if (add_avail(&p.qctl[q].avail, -1) <= 0) {  // taken meanwhile: give the unit back
+            add_avail(&p.qctl[q].avail, 1);
+            continue;
+        }
+        // one unit of avail = one pushed, unclaimed item, so this slot is reserved
+        const unsigned long long h = atomicAdd(&p.qctl[q].head, 1ull);
+        const unsigned long long *slot = p.queue[q] + h;
+        unsigned long long v;
+        while ((v = ld_volatile(slot)) == kEmptySlot) {
+            if (global_ns() - t0 > p.timeout_ns) {
+                report_error(p.ctl, MTD_ERR_TIMEOUT, 0);
+                return kCmdExit;
+            }
+            __nanosleep(20);
+        }
+        __threadfence();
+        *task = static_cast<int>(v >> 32);
+        *item = static_cast<int>(v & 0xffffffffull);
+        return kCmdWork;
+    }
+    return kCmdNone;
+}
+
+// One thread of a CTA: claim one work item, waiting (bounded) while none is ready.
 __device__ __forceinline__ int pop_item(const RunArgs &p, int *task, int *item) {
     const unsigned long long t0 = global_ns();
     unsigned int backoff = 32;
     while (true) {
-        const int abort = ld_volatile(&p.ctl->abort);
-        const int done = ld_volatile(&p.ctl->tasks_done);
-        long long avail[kNumQueues];
-#pragma unroll
-        for (int q = 0; q < kNumQueues; ++q)
-            avail[q] = static_cast<long long>(
-                ld_volatile(reinterpret_cast<const unsigned long long *>(&p.qctl[q].avail)));
-        if (abort || done >= p.n_tasks) return kCmdExit;
-        for (int q = 0; q < kNumQueues; ++q) {
-            if (avail[q] <= 0) continue;
-            if (add_avail(&p.qctl[q].avail, -1) <= 0) {  // taken meanwhile: give the unit back
-                add_avail(&p.qctl[q].avail, 1);
-                continue;
-            }
-            // one unit of avail = one pushed, unclaimed item, so this slot is reserved
-            const unsigned long long h = atomicAdd(&p.qctl[q].head, 1ull);
-            const unsigned long long *slot = p.queue[q] + h;
-            unsigned long long v;
-            while ((v = ld_volatile(slot)) == kEmptySlot) {
-                if (global_ns() - t0 > p.timeout_ns) {
-                    report_error(p.ctl, MTD_ERR_TIMEOUT, 0);
-                    return kCmdExit;
-                }
-                __nanosleep(20);
-            }
-            __threadfence();
-            *task = static_cast<int>(v >> 32);
-            *item = static_cast<int>(v & 0xffffffffull);
-            return kCmdWork;
-        }
+        const int cmd = claim_item(p, task, item, t0);
+        if (cmd != kCmdNone) return cmd;
         if (global_ns() - t0 > p.timeout_ns) {
             report_error(p.ctl, MTD_ERR_TIMEOUT, 0);
             return kCmdExit;
@@ -136,7 +142,7 @@ __device__ __forceinline__ int pop_item(const RunArgs &p, int *task, int *item) 
     }
 }
 
-// Thread 0 of a CTA, after the whole CTA finished an item of `task`.
+// One thread of a CTA, after the threads that wrote an item of `task` passed a barrier with it.
 __device__ __forceinline__ void complete_item(const RunArgs &p, int task) {
     __threadfence();
     if (atomicSub(&p.items_left[task], 1) != 1) return;
@@ -152,6 +158,27 @@ __device__ __forceinline__ void complete_item(const RunArgs &p, int task) {
     atomicAdd(&p.ctl->tasks_done, 1);
 }
 
+// One thread, once every thread that wrote the item's results has passed a barrier with it:
+// complete the item (unless it failed), count it and, when tracing, record
+// (start, end, SM, task << 32 | item).
+__device__ __forceinline__ void finish_item(const RunArgs &p, int task, int item, unsigned long long t_start, bool ok) {
+    if (ok) complete_item(p, task);
+    if (!p.trace) {
+        atomicAdd(&p.ctl->items_done, 1ull);  // result unused: no round trip
+        return;
+    }
+    const long long slot = static_cast<long long>(atomicAdd(&p.ctl->items_done, 1ull));
+    if (slot < p.trace_cap) {
+        unsigned int smid;
+        asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+        unsigned long long *rec = p.trace + 4 * slot;
+        rec[0] = t_start;
+        rec[1] = global_ns();
+        rec[2] = smid;
+        rec[3] = (static_cast<unsigned long long>(task) << 32) | static_cast<unsigned int>(item);
+    }
+}
+
 // Element type of the matrix a run factors: double (the reference's FP64 arithmetic) or
 // float (low-precision Cholesky factor of the mixed-precision solver: SPLIT = 1 TF32
 // products, SPLIT = 3 FP32-accurate split-TF32 products).
@@ -164,48 +191,68 @@ constexpr bool uses_tcgen05() {
     return VEC == 2 && sizeof(T) == 4 && SPLIT == 1 && !ADJ;
 }
 
-// C -= A B^T (GEMM_NT) or the lower part of C -= A A^T (SYRK_LN), one 128 x 128 output tile
-// per item, on tcgen05.
-__device__ __forceinline__ int op_update_tc(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem,
-                                            tc::State *tcs, const void *tmap) {
-    int r0, c0, mm, nn, brow;
-    bool lower = false;
-    const float *B;
+// One 128 x 128 output tile of C -= A B^T (GEMM_NT) or of the lower part of C -= A A^T
+// (SYRK_LN): item -> output offset (r0, c0) inside the task's tile, extent mm x nn, the first
+// row and column of its B panel, and whether it is a diagonal SYRK block.
+struct UpdateGeom {
+    int r0, c0, mm, nn, brow, bcol;
+    bool lower;
+};
+
+__device__ __forceinline__ UpdateGeom update_geom(const DevTask &t, int item) {
+    UpdateGeom g;
     if (t.op == MTD_OP_SYRK_LN) {
         int pb = 0;
         while ((pb + 1) * (pb + 2) / 2 <= item) ++pb;
         const int qb = item - pb * (pb + 1) / 2;
-        r0 = pb * kGemmTile;
-        c0 = qb * kGemmTile;
-        mm = min(kGemmTile, t.m - r0);
-        nn = min(kGemmTile, t.m - c0);
-        lower = pb == qb;
-        B = at<float>(m, t.ar + c0, t.ac);
-        brow = t.ar + c0;
+        g.r0 = pb * kGemmTile;
+        g.c0 = qb * kGemmTile;
+        g.mm = min(kGemmTile, t.m - g.r0);
+        g.nn = min(kGemmTile, t.m - g.c0);
+        g.lower = pb == qb;
+        g.brow = t.ar + g.c0;
+        g.bcol = t.ac;  // SYRK's B panel starts in the same column as A; GEMM_NT's may not
     } else {
         const int nbn = (t.n + kGemmTile - 1) / kGemmTile;
-        r0 = (item / nbn) * kGemmTile;
-        c0 = (item % nbn) * kGemmTile;
-        mm = min(kGemmTile, t.m - r0);
-        nn = min(kGemmTile, t.n - c0);
-        B = at<float>(m, t.br + c0, t.bc);
-        brow = t.br + c0;
+        g.r0 = (item / nbn) * kGemmTile;
+        g.c0 = (item % nbn) * kGemmTile;
+        g.mm = min(kGemmTile, t.m - g.r0);
+        g.nn = min(kGemmTile, t.n - g.c0);
+        g.lower = false;
+        g.brow = t.br + g.c0;
+        g.bcol = t.bc;
     }
-    // the swizzled operand layout wants 1024-byte aligned stage buffers
-    uint8_t *s = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem) + 1023) & ~uintptr_t(1023));
-    float *C = at<float>(m, t.cr + r0, t.cc + c0);
-    // SYRK's B panel starts in the same column as A; GEMM_NT's may not
-    const int bcol = t.op == MTD_OP_SYRK_LN ? t.ac : t.bc;
-    // BF16 updates (operands from the BF16 copy of the panels, same coordinates) when the
-    // depth is whole 128-column stages and both operand slices start on 64-row atoms
-    const bool bf16 = p.tma_bf16 && t.k % tc::kBfBK == 0 && t.ac == bcol && (t.ar + r0) % 64 == 0 && brow % 64 == 0;
-    const bool ok = bf16 ? tc::gemm_nt_tma_bf16<kThreads>(tcs, s, p.tmap_bf16, t.ar + r0, brow, t.ac, t.k, mm, nn, C,
-                                                          m.lda, lower, 0, 0, p.timeout_ns)
-                    : (tmap && t.k % tc::kTmaBK == 0 && t.ac == bcol)
-                        ? tc::gemm_nt_tma<kThreads>(tcs, s, tmap, p.tma, t.ar + r0, brow, t.ac, t.k, mm, nn, C, m.lda,
-                                                    lower, 0, 0, p.timeout_ns)
-                        : tc::gemm_nt<kThreads>(tcs, s, at<float>(m, t.ar + r0, t.ac), m.lda, B, m.lda, mm, nn, t.k, C,
-                                                m.lda, lower, 0, 0, p.timeout_ns);
+    return g;
+}
+
+enum { kTcStaged = 0, kTcTmaTf32 = 1, kTcTmaBf16 = 2 };
+
+// How a GEMM_NT / SYRK_LN item runs on tcgen05: BF16 operands from the BF16 copy of the
+// panels when the depth is whole 128-column stages and both operand slices start on 64-row
+// atoms; TF32 operands by TMA from the matrix's tensor map when the depth is whole 64-column
+// stages; otherwise staged by cp.async.
+__device__ __forceinline__ int tc_path(const RunArgs &p, const DevTask &t, const UpdateGeom &g, bool tmap) {
+    if (t.op != MTD_OP_GEMM_NT && t.op != MTD_OP_SYRK_LN) return kTcStaged;
+    if (p.tma_bf16 && t.k % tc::kBfBK == 0 && t.ac == g.bcol && (t.ar + g.r0) % 64 == 0 && g.brow % 64 == 0)
+        return kTcTmaBf16;
+    if (tmap && t.k % tc::kTmaBK == 0 && t.ac == g.bcol) return kTcTmaTf32;
+    return kTcStaged;
+}
+
+// The 1024-byte aligned start of the tcgen05 stage buffers (the swizzled layouts want it).
+__device__ __forceinline__ uint8_t *tc_stages(void *smem) {
+    return reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem) + 1023) & ~uintptr_t(1023));
+}
+
+// A GEMM_NT / SYRK_LN item with cp.async-staged operands on tcgen05, start to finish (the
+// persistent loop runs the TMA items itself, with their C update deferred).
+__device__ __forceinline__ int op_update_tc(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem,
+                                            tc::State *tcs) {
+    const UpdateGeom g = update_geom(t, item);
+    const float *B = at<float>(m, g.brow, g.bcol);
+    float *C = at<float>(m, t.cr + g.r0, t.cc + g.c0);
+    const bool ok = tc::gemm_nt<kThreads>(tcs, tc_stages(smem), at<float>(m, t.ar + g.r0, t.ac), m.lda, B, m.lda, g.mm,
+                                          g.nn, t.k, C, m.lda, g.lower, 0, 0, p.timeout_ns);
     if (!ok) {
         if (threadIdx.x == 0) report_error(p.ctl, MTD_ERR_TIMEOUT, 0);
         return MTD_ERR_TIMEOUT;
@@ -215,11 +262,11 @@ __device__ __forceinline__ int op_update_tc(const RunArgs &p, const MatCtx &m, c
 
 template <int VEC, typename T, int SPLIT = 1, bool ADJ = false>
 __device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int item, void *smem,
-                                        tc::State *tcs = nullptr, const void *tmap = nullptr) {
+                                        tc::State *tcs = nullptr) {
     if constexpr (ADJ) return dispatch_adjoint<T, VEC, SPLIT>(p, t, item, smem);
     const MatCtx m = mat_ctx<T>(p, t);
     if constexpr (uses_tcgen05<VEC, T, SPLIT, ADJ>())
-        if (t.op == MTD_OP_GEMM_NT || t.op == MTD_OP_SYRK_LN) return op_update_tc(p, m, t, item, smem, tcs, tmap);
+        if (t.op == MTD_OP_GEMM_NT || t.op == MTD_OP_SYRK_LN) return op_update_tc(p, m, t, item, smem, tcs);
     if constexpr (sizeof(T) == 8) {
         switch (t.op) {
         case MTD_OP_POTRF: return op_potrf<T, VEC>(p, m, t, smem);
@@ -245,54 +292,136 @@ __device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int 
     return MTD_ERR_INVALID_ARG;
 }
 
-template <int VEC, typename T, int SPLIT = 1, bool ADJ = false>
-__global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const __grid_constant__ RunArgs p) {
-    extern __shared__ __align__(128) double smem[];
+__device__ __forceinline__ void load_task(const RunArgs &p, int task, DevTask *t) {
+    const int4 *src = reinterpret_cast<const int4 *>(p.tasks + task);
+    int4 *dst = reinterpret_cast<int4 *>(t);
+#pragma unroll
+    for (int w = 0; w < int(sizeof(DevTask) / sizeof(int4)); ++w) dst[w] = __ldg(src + w);
+}
+
+// Named barrier 1 over the threads of warps 1 .. 15 (barrier 0 is __syncthreads).
+__device__ __forceinline__ void sync_drain_warps() {
+    asm volatile("bar.sync 1, %0;" ::"r"(kThreads - 32) : "memory");
+}
+
+// The persistent loop of the tcgen05 kernel (TF32 / BF16 Cholesky factor).  A TMA item
+// (GEMM_NT / SYRK_LN with operands fetched by TMA) runs its loads and MMAs on thread 0 into
+// one of the two TMEM accumulators while warps 1 .. 15 fetch its C values into registers;
+// its C update is deferred to the top of the next iteration, where warps 1 .. 15 write it
+// and thread 32 completes the item (releasing its successors) while thread 0 claims the
+// next item.  So a TMA item's C reads overlap its own MMAs, and its C update and completion
+// overlap the next claim.  The claim may wait: the pending item's completion never depends
+// on thread 0.  The next TMA item writes the other accumulator.
+// (Measured against the alternatives on one B200, Cholesky N = 32768, tile 1536: deferring
+// the C update further, into the next item's MMAs, or starting those MMAs before the C
+// update ends, streams GEMM items faster but completes them later, and the factorisation,
+// which waits on its dependency chain, comes out slower.)
+template <int VEC, typename T, int SPLIT>
+__device__ __forceinline__ void persistent_loop_tc(const RunArgs &p, double *smem, tc::State &tcs) {
     __shared__ int s_cmd, s_task, s_item;
-    __shared__ tc::State tcs;
-    constexpr bool kTc = uses_tcgen05<VEC, T, SPLIT, ADJ>();
-    if constexpr (kTc) tc::init(&tcs);  // TMEM accumulator and barriers, held for the whole run
-    if (threadIdx.x == 0) atomicMin(&p.ctl->start_ns, global_ns());
+    __shared__ tc::Pending pend;
+    __shared__ uint32_t s_buf;       // thread 0: the accumulator the next TMA item writes
+    float cv[tc::kDrainChunks][16];  // warps 1 .. 15: the pending item's C values
+    if (threadIdx.x == 0) {
+        pend.valid = 0;
+        s_buf = 0;
+    }
+    __syncthreads();
     while (true) {
         if (threadIdx.x == 0) {
             int tk = 0, it = 0;
             s_cmd = pop_item(p, &tk, &it);
             s_task = tk;
             s_item = it;
+        } else if (threadIdx.x >= 32 && pend.valid) {
+            tc::drain(pend, cv);
+            sync_drain_warps();
+            if (threadIdx.x == 32) finish_item(p, pend.task, pend.item, pend.t_start, true);
         }
         __syncthreads();
         const int cmd = s_cmd, task = s_task, item = s_item;
         if (cmd != kCmdWork) break;
+        if (threadIdx.x == 0) pend.valid = 0;  // drained above; read again only after a barrier
         const unsigned long long t_start = p.trace ? global_ns() : 0ull;
         DevTask t;
-        {
-            const int4 *src = reinterpret_cast<const int4 *>(p.tasks + task);
-            int4 *dst = reinterpret_cast<int4 *>(&t);
-#pragma unroll
-            for (int w = 0; w < int(sizeof(DevTask) / sizeof(int4)); ++w) dst[w] = __ldg(src + w);
+        load_task(p, task, &t);
+        const UpdateGeom g = update_geom(t, item);
+        const int path = tc_path(p, t, g, p.tma != 0);
+        if (path != kTcStaged) {
+            const MatCtx m = mat_ctx<T>(p, t);
+            float *C = at<float>(m, t.cr + g.r0, t.cc + g.c0);
+            if (threadIdx.x == 0) {
+                const uint32_t acc = tcs.taddr + tc::kAccCols * s_buf;
+                // the tensor maps' addresses are taken on the kernel parameter itself
+                const bool ok = path == kTcTmaBf16
+                                    ? tc::mainloop_tma_bf16(&tcs, tc_stages(smem), p.tmap_bf16, t.ar + g.r0, g.brow,
+                                                            t.ac, t.k, acc, p.timeout_ns)
+                                    : tc::mainloop_tma(&tcs, tc_stages(smem), p.tmap, p.tma, t.ar + g.r0, g.brow,
+                                                       t.ac, t.k, acc, p.timeout_ns);
+                if (ok) {
+                    pend.C = C;
+                    pend.ldc = m.lda;
+                    pend.M = g.mm;
+                    pend.N = g.nn;
+                    pend.lower = g.lower ? 1 : 0;
+                    pend.task = task;
+                    pend.item = item;
+                    pend.t_start = t_start;
+                    pend.acc = acc;
+                    pend.valid = 1;
+                    s_buf ^= 1u;
+                } else {
+                    report_error(p.ctl, MTD_ERR_TIMEOUT, 0);
+                }
+            } else if (threadIdx.x >= 32) {
+                tc::prefetch_c(C, m.lda, g.mm, g.nn, g.lower, cv);
+            }
+            __syncthreads();
+            continue;
         }
-        // the tensor map's address is taken here, on the kernel parameter itself
-        const int st = dispatch<VEC, T, SPLIT, ADJ>(p, t, item, smem, &tcs, p.tma ? p.tmap : nullptr);
+        const int st = dispatch<VEC, T, SPLIT, false>(p, t, item, smem, &tcs);
+        // nothing is pending here (drained above): redefining cv after the tile operation
+        // frees its registers during it
+#pragma unroll
+        for (int c = 0; c < tc::kDrainChunks; ++c)
+#pragma unroll
+            for (int j = 0; j < 16; ++j) cv[c][j] = 0.f;
         __syncthreads();
-        if (threadIdx.x == 0) {
-            if (st == 0) complete_item(p, task);
-            if (!p.trace) {
-                atomicAdd(&p.ctl->items_done, 1ull);  // result unused: no round trip
-                continue;
+        if (threadIdx.x == 0) finish_item(p, task, item, t_start, st == 0);
+    }
+}
+
+template <int VEC, typename T, int SPLIT = 1, bool ADJ = false>
+__global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const __grid_constant__ RunArgs p) {
+    extern __shared__ __align__(128) double smem[];
+    constexpr bool kTc = uses_tcgen05<VEC, T, SPLIT, ADJ>();
+    if (threadIdx.x == 0) atomicMin(&p.ctl->start_ns, global_ns());
+    if constexpr (kTc) {
+        __shared__ tc::State tcs;
+        tc::init(&tcs);  // TMEM accumulators and barriers, held for the whole run
+        persistent_loop_tc<VEC, T, SPLIT>(p, smem, tcs);
+        tc::release(&tcs);
+        return;
+    } else {
+        __shared__ int s_cmd, s_task, s_item;
+        while (true) {
+            if (threadIdx.x == 0) {
+                int tk = 0, it = 0;
+                s_cmd = pop_item(p, &tk, &it);
+                s_task = tk;
+                s_item = it;
             }
-            const long long slot = static_cast<long long>(atomicAdd(&p.ctl->items_done, 1ull));
-            if (slot < p.trace_cap) {
-                unsigned int smid;
-                asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
-                unsigned long long *rec = p.trace + 4 * slot;
-                rec[0] = t_start;
-                rec[1] = global_ns();
-                rec[2] = smid;
-                rec[3] = (static_cast<unsigned long long>(task) << 32) | static_cast<unsigned int>(item);
-            }
+            __syncthreads();
+            const int cmd = s_cmd, task = s_task, item = s_item;
+            if (cmd != kCmdWork) break;
+            const unsigned long long t_start = p.trace ? global_ns() : 0ull;
+            DevTask t;
+            load_task(p, task, &t);
+            const int st = dispatch<VEC, T, SPLIT, ADJ>(p, t, item, smem);
+            __syncthreads();
+            if (threadIdx.x == 0) finish_item(p, task, item, t_start, st == 0);
         }
     }
-    if constexpr (kTc) tc::release(&tcs);
 }
 
 // One task as an ordinary launch (grid = its work items): the node kernel of the

@@ -12,6 +12,9 @@
 // stage and commits the group to that stage's mbarrier; the stage's buffer is refilled only
 // after the barrier says the MMAs that read it are done.  The epilogue reads the accumulator
 // with tcgen05.ld (warp w: TMEM lanes 32 (w % 4) .., columns 32 (w / 4) ..) and updates C.
+// Items whose operands come by TMA (mainloop_tma, mainloop_tma_bf16) run their pipeline on
+// thread 0 alone, into one of two accumulators; the scheduler defers their C update
+// (prefetch_c during the MMAs, drain afterwards, both by warps 1 .. 15).
 //
 // Every mbarrier wait is bounded by a %globaltimer deadline; on expiry the caller's error
 // word is set and the item ends (its result is then not used: the run reports the error).
@@ -32,7 +35,10 @@ constexpr int kAtomK = 4 * kAtomMN;   // bytes between K-adjacent atoms (4 MN at
 constexpr int kOperandBytes = (kBK / 4) * kAtomK;    // 128 x 32 FP32 = 16 KB
 constexpr int kStageBytes = 2 * kOperandBytes;       // A and B
 constexpr int kSmemBytes = kStages * kStageBytes;    // 192 KB
-constexpr uint32_t kTmemCols = 128;
+// Two 128-column FP32 accumulators: the TMA items alternate between them, so one item's
+// MMAs run while the previous item's accumulator is still being read out (see drain).
+constexpr uint32_t kAccCols = 128;
+constexpr uint32_t kTmemCols = 2 * kAccCols;
 
 // Instruction descriptor: F32 accumulator, TF32 A and B, both MN-major, M = 128, N = 128.
 constexpr uint32_t kIdescTf32 = (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | (1u << 16) |
@@ -303,23 +309,23 @@ static_assert(kTmaStages * kTmaStageBytes <= kSmemBytes, "TMA stages fit the eng
 static_assert(kTmaStages <= kStages, "TMA stages use the engine's barriers");
 enum { kTmaNone = 0, kTmaMap2D = 1, kTmaMap3D = 2 };
 
-// C -= A B^T as gemm_nt, with both operands fetched by TMA from the FP32 matrix `map`
-// describes, 128-byte swizzle with 32-byte atoms (an atom row k holds 32 consecutive MN
-// elements of column k, its 32-byte chunks at c ^ (k % 4)).  A = rows a_row .. a_row + 127,
-// B = rows b_row .., columns k0 .. k0 + K - 1 (K a multiple of 64; a_row, b_row multiples of
-// 32; rows past the matrix read as zero).  map_kind kTmaMap3D: dims (32 rows of an atom,
-// columns, atoms), box 32 x 64 x 4, one load per operand and stage; kTmaMap2D: dims (rows,
-// columns), box 32 x 64, four loads per operand and stage (the number of TMA instructions,
-// not the bytes, limited the 32 x 32 boxes of the first design to ~25 GB/s per SM).  One
-// thread runs the pipeline: per stage one expect_tx and the loads on full[s], then, once the
-// stage has landed, 8 MMAs committed to mbar[s]; a stage is reloaded after its MMAs are done.
-// Operands must already be TF32 values (the tensor core truncates what it reads).
-template <int THREADS>
-__device__ bool gemm_nt_tma(State *st, uint8_t *smem, const void *map, int map_kind, int a_row, int b_row, int k0,
-                            int K, int M, int N, float *C, int64_t ldc, bool lower_only, int r0, int c0,
-                            unsigned long long timeout_ns) {
+// acc(128 x 128) = A B^T into the accumulator at TMEM address `acc`, both operands fetched by
+// TMA from the FP32 matrix `map` describes, 128-byte swizzle with 32-byte atoms (an atom row k
+// holds 32 consecutive MN elements of column k, its 32-byte chunks at c ^ (k % 4)).
+// A = rows a_row .. a_row + 127, B = rows b_row .., columns k0 .. k0 + K - 1 (K a multiple
+// of 64; a_row, b_row multiples of 32; rows past the matrix read as zero).  map_kind
+// kTmaMap3D: dims (32 rows of an atom, columns, atoms), box 32 x 64 x 4, one load per
+// operand and stage; kTmaMap2D: dims (rows, columns), box 32 x 64, four loads per operand
+// and stage (the number of TMA instructions, not the bytes, limited the 32 x 32 boxes of
+// the first design to ~25 GB/s per SM).  Thread 0 alone runs it: per stage one expect_tx
+// and the loads on full[s], then, once the stage has landed, 8 MMAs committed to mbar[s]; a
+// stage is reloaded after its MMAs are done.  On a true return every MMA has completed (the
+// accumulator is final and every stage free); false if a wait timed out.  Operands must
+// already be TF32 values (the tensor core truncates what it reads).
+__device__ bool mainloop_tma(State *st, uint8_t *smem, const void *map, int map_kind, int a_row, int b_row, int k0,
+                             int K, uint32_t acc, unsigned long long timeout_ns) {
     bool ok = true;
-    if (threadIdx.x == 0) {
+    {
         const unsigned long long deadline = now_ns() + timeout_ns;
         const int nk = K / kTmaBK;
         uint32_t ph = st->phases, fph = st->fphases;
@@ -358,7 +364,7 @@ __device__ bool gemm_nt_tma(State *st, uint8_t *smem, const void *map, int map_k
                 asm volatile(
                     "{\n\t.reg .pred p;\n\t"
                     "setp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(st->taddr),
+                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(acc),
                     "l"(ad), "l"(bd), "r"(kIdescTf32), "r"((kt > 0 || g > 0) ? 1u : 0u)
                     : "memory");
             }
@@ -383,13 +389,7 @@ __device__ bool gemm_nt_tma(State *st, uint8_t *smem, const void *map, int map_k
         st->phases = ph;
         st->fphases = fph;
     }
-    // the other threads fetch their part of C while thread 0 runs the pipeline
-    float cv[32];
-    load_c(cv, M, N, C, ldc, lower_only, r0, c0);
-    __shared__ int s_ok;
-    if (threadIdx.x == 0) s_ok = ok ? 1 : 0;
-    __syncthreads();
-    return epilogue(st, s_ok != 0, cv, M, N, C, ldc, lower_only, r0, c0);
+    return ok;
 }
 
 // BF16 updates: C -= A B^T with BF16 operands read by TMA from the BF16 copy of the panels
@@ -398,7 +398,7 @@ __device__ bool gemm_nt_tma(State *st, uint8_t *smem, const void *map, int map_k
 // 128 MN rows x kBfBK columns per operand: two atoms of kBfBK rows x 128 bytes, 16 KB apart
 // (LBO), 8-row groups 1 KB apart (SBO), layout type 2 (128-byte swizzle); this layout was
 // checked bit-exact against a host product of the same BF16 values.  a_row, b_row multiples
-// of 64, K a multiple of kBfBK; otherwise as gemm_nt_tma.
+// of 64, K a multiple of kBfBK; otherwise as mainloop_tma (thread 0 alone, into `acc`).
 constexpr int kBfBK = 128;
 constexpr int kBfStages = 3;
 constexpr int kBfAtomBytes = kBfBK * 128;                   // 64 BF16 x kBfBK rows: 16 KB
@@ -409,16 +409,14 @@ static_assert(kBfStages <= kStages, "BF16 stages use the engine's barriers");
 constexpr uint32_t kIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
                                 (uint32_t(kN >> 3) << 17) | (uint32_t(kM >> 4) << 24);
 
-template <int THREADS>
-__device__ bool gemm_nt_tma_bf16(State *st, uint8_t *smem, const void *map, int a_row, int b_row, int k0, int K, int M,
-                                 int N, float *C, int64_t ldc, bool lower_only, int r0, int c0,
-                                 unsigned long long timeout_ns) {
+__device__ bool mainloop_tma_bf16(State *st, uint8_t *smem, const void *map, int a_row, int b_row, int k0, int K,
+                                  uint32_t acc, unsigned long long timeout_ns) {
     bool ok = true;
-    if (threadIdx.x == 0) {
+    {
         const unsigned long long deadline = now_ns() + timeout_ns;
         const int nk = K / kBfBK;
         uint32_t ph = st->phases, fph = st->fphases;
-        asm volatile("fence.proxy.async.global;" ::: "memory");  // see gemm_nt_tma
+        asm volatile("fence.proxy.async.global;" ::: "memory");  // see mainloop_tma
         auto issue = [&](int s, int kt) {
             const uint32_t bar = smem_addr(&st->full[s]), base = smem_addr(smem + s * kBfStageBytes);
             const int k = k0 + kt * kBfBK;
@@ -443,7 +441,7 @@ __device__ bool gemm_nt_tma_bf16(State *st, uint8_t *smem, const void *map, int 
                 asm volatile(
                     "{\n\t.reg .pred p;\n\t"
                     "setp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(st->taddr),
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(acc),
                     "l"(ad), "l"(bd), "r"(kIdescBf16), "r"((kt > 0 || g > 0) ? 1u : 0u)
                     : "memory");
             }
@@ -465,12 +463,79 @@ __device__ bool gemm_nt_tma_bf16(State *st, uint8_t *smem, const void *map, int 
         st->phases = ph;
         st->fphases = fph;
     }
-    float cv[32];
-    load_c(cv, M, N, C, ldc, lower_only, r0, c0);
-    __shared__ int s_ok_bf;
-    if (threadIdx.x == 0) s_ok_bf = ok ? 1 : 0;
-    __syncthreads();
-    return epilogue(st, s_ok_bf != 0, cv, M, N, C, ldc, lower_only, r0, c0);
+    return ok;
+}
+
+// A TMA item whose accumulator is final but whose update of C is still to be done.
+struct Pending {
+    float *C;
+    int64_t ldc;
+    int M, N, lower;   // C(r, c) for r < M, c < N (and r >= c when lower)
+    int task, item;
+    unsigned long long t_start;
+    uint32_t acc;      // TMEM address of its accumulator
+    int valid;
+};
+
+// The C update of an item is shared by warps 1 .. 15 (warp 0 runs the pipelines).  A warp
+// covers TMEM lane quarter q = warp % 4 (rows 32 q ..); the quarter's 8 chunks of 16 columns
+// are dealt to the warps w = q (mod 4) of 1 .. 15 -- three for q = 0 (chunks first + 3 c),
+// four otherwise (first + 4 c) -- so a warp holds at most 3 chunks.
+constexpr int kDrainChunks = 3;
+__device__ __forceinline__ void drain_share(int &q, int &first, int &step) {
+    const int warp = threadIdx.x >> 5;
+    q = warp & 3;
+    first = q == 0 ? (warp >> 2) - 1 : (warp >> 2);
+    step = q == 0 ? 3 : 4;
+}
+
+// Warps 1 .. 15, while thread 0 runs the item's loads and MMAs: this thread's C values of the
+// item (row 32 q + lane of its chunks; 0 outside the block or above the diagonal), all
+// loads issued back to back.
+__device__ __forceinline__ void prefetch_c(const float *C, int64_t ldc, int M, int N, bool lower,
+                                           float (&cv)[kDrainChunks][16]) {
+    int q, first, step;
+    drain_share(q, first, step);
+    const int row = q * 32 + (threadIdx.x & 31);
+#pragma unroll
+    for (int c = 0; c < kDrainChunks; ++c) {
+        const int ch = first + c * step;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int col = ch * 16 + j;
+            const bool in = ch < kN / 16 && row < M && col < N && (!lower || row >= col);
+            cv[c][j] = in ? __ldcg(C + row + int64_t(col) * ldc) : 0.f;
+        }
+    }
+}
+
+// Warps 1 .. 15, while thread 0 claims and starts the next item: C = cv - accumulator of `pd`
+// (tcgen05.ld of each 16-column chunk, then its stores: one 128-byte line per warp and column).
+__device__ __forceinline__ void drain(const Pending &pd, const float (&cv)[kDrainChunks][16]) {
+    int q, first, step;
+    drain_share(q, first, step);
+    const int row = q * 32 + (threadIdx.x & 31);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+    for (int c = 0; c < kDrainChunks; ++c) {
+        const int ch = first + c * step;
+        if (ch >= kN / 16) break;  // warp-uniform
+        uint32_t v[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(pd.acc + (uint32_t(q * 32) << 16) + uint32_t(ch * 16)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int col = ch * 16 + j;
+            if (row < pd.M && col < pd.N && (!pd.lower || row >= col))
+                pd.C[row + int64_t(col) * pd.ldc] = cv[c][j] - __uint_as_float(v[j]);
+        }
+    }
+    // the accumulator is written again (two TMA items later) only after a CTA barrier
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 }
 
 }  // namespace tc

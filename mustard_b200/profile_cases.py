@@ -14,7 +14,7 @@
 Each case runs `--runs` launches (default 2: the first is the one to capture with
 `-c 1`), checks the run status, and prints the device time of the last launch.  With
 `--trace` the runs record per-item timestamps and the line adds, per tile operation, the
-items, median and summed item time, the busy fraction (summed item time over SMs x span)
+items, median and summed item time, the busy fraction (time inside items over SMs x span)
 and the critical path's composition (mustard_b200.trace_analysis); `--trace-out FILE`
 also writes the records, task spans and critical path as JSON.
 Inputs are the seeded generators of the benchmark (larger than L2 from n = 4096).
@@ -39,7 +39,6 @@ def op_breakdown(g):
         return {}
     t0 = min(r[0] for r in tr)
     t1 = max(r[1] for r in tr)
-    sms = len({r[2] for r in tr})
     per = {}
     for s, e, _sm, task, _item in tr:
         per.setdefault(OP_NAMES.get(g.device_task_op(task), "other"), []).append((e - s) * 1e-3)
@@ -49,7 +48,8 @@ def op_breakdown(g):
         d.sort()
         ops[name] = {"items": len(d), "median_us": d[len(d) // 2], "sum_ms": sum(d) * 1e-3,
                      "share": sum(d) / total}
-    return {"span_ms": (t1 - t0) * 1e-6, "busy": total / (sms * (t1 - t0) * 1e-3), "ops": ops}
+    from mustard_b200 import trace_analysis
+    return {"span_ms": (t1 - t0) * 1e-6, "busy": trace_analysis.busy_fraction(tr), "ops": ops}
 
 
 def main():

@@ -4,8 +4,10 @@ A traced run (``TaskGraph.set_trace(True)``) records, per work item, the %global
 at which its CTA started and finished it, the SM and the device task.  From those records:
 
 - a task's span runs from its first item's start to its last item's end;
-- the busy fraction is the summed item time over (SMs x the run's span); the idle fraction
-  is the rest (queue waits, dependency stalls, the tail);
+- the busy fraction is the time each SM spent inside at least one item, summed over SMs,
+  over (SMs x the run's span); the idle fraction is the rest (queue waits, dependency
+  stalls, the tail).  Items of one SM may overlap: the tensor-core kernel finishes an item's
+  C update while its next item's loads and MMAs already run;
 - the critical path is walked back from the task that ended last, each time to the
   predecessor (device task dependencies) that ended last; along it, ``wait`` is the time
   from that predecessor's end to the task's first item start (the scheduler's hand-off
@@ -38,8 +40,21 @@ def busy_fraction(records):
         return 0.0
     t0 = min(r[0] for r in records)
     t1 = max(r[1] for r in records)
-    sms = len({r[2] for r in records})
-    return sum(e - s for s, e, _, _, _ in records) / (sms * (t1 - t0))
+    per_sm = {}
+    for s, e, sm, _, _ in records:
+        per_sm.setdefault(sm, []).append((s, e))
+    busy = 0
+    for iv in per_sm.values():  # union of the SM's item intervals
+        iv.sort()
+        cs, ce = iv[0]
+        for s, e in iv[1:]:
+            if s > ce:
+                busy += ce - cs
+                cs, ce = s, e
+            else:
+                ce = max(ce, e)
+        busy += ce - cs
+    return busy / (len(per_sm) * (t1 - t0))
 
 
 def critical_path(graph, spans):

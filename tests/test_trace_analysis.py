@@ -40,3 +40,9 @@ def test_spans_busy_and_critical_path(tmp_path):
     assert abs(s["critical_path"]["per_op"]["POTRF"]["in_task_ms"] - 150e-6) < 1e-15
     out = json.load(open(tmp_path / "t.json"))
     assert len(out["records"]) == len(RECORDS) and set(out["tasks"]) == {"0", "1", "2", "3", "4"}
+
+
+def test_busy_counts_overlapping_items_of_an_sm_once():
+    # SM 0: an item whose C update (100..130) overlaps the next item (110..200), then a gap
+    recs = [(0, 130, 0, 0, 0), (110, 200, 0, 1, 0), (250, 300, 0, 2, 0), (0, 300, 1, 3, 0)]
+    assert abs(trace_analysis.busy_fraction(recs) - (250 + 300) / (2 * 300)) < 1e-12
