@@ -47,6 +47,23 @@ REASON_BITS = {
 }
 
 
+def max_over_ranks(x, dist, device):
+    """The largest x over all ranks (every rank must call it, in the same order); x itself
+    in a single-process run.  Step times are reported as the slowest rank's."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world, flops_per_rank_step, ms_per_step):
+    """Whole-job TFLOP/s of `world` replicas, each doing flops_per_rank_step per step, timed
+    by the slowest rank's ms_per_step."""
+    return world * flops_per_rank_step / (ms_per_step * 1e-3) / 1e12
+
+
 def flops_lu(n):
     return 2.0 * n ** 3 / 3.0
 
@@ -274,13 +291,9 @@ def main():
     stats_lu = g_lu.stats() if args.trace else None
     stats_ch = g_ch.stats() if args.trace else None
 
-    dev_ms = (t_lu + t_ch) / args.steps
-    if dist:
-        tt = torch.tensor([dev_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        dev_ms = float(tt.item())
+    dev_ms = max_over_ranks((t_lu + t_ch) / args.steps, dist, dev)
     flops_step = (flops_lu(n) if args.only != "chol" else 0.0) + (flops_chol(n) if args.only != "lu" else 0.0)
-    value = world * flops_step / (dev_ms * 1e-3) / 1e12
+    value = aggregate_rate(world, flops_step, dev_ms)
 
     # --- end to end through the public API with host buffers ---------------------
     e2e = None
@@ -343,13 +356,9 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         check_status()
-        e2e_ms = e0.elapsed_time(e1) / args.steps
-        if dist:
-            tt = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_ms = float(tt.item())
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, dev)
         nbytes = n * n * 8
-        e2e = {"value": world * flops_step / (e2e_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
+        e2e = {"value": aggregate_rate(world, flops_step, e2e_ms), "unit": "TFLOP/s",
                "h2d_bytes_per_step": 2 * nbytes, "d2h_bytes_per_step": 2 * nbytes, "ms_per_step": e2e_ms}
         del h_lu, h_ch, out_lu, out_ch, bufs
 
