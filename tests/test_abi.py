@@ -127,3 +127,62 @@ def test_trsm_needs_matching_diagonal_factorisation(mtd):
     with pytest.raises(mtd.MtdError) as e:
         g.finalize()
     assert e.value.status == 7
+
+
+def _deps_restated(tasks):
+    """Last writer of every tile a task reads or writes (mustard/mustard.h:279-296), plus --
+    for custom graphs -- every task that read the written tile since its last write."""
+    last, readers, out = {}, {}, []
+    for idx, (_op, write, reads) in enumerate(tasks):
+        d = {last[t] for t in list(reads) + [write] if t in last}
+        d |= set(readers.get(write, ()))
+        out.append(sorted(d))
+        last[write] = idx
+        readers[write] = []
+        for t in reads:
+            if t != write:
+                readers.setdefault(t, []).append(idx)
+    return out
+
+
+def _random_cholesky_ops(draw, st, t):
+    """One valid Cholesky-shaped task on a t x t tile grid: (op name, write, reads)."""
+    kind = draw(st.sampled_from(["OP_POTRF", "OP_TRSM_RLT", "OP_SYRK_LN", "OP_GEMM_NT"]))
+    if kind == "OP_POTRF":
+        k = draw(st.integers(0, t - 1))
+        return kind, (k, k), [(k, k)]
+    if kind == "OP_GEMM_NT":
+        k = draw(st.integers(0, t - 3))
+        i = draw(st.integers(k + 1, t - 2))
+        j = draw(st.integers(i + 1, t - 1))
+        return kind, (j, i), [(j, i), (j, k), (i, k)]
+    k = draw(st.integers(0, t - 2))
+    i = draw(st.integers(k + 1, t - 1))
+    if kind == "OP_TRSM_RLT":
+        return kind, (i, k), [(k, k), (i, k)]
+    return kind, (i, i), [(i, k), (i, i)]
+
+
+def test_custom_graph_dependencies_property(mtd):
+    """Random task lists on a 4 x 4 grid: the library's dependency lists equal the restated
+    rule (read-after-write, write-after-write and write-after-read edges)."""
+    hypothesis = pytest.importorskip("hypothesis")
+    st = hypothesis.strategies
+
+    @st.composite
+    def task_lists(draw):
+        return [_random_cholesky_ops(draw, st, 4) for _ in range(draw(st.integers(1, 40)))]
+
+    @hypothesis.settings(max_examples=150, deadline=None, database=None)
+    @hypothesis.given(task_lists())
+    def check(tasks):
+        g = mtd.TaskGraph(mtd.KIND_CUSTOM, 400, 100)
+        try:
+            for op, write, reads in tasks:
+                g.add_task(getattr(mtd, op), write, reads)
+            want = _deps_restated(tasks)
+            assert [g.deps(i) for i in range(len(tasks))] == want
+        finally:
+            g.close()
+
+    check()
