@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <mutex>
@@ -75,11 +76,16 @@ struct mtd_graph {
 
 namespace {
 
+// Once per device and vector width: the kernels' dynamic shared-memory limits.  Runs on
+// different graphs may start from several host threads at once.
 template <int VEC>
 int smem_setup(int device) {
-    static bool done[64] = {false};
+    static std::atomic<bool> done[64];
+    static std::mutex mu;
     if (device < 0 || device >= 64) return MTD_ERR_INVALID_ARG;
-    if (!done[device]) {
+    if (done[device].load(std::memory_order_acquire)) return MTD_OK;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!done[device].load(std::memory_order_relaxed)) {
         const int bytes = kOpSmemBytes();
         if (cudaFuncSetAttribute(persistent_kernel<VEC, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  bytes) != cudaSuccess ||
@@ -94,7 +100,7 @@ int smem_setup(int device) {
             cudaFuncSetAttribute(persistent_kernel<VEC, float, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  bytes) != cudaSuccess)
             return MTD_ERR_CUDA;
-        done[device] = true;
+        done[device].store(true, std::memory_order_release);
     }
     return MTD_OK;
 }
