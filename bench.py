@@ -149,8 +149,19 @@ def cpu_cores():
         return os.cpu_count()
 
 
-def run_reference(args, rank):
-    """The reference arm: the oracle port of the reference's tiled algorithm on the host."""
+def workload_config(args, world):
+    """The `config` of both arms' JSON lines: the workload the metric is quoted on."""
+    n = args.n
+    return {"workload": f"plain FP64 tiled LU + Cholesky, N={n}", "n": n,
+            "tile_lu": args.tile_lu, "tile_chol": args.tile_chol,
+            "lu_input": "U[-1,1) + N*I", "chol_input": "B B^T/N + I, B=U[-1,1)",
+            "parallelism": f"replicas{world}" if world > 1 else "1 GPU",
+            "l2": "inputs (4.6 GB each) larger than the 126 MB L2"}
+
+
+def run_reference(args, rank, world):
+    """The reference arm: the oracle port of the reference's tiled algorithm on the host,
+    timed on a bounded sample (N = --cpu-n) of the workload in `config`."""
     if rank != 0:
         return
     cores = cpu_cores()
@@ -169,8 +180,7 @@ def run_reference(args, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": f"tiled LU + Cholesky FP64, N={args.cpu_n} (CPU sample of N={args.n})",
-                                        "n": args.cpu_n, "tile": args.cpu_tile},
+        "data": "synthetic", "config": workload_config(args, world),
         "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -209,7 +219,7 @@ def main():
     args.warmup = max(3, args.warmup)
 
     if args.impl == "reference":
-        run_reference(args, rank)
+        run_reference(args, rank, world)
         return
 
     import torch
@@ -417,11 +427,7 @@ def main():
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"plain FP64 tiled LU + Cholesky, N={n}", "n": n,
-                       "tile_lu": args.tile_lu, "tile_chol": args.tile_chol,
-                       "lu_input": "U[-1,1) + N*I", "chol_input": "B B^T/N + I, B=U[-1,1)",
-                       "parallelism": f"replicas{world}" if world > 1 else "1 GPU",
-                       "l2": "inputs (4.6 GB each) larger than the 126 MB L2"},
+            "config": workload_config(args, world),
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "mixed_ir": mixed,
             "clocks": clocks.summary(),
             "gpu_launches": args.steps * (1 if args.only else 2) * launches_per_run,

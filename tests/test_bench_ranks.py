@@ -1,6 +1,7 @@
 """bench.py's multi-rank host logic, on CPU: two gloo ranks take the same steps the NCCL ranks
 of `bench.py --gpus 2` take (barrier, max over ranks of the step time, whole-job rate)."""
 import datetime
+import os
 import socket
 
 import pytest
@@ -52,3 +53,31 @@ def test_two_ranks_report_the_slowest_rank_and_the_whole_job_rate():
     assert all(ms == 11.0 for _, ms, _ in out)  # both ranks see the slowest rank's time
     # two replicas of 1e12 flop per step in 11 ms: 181.8 TFLOP/s for the whole job
     assert all(v == pytest.approx(2 * 1e12 / 11e-3 / 1e12) for _, _, v in out)
+
+
+def _reference_arm(env_extra):
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, **env_extra)
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "3", "--cpu-n", "600", "--cpu-tile", "300"],
+                         capture_output=True, text=True, env=env, timeout=300)
+    assert out.returncode == 0, out.stderr
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    return [json.loads(l) for l in lines]
+
+
+def test_reference_arm_line_and_other_ranks():
+    (line,) = _reference_arm({"RANK": "0", "WORLD_SIZE": "1"})
+    assert line["impl"] == "reference" and line["metric"] == bench.METRIC and line["unit"] == "TFLOP/s"
+    assert line["higher_is_better"] is True and line["value"] > 0
+    # the workload of the measured arm; the CPU sample is described in cpu_baseline
+    assert line["config"]["workload"] == "plain FP64 tiled LU + Cholesky, N=24000"
+    cb = line["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["value"] == line["value"] and cb["cores"] >= 1 and "N=600" in cb["sample"]
+    assert line["e2e"] == {"value": line["value"], "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
+    # under torchrun only rank 0 works and prints
+    assert _reference_arm({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"}) == []
