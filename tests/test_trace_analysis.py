@@ -46,3 +46,20 @@ def test_busy_counts_overlapping_items_of_an_sm_once():
     # SM 0: an item whose C update (100..130) overlaps the next item (110..200), then a gap
     recs = [(0, 130, 0, 0, 0), (110, 200, 0, 1, 0), (250, 300, 0, 2, 0), (0, 300, 1, 3, 0)]
     assert abs(trace_analysis.busy_fraction(recs) - (250 + 300) / (2 * 300)) < 1e-12
+
+
+def test_op_breakdown_of_a_traced_run():
+    from mustard_b200 import profile_cases
+
+    class Traced(FakeGraph):
+        def trace(self):
+            return RECORDS
+
+    out = profile_cases.op_breakdown(Traced())
+    assert abs(out["span_ms"] - 500e-6) < 1e-15
+    assert abs(out["busy"] - trace_analysis.busy_fraction(RECORDS)) < 1e-12
+    ops = out["ops"]
+    assert set(ops) == {"POTRF", "TRSM_RLT", "GEMM_NT"}
+    assert ops["POTRF"]["items"] == 2 and ops["TRSM_RLT"]["items"] == 3 and ops["GEMM_NT"]["items"] == 2
+    assert abs(sum(o["share"] for o in ops.values()) - 1.0) < 1e-12
+    assert abs(ops["TRSM_RLT"]["sum_ms"] - (90 + 190 + 145) * 1e-6) < 1e-15
