@@ -2,7 +2,9 @@
 
 ``spd_kappa(n, kappa, seed)``  -- B B^T / n + alpha I with alpha = (4/3) / (kappa - 1): the
                                  spectrum of B B^T / n (B = U[-1, 1), variance 1/3) fills
-                                 [~0, 4/3], so cond_2(A) ~= kappa (the configs' inputs)
+                                 [~0, 4/3], so cond_2(A) ~= kappa (the configs' inputs) while
+                                 alpha is far above the smallest eigenvalue of B B^T / n,
+                                 about 1 / (3 n^2) (at n = 32768: kappa up to 1e8)
 ``rhs(n, k, seed)``            -- right-hand sides with i.i.d. N(0, 1) entries
 ``solve_fp64(a, b)``           -- LAPACK dpotrf/dpotrs reference solution in FP64
 ``backward_error(a, x, b)``    -- max over columns of ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf)
