@@ -1,0 +1,233 @@
+"""A model of the persistent scheduler's device protocol (scheduler.cuh), checked on CPU under
+random interleavings of CTAs.
+
+Each CTA is a coroutine that yields at every step the device performs as one global memory
+operation, so a random scheduler explores interleavings the GPU may produce:
+
+- claim (claim_item): read `avail`; fetch-and-add -1 on `avail`, undone if the old value
+  was not positive; fetch-and-add +1 on `head`; wait for the reserved slot to be written;
+- run the item, then complete it (complete_item): decrement the task's items-left counter;
+  the last item decrements each successor's predecessor counter, and a successor that
+  reaches zero is pushed (release_task): fetch-and-add on `tail`, write the slots, then
+  fetch-and-add their number on `avail`.  A task without items (a join) completes on the
+  spot and releases its own successors.
+
+Checked: every work item runs exactly once, no task starts before every item of its
+predecessors has run, every queue slot is claimed once, and the run terminates.
+"""
+import random
+
+import pytest
+
+EMPTY = None
+
+
+class Queue:
+    def __init__(self, cap):
+        self.avail = 0
+        self.head = 0
+        self.tail = 0
+        self.slots = [EMPTY] * cap
+
+
+class Model:
+    def __init__(self, n_items, succ, deps, queue_of, n_queues):
+        self.n_items = n_items                 # per task (0: a join)
+        self.succ = succ
+        self.deps = list(deps)                 # predecessor counters
+        self.items_left = list(n_items)
+        self.queue_of = queue_of
+        self.queues = [Queue(sum(n for t, n in enumerate(n_items) if queue_of[t] == q) + 1)
+                       for q in range(n_queues)]
+        self.tasks_done = 0
+        self.n_tasks = len(n_items)
+        self.finished = [0] * len(n_items)     # items of each task whose work is done
+        self.data_done = set()                 # tasks whose every item (or join) is done
+        self.done_tasks = set()                # tasks counted in tasks_done
+        self.runs = []                         # (task, item) in execution order
+        self.started = {}
+
+    # release_task: a stack of tasks whose counters reached zero (joins complete on the spot)
+    def release(self, task):
+        stack = [task]
+        while stack:
+            tk = stack.pop()
+            n = self.n_items[tk]
+            if n > 0:
+                q = self.queues[self.queue_of[tk]]
+                base = q.tail
+                q.tail += n
+                yield
+                for i in range(n):
+                    q.slots[base + i] = (tk, i)
+                    yield
+                q.avail += n                   # after the slots (the device fences in between)
+                yield
+                continue
+            self.data_done.add(tk)             # a join: nothing to run
+            for s in self.succ[tk]:
+                self.deps[s] -= 1
+                left = self.deps[s]
+                yield
+                if left == 0:
+                    stack.append(s)
+            self.done_tasks.add(tk)
+            self.tasks_done += 1
+            yield
+
+    def complete(self, task):
+        self.items_left[task] -= 1
+        left = self.items_left[task]
+        yield
+        if left != 0:
+            return
+        for s in self.succ[task]:
+            self.deps[s] -= 1
+            left_s = self.deps[s]
+            yield
+            if left_s == 0:
+                yield from self.release(s)
+        self.done_tasks.add(task)
+        self.tasks_done += 1
+        yield
+
+    def cta(self):
+        while True:
+            if self.tasks_done >= self.n_tasks:
+                return
+            claimed = None
+            avail = [q.avail for q in self.queues]  # one round trip
+            yield
+            for qi, q in enumerate(self.queues):
+                if avail[qi] <= 0:
+                    continue
+                old = q.avail
+                q.avail -= 1
+                yield
+                if old <= 0:                  # taken meanwhile: give the unit back
+                    q.avail += 1
+                    yield
+                    continue
+                h = q.head
+                q.head += 1
+                yield
+                while q.slots[h] is EMPTY:    # reserved: its producer is between tail and write
+                    yield
+                claimed = q.slots[h]
+                q.slots[h] = "claimed"
+                break
+            if claimed is None:
+                yield                         # back off and retry
+                continue
+            task, item = claimed
+            self.started.setdefault(task, set(self.data_done))
+            self.runs.append((task, item))
+            yield                             # the item's work
+            self.finished[task] += 1
+            if self.finished[task] == self.n_items[task]:
+                self.data_done.add(task)
+            yield from self.complete(task)
+
+
+def cholesky_dag(t):
+    """The reference's tiled Cholesky task list (cholesky_mustard.cu:224-395) as tasks with
+    items, last-writer predecessors, and the three-queue assignment (0: POTRF/TRSM/SYRK and
+    the updates one column ahead, 1: two to three ahead, 2: the rest)."""
+    tasks, write_of = [], {}
+    for k in range(t):
+        tasks.append(("POTRF", (k, k), [(k, k)], 0))
+        for i in range(k + 1, t):
+            tasks.append(("TRSM", (i, k), [(k, k), (i, k)], 0))
+        for i in range(k + 1, t):
+            tasks.append(("SYRK", (i, i), [(i, i), (i, k)], 0))
+            for j in range(i + 1, t):
+                ahead = i - k
+                tasks.append(("GEMM", (j, i), [(j, i), (j, k), (i, k)], 0 if ahead <= 1 else 1 if ahead <= 3 else 2))
+    preds = []
+    for idx, (_op, w, reads, _q) in enumerate(tasks):
+        preds.append(sorted({write_of[x] for x in reads + [w] if x in write_of}))
+        write_of[w] = idx
+    succ = [[] for _ in tasks]
+    for i, ps in enumerate(preds):
+        for p in ps:
+            succ[p].append(i)
+    return tasks, preds, succ
+
+
+def run_model(tasks, preds, succ, n_items, n_ctas, seed, max_steps=2_000_000):
+    rng = random.Random(seed)
+    m = Model(n_items, succ, [len(p) for p in preds], [q for *_, q in tasks], 3)
+    for r in (i for i, p in enumerate(preds) if not p):  # kernel_populate_queue
+        for _ in m.release(r):
+            pass
+    ctas = [m.cta() for _ in range(n_ctas)]
+    live = list(range(n_ctas))
+    steps = 0
+    while live:
+        i = rng.choice(live)
+        try:
+            next(ctas[i])
+        except StopIteration:
+            live.remove(i)
+        steps += 1
+        assert steps < max_steps, "no termination"
+    return m
+
+
+@pytest.mark.parametrize("t,n_ctas,seed", [(3, 2, 1), (4, 4, 2), (5, 8, 3), (6, 3, 4), (6, 16, 5)])
+def test_cholesky_dag_runs_each_item_once_in_dependency_order(t, n_ctas, seed):
+    tasks, preds, succ = cholesky_dag(t)
+    rng = random.Random(seed)
+    # a few items per task, and some joins (no items) like the nested factorisations' joins
+    n_items = [0 if (idx % 7 == 3 and preds[idx]) else rng.randint(1, 3) for idx in range(len(tasks))]
+    m = run_model(tasks, preds, succ, n_items, n_ctas, seed)
+    want = sorted((tk, i) for tk, n in enumerate(n_items) for i in range(n))
+    assert sorted(m.runs) == want                       # every item exactly once
+    assert m.tasks_done == len(tasks) and m.done_tasks == set(range(len(tasks)))
+    for tk, done_before in m.started.items():          # predecessors' work done before a start
+        assert set(preds[tk]) <= done_before, tk
+    for q in m.queues:                                  # every pushed slot claimed once
+        assert q.head == q.tail and q.avail == 0
+        assert all(s in (EMPTY, "claimed") for s in q.slots)
+        assert q.slots[:q.tail] == ["claimed"] * q.tail
+
+
+def test_model_detects_a_broken_claim():
+    """The checks catch a mistake: a claim that skips the avail count (reads head blindly)
+    ends with items run twice or never, or claims a slot nobody reserved."""
+    tasks, preds, succ = cholesky_dag(4)
+    n_items = [2] * len(tasks)
+
+    class Broken(Model):
+        def cta(self):
+            while self.tasks_done < self.n_tasks:
+                q = self.queues[0]
+                if q.head >= len(q.slots) - 1:
+                    return
+                h = q.head
+                yield
+                q.head = h + 1                # not atomic: two CTAs can take the same slot
+                yield
+                if q.slots[h] in (EMPTY, "claimed"):
+                    return
+                task, item = q.slots[h]
+                self.runs.append((task, item))
+                yield from self.complete(task)
+
+    rng = random.Random(7)
+    m = Broken(n_items, succ, [len(p) for p in preds], [0] * len(tasks), 3)
+    for r in (i for i, p in enumerate(preds) if not p):
+        for _ in m.release(r):
+            pass
+    ctas = [m.cta() for _ in range(6)]
+    live = list(range(6))
+    for _ in range(200_000):
+        if not live:
+            break
+        i = rng.choice(live)
+        try:
+            next(ctas[i])
+        except StopIteration:
+            live.remove(i)
+    want = sorted((tk, i) for tk, n in enumerate(n_items) for i in range(n))
+    assert sorted(m.runs) != want
