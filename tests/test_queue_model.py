@@ -12,8 +12,12 @@ operation, so a random scheduler explores interleavings the GPU may produce:
   fetch-and-add their number on `avail`.  A task without items (a join) completes on the
   spot and releases its own successors.
 
-Checked: every work item runs exactly once, no task starts before every item of its
-predecessors has run, every queue slot is claimed once, and the run terminates.
+The tcgen05 kernel's variant (`deferred`): a GEMM / SYRK item is completed only during the
+CTA's next claim, the completion and the claim interleaving step by step.
+
+Checked, in both: every work item runs exactly once, no task starts before every item of its
+predecessors has run, every queue slot is claimed once, and the run terminates (a CTA holding
+a pending item never waits on itself).
 """
 import random
 
@@ -91,42 +95,82 @@ class Model:
         self.tasks_done += 1
         yield
 
+    def claim(self):
+        """One attempt (claim_item); returns (task, item), "exit" or None."""
+        if self.tasks_done >= self.n_tasks:
+            return "exit"
+        avail = [q.avail for q in self.queues]  # one round trip
+        yield
+        for qi, q in enumerate(self.queues):
+            if avail[qi] <= 0:
+                continue
+            old = q.avail
+            q.avail -= 1
+            yield
+            if old <= 0:                      # taken meanwhile: give the unit back
+                q.avail += 1
+                yield
+                continue
+            h = q.head
+            q.head += 1
+            yield
+            while q.slots[h] is EMPTY:        # reserved: its producer is between tail and write
+                yield
+            claimed = q.slots[h]
+            q.slots[h] = "claimed"
+            return claimed
+        return None
+
+    def run_item(self, task, item):
+        self.started.setdefault(task, set(self.data_done))
+        self.runs.append((task, item))
+        yield                                 # the item's work
+        self.finished[task] += 1
+        if self.finished[task] == self.n_items[task]:
+            self.data_done.add(task)
+
     def cta(self):
         while True:
-            if self.tasks_done >= self.n_tasks:
+            claimed = yield from self.claim()
+            if claimed == "exit":
                 return
-            claimed = None
-            avail = [q.avail for q in self.queues]  # one round trip
-            yield
-            for qi, q in enumerate(self.queues):
-                if avail[qi] <= 0:
-                    continue
-                old = q.avail
-                q.avail -= 1
-                yield
-                if old <= 0:                  # taken meanwhile: give the unit back
-                    q.avail += 1
-                    yield
-                    continue
-                h = q.head
-                q.head += 1
-                yield
-                while q.slots[h] is EMPTY:    # reserved: its producer is between tail and write
-                    yield
-                claimed = q.slots[h]
-                q.slots[h] = "claimed"
-                break
             if claimed is None:
                 yield                         # back off and retry
                 continue
-            task, item = claimed
-            self.started.setdefault(task, set(self.data_done))
-            self.runs.append((task, item))
-            yield                             # the item's work
-            self.finished[task] += 1
-            if self.finished[task] == self.n_items[task]:
-                self.data_done.add(task)
-            yield from self.complete(task)
+            yield from self.run_item(*claimed)
+            yield from self.complete(claimed[0])
+
+    def cta_deferred(self, deferred_ops, rng):
+        """The tcgen05 kernel's loop: an item of a deferred kind is completed only at the
+        next claim, by other threads of the CTA, while thread 0 claims (the two interleave
+        step by step); an item of another kind finds nothing pending and completes at once."""
+        pending = None
+        while True:
+            gens = {"claim": self.claim()}
+            if pending is not None:
+                gens["complete"] = self.complete(pending)
+            result = None
+            while gens:
+                k = rng.choice(sorted(gens))
+                try:
+                    next(gens[k])
+                except StopIteration as e:
+                    if k == "claim":
+                        result = e.value
+                    del gens[k]
+                yield
+            pending = None
+            if result == "exit":
+                return
+            if result is None:
+                yield
+                continue
+            task, item = result
+            yield from self.run_item(task, item)
+            if self.op[task] in deferred_ops:
+                pending = task
+            else:
+                yield from self.complete(task)
 
 
 def cholesky_dag(t):
@@ -154,13 +198,15 @@ def cholesky_dag(t):
     return tasks, preds, succ
 
 
-def run_model(tasks, preds, succ, n_items, n_ctas, seed, max_steps=2_000_000):
+def run_model(tasks, preds, succ, n_items, n_ctas, seed, deferred=False, max_steps=2_000_000):
     rng = random.Random(seed)
     m = Model(n_items, succ, [len(p) for p in preds], [q for *_, q in tasks], 3)
+    m.op = [op for op, *_ in tasks]
     for r in (i for i, p in enumerate(preds) if not p):  # kernel_populate_queue
         for _ in m.release(r):
             pass
-    ctas = [m.cta() for _ in range(n_ctas)]
+    ctas = [m.cta_deferred({"GEMM", "SYRK"}, random.Random(seed * 31 + c)) if deferred else m.cta()
+            for c in range(n_ctas)]
     live = list(range(n_ctas))
     steps = 0
     while live:
@@ -174,13 +220,14 @@ def run_model(tasks, preds, succ, n_items, n_ctas, seed, max_steps=2_000_000):
     return m
 
 
-@pytest.mark.parametrize("t,n_ctas,seed", [(3, 2, 1), (4, 4, 2), (5, 8, 3), (6, 3, 4), (6, 16, 5)])
-def test_cholesky_dag_runs_each_item_once_in_dependency_order(t, n_ctas, seed):
+@pytest.mark.parametrize("deferred", [False, True])
+@pytest.mark.parametrize("t,n_ctas,seed", [(3, 2, 1), (4, 4, 2), (5, 8, 3), (6, 3, 4), (6, 16, 5), (2, 1, 6)])
+def test_cholesky_dag_runs_each_item_once_in_dependency_order(t, n_ctas, seed, deferred):
     tasks, preds, succ = cholesky_dag(t)
     rng = random.Random(seed)
     # a few items per task, and some joins (no items) like the nested factorisations' joins
     n_items = [0 if (idx % 7 == 3 and preds[idx]) else rng.randint(1, 3) for idx in range(len(tasks))]
-    m = run_model(tasks, preds, succ, n_items, n_ctas, seed)
+    m = run_model(tasks, preds, succ, n_items, n_ctas, seed, deferred=deferred)
     want = sorted((tk, i) for tk, n in enumerate(n_items) for i in range(n))
     assert sorted(m.runs) == want                       # every item exactly once
     assert m.tasks_done == len(tasks) and m.done_tasks == set(range(len(tasks)))
