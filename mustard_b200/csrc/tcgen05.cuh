@@ -482,12 +482,32 @@ struct Pending {
 // are dealt to the warps w = q (mod 4) of 1 .. 15 -- three for q = 0 (chunks first + 3 c),
 // four otherwise (first + 4 c) -- so a warp holds at most 3 chunks.
 constexpr int kDrainChunks = 3;
+__host__ __device__ constexpr int drain_first(int warp) { return (warp & 3) == 0 ? (warp >> 2) - 1 : (warp >> 2); }
+__host__ __device__ constexpr int drain_step(int warp) { return (warp & 3) == 0 ? 3 : 4; }
 __device__ __forceinline__ void drain_share(int &q, int &first, int &step) {
     const int warp = threadIdx.x >> 5;
     q = warp & 3;
-    first = q == 0 ? (warp >> 2) - 1 : (warp >> 2);
-    step = q == 0 ? 3 : 4;
+    first = drain_first(warp);
+    step = drain_step(warp);
 }
+// Every (lane quarter, 16-column chunk) of the accumulator is written by exactly one of warps
+// 1 .. 15, a warp of that quarter, within kDrainChunks chunks of its own.
+constexpr bool drain_covers_once() {
+    for (int q = 0; q < 4; ++q)
+        for (int ch = 0; ch < kN / 16; ++ch) {
+            int owners = 0;
+            for (int w = 1; w < 16; ++w) {
+                if ((w & 3) != q) continue;
+                for (int c = 0; c < kDrainChunks; ++c)
+                    if (drain_first(w) + c * drain_step(w) == ch) ++owners;
+            }
+            if (owners != 1) return false;
+        }
+    for (int w = 1; w < 16; ++w)  // and no warp has a chunk beyond the ones it holds
+        if (drain_first(w) < 0 || drain_first(w) + kDrainChunks * drain_step(w) < kN / 16) return false;
+    return true;
+}
+static_assert(drain_covers_once(), "the C update covers the accumulator once");
 
 // Warps 1 .. 15, while thread 0 runs the item's loads and MMAs: this thread's C values of the
 // item (row 32 q + lane of its chunks; 0 outside the block or above the diagonal), all
