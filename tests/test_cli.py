@@ -48,3 +48,17 @@ def test_ragged_tile_and_generators():
     rc, out, err = run("lu_mustard", "-n=2500", "--tile=768", "--subgraph", "--gen=uniform", "--verify", "-v")
     assert rc == 0, err
     assert "Result passes verification: 1" in out and "totalNodes=" in out
+
+
+@pytest.mark.gpu
+def test_dot_dump_has_the_reference_dependencies(tmp_path):
+    # --dot writes ./graph.dot (cholesky_mustard.cu:447-450): one edge per predecessor
+    from oracle import tiled
+    p = subprocess.run([os.path.join(BIN, "cholesky_mustard"), "-n=900", "-t=3", "--subgraph", "--dot"],
+                       capture_output=True, text=True, timeout=300, cwd=str(tmp_path))
+    assert p.returncode == 0, p.stderr
+    text = (tmp_path / "graph.dot").read_text()
+    assert text.startswith("digraph tasks {") and text.rstrip().endswith("}")
+    edges = sorted(tuple(map(int, m)) for m in re.findall(r"(\d+) -> (\d+);", text))
+    deps = tiled.subgraph_dependencies(tiled.cholesky_tasks(3))
+    assert edges == sorted((d, t) for t, ds in enumerate(deps) for d in ds)
