@@ -20,7 +20,8 @@ cpu_baseline= the oracle's restatement of the reference's tiled algorithm (scipy
               OpenBLAS tile calls on all host cores) on a bounded sample.
 mixed_ir    = time-to-solution of an FP64-accurate SPD solve at the same N (rank 0, after
               the timed steps): plain FP64 Cholesky + solve against a TF32 tensor-core
-              factor + FP64 iterative refinement to normwise backward error 1e-13.
+              factor + FP64 iterative refinement to normwise backward error 1e-13; the
+              same with BF16 updates beside it (`bf16_ir`).
 
 `--impl reference` times that CPU implementation alone (rank 0; other ranks exit 0).
 Multi-GPU: the path does not shard, so `--gpus N` runs N independent replicas
@@ -421,6 +422,19 @@ def main():
                         "factor_ms": lp.get("factor_ms"), "solve_ms": lp.get("solve_ms")},
             "ratio_vs_fp64": lp.get("ratio_vs_fp64"),
         }
+        # the same solve with BF16 updates (tcgen05 kind::f16 from a BF16 copy of the panels);
+        # reported beside the TF32 one, which the ratio above keeps
+        try:
+            bf = mixed_bench.run_case(n, args.tile_chol, args.mixed_kappa, 1, args.seed,
+                                      [(mtd.PREC_BF16, mtd.REFINE_IR, 0.0)], 1e-13, 30, 2)[1]
+            mixed["bf16_ir"] = {"time_to_solution_ms": bf.get("time_to_solution_ms"),
+                                "tflops": bf.get("fp64_equiv_tflops"), "iterations": bf.get("iterations"),
+                                "backward_error": bf.get("backward_error"),
+                                "forward_error_vs_fp64": bf.get("forward_error_vs_fp64"),
+                                "factor_ms": bf.get("factor_ms"), "solve_ms": bf.get("solve_ms"),
+                                "ratio_vs_fp64": bf.get("ratio_vs_fp64")}
+        except Exception as e:  # a side report: the line above stands without it
+            mixed["bf16_ir"] = {"error": f"{type(e).__name__}: {e}"}
 
     if rank == 0:
         line = {
