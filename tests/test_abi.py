@@ -186,3 +186,32 @@ def test_custom_graph_dependencies_property(mtd):
             g.close()
 
     check()
+
+
+def test_header_is_a_c_abi(tmp_path):
+    """include/mustard_b200.h compiles as strict C99 and a C program links and calls the
+    library (no C++ in the boundary)."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lib_dir = os.path.join(root, "mustard_b200", "lib")
+    src = tmp_path / "abi.c"
+    src.write_text('#include "mustard_b200.h"\n'
+                   '#include <stdio.h>\n'
+                   'int main(void) {\n'
+                   '    const char *s = mtd_strerror(MTD_ERR_INVALID_ARG);\n'
+                   '    printf("%d %s\\n", mtd_abi_version(), s ? s : "");\n'
+                   '    return mtd_abi_version() == MTD_ABI_VERSION ? 0 : 1;\n'
+                   '}\n')
+    exe = tmp_path / "abi"
+    cc = subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror",
+                         "-I", os.path.join(root, "include"), str(src), "-o", str(exe),
+                         "-L", lib_dir, "-lmustard_b200", f"-Wl,-rpath,{lib_dir}"],
+                        capture_output=True, text=True)
+    assert cc.returncode == 0, cc.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert run.returncode == 0, run.stderr  # the library's ABI version is the header's
+    assert len(run.stdout.split()) > 1       # and mtd_strerror names the status
