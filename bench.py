@@ -16,14 +16,22 @@ e2e         = the same flop count / time of: pinned-host -> device copy of both 
 roofline    = the persistent kernel against the FP64 tensor-core (DMMA) peak measured
               live by a register-only probe (the datasheet figure, 37 TFLOP/s, is
               reported beside it).
-cpu_baseline= the oracle's restatement of the reference's tiled algorithm (scipy /
-              OpenBLAS tile calls on all host cores) on a bounded sample.
+cpu_baseline= host LAPACK dgetrf + dpotrf (scipy's OpenBLAS, all host cores) on the same
+              two N = 24000 inputs, after a small warm-up call; mean over the runs.
+parity      = the factors of one more LU and Cholesky (after the timed steps) checked on the
+              device (probe residual ||(A - LU) X|| / ||A X|| over 8 random columns) and
+              against LAPACK's factors of the same inputs (max |diff| / max |LAPACK|).
+reference_gpu (opt-in, --reference-gpu) = the reference's own 1-rank build (oracle/_ref/,
+              built from its sources by oracle/ref/Makefile) timed on the same GPU in its
+              --subgraph and single-cuSOLVER-call modes, at N = 24000.
 mixed_ir    = time-to-solution of an FP64-accurate SPD solve at the same N (rank 0, after
               the timed steps): plain FP64 Cholesky + solve against a TF32 tensor-core
               factor + FP64 iterative refinement to normwise backward error 1e-13; the
               same with BF16 updates beside it (`bf16_ir`).
 
-`--impl reference` times that CPU implementation alone (rank 0; other ranks exit 0).
+`--impl reference` times the oracle's restatement of the reference's tiled algorithm (scipy /
+OpenBLAS tile calls, all host cores) alone, on a bounded sample N = --cpu-n that its config
+states (rank 0; other ranks exit 0): the reference has no CPU implementation of its own.
 Multi-GPU: the path does not shard, so `--gpus N` runs N independent replicas
 (weak scaling), timed as the max over ranks.
 """
@@ -150,6 +158,117 @@ def cpu_cores():
         return os.cpu_count()
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def lapack_baseline(a_lu, a_ch, runs, budget_s):
+    """Host LAPACK on the benchmark's own inputs: dgetrf (partial pivoting; the LU input is
+    column diagonally dominant, so it makes no row swaps and equals the no-pivot LU -- the
+    pivots are checked) and dpotrf (lower), through scipy's OpenBLAS on all host cores.  One
+    warm-up call at n = 2048, then up to `runs` timed runs of each (fewer once `budget_s` is
+    spent), each on a fresh copy made outside the clock.  Returns the record and the last
+    run's factors."""
+    import numpy as np
+    from scipy.linalg import lapack
+    from threadpoolctl import threadpool_info, threadpool_limits
+    cores = cpu_cores()
+    n = a_lu.shape[0]
+    with threadpool_limits(cores, user_api="blas"):
+        lapack.dgetrf(np.array(a_lu[:2048, :2048], order="F"), overwrite_a=1)
+        lapack.dpotrf(np.array(a_ch[:2048, :2048], order="F"), lower=1, overwrite_a=1)
+        t_lu, t_ch = [], []
+        f_lu = f_ch = None
+        start = time.perf_counter()
+        for _ in range(max(1, runs)):
+            f_lu = f_ch = None
+            w = np.array(a_lu, order="F", copy=True)
+            t0 = time.perf_counter()
+            f_lu, piv, info = lapack.dgetrf(w, overwrite_a=1)
+            t1 = time.perf_counter()
+            if info != 0 or not np.array_equal(piv, np.arange(n)):
+                raise RuntimeError("LAPACK dgetrf pivoted or failed on the diagonally dominant input")
+            w = np.array(a_ch, order="F", copy=True)
+            t2 = time.perf_counter()
+            f_ch, info = lapack.dpotrf(w, lower=1, clean=0, overwrite_a=1)
+            t3 = time.perf_counter()
+            if info != 0:
+                raise RuntimeError(f"LAPACK dpotrf failed (info {info})")
+            t_lu.append(t1 - t0)
+            t_ch.append(t3 - t2)
+            if time.perf_counter() - start > budget_s:
+                break
+        blas = [f"{i.get('internal_api')} {i.get('version')}" for i in threadpool_info() if i.get("user_api") == "blas"]
+    mean_lu, mean_ch = sum(t_lu) / len(t_lu), sum(t_ch) / len(t_ch)
+    rec = {"value": (flops_lu(n) + flops_chol(n)) / (mean_lu + mean_ch) / 1e12, "unit": "TFLOP/s",
+           "cores": cores, "kind": "lapack", "cpu_model": cpu_model(), "blas": blas, "runs": len(t_lu),
+           "lu_s": t_lu, "chol_s": t_ch,
+           "lu_tflops": flops_lu(n) / mean_lu / 1e12, "chol_tflops": flops_chol(n) / mean_ch / 1e12,
+           "sample": (f"host LAPACK dgetrf + dpotrf at N={n} on the same inputs as the GPU steps, "
+                      f"{cores} threads, mean of {len(t_lu)} run(s) after a warm-up call at n=2048")}
+    return rec, f_lu, f_ch
+
+
+def to_host(t):
+    """Column-major CUDA matrix -> numpy array in Fortran order (same entries)."""
+    return t.t().contiguous().cpu().numpy().T
+
+
+def reference_gpu_baseline(n, timeout):
+    """The reference's own 1-rank build on this GPU (oracle/_ref/lu_mustard, cholesky_mustard):
+    its device-side scheduler (--subgraph) at T = 6 (and T = 8 for Cholesky: 120 tasks, the
+    most its scheduler's device graph launches allow) with its default and the published SM
+    limit, and its single cuSOLVER call; 4 runs each, run 0 dropped as its own scripts do."""
+    from oracle import reference_gpu as rg
+    if not rg.available():
+        return {"unavailable": "the reference's drivers are not built (oracle/ref/Makefile)"}
+    out = {"runs": []}
+    plan = [("lu", 6, "subgraph", 20), ("lu", 6, "subgraph", 100), ("lu", 1, "single", 20),
+            ("chol", 6, "subgraph", 20), ("chol", 8, "subgraph", 20), ("chol", 6, "subgraph", 100),
+            ("chol", 1, "single", 20)]
+    for kind, t, mode, sm in plan:
+        if n % t:
+            continue
+        try:
+            rec = rg.run(kind, n, t, mode, runs=4, sm=sm, timeout=timeout)
+        except Exception as e:  # a side report: the line stands without it
+            rec = {"kind": kind, "t": t, "mode": mode, "sm": sm, "error": f"{type(e).__name__}: {e}"}
+        rec.pop("tail", None) if rec.get("rc") == 0 else None
+        out["runs"].append(rec)
+    for kind in ("lu", "chol"):
+        ok = [r for r in out["runs"] if r.get("kind") == kind and r.get("tflops_mean")]
+        if ok:
+            best = max(ok, key=lambda r: r["tflops_mean"])
+            out[f"{kind}_best"] = {k: best[k] for k in ("mode", "t", "sm", "tflops_mean", "tflops_best", "mean_s")}
+            sub = [r for r in ok if r["mode"] == "subgraph"]
+            if sub:
+                bs = max(sub, key=lambda r: r["tflops_mean"])
+                out[f"{kind}_subgraph_best"] = {k: bs[k] for k in ("t", "sm", "tflops_mean", "tflops_best", "mean_s")}
+    return out
+
+
+# FP64 kernel sources whose DRAM traffic `roofline.traffic` reports; the figure comes from
+# one ncu capture and is reported only while these files still hash to the captured state.
+TRAFFIC_SOURCES = ["mustard_b200/csrc/scheduler.cuh", "mustard_b200/csrc/mma.cuh", "mustard_b200/csrc/tile_ops.cuh",
+                   "mustard_b200/csrc/device_types.hpp", "mustard_b200/csrc/dag.cpp"]
+
+
+def kernel_sources_sha16():
+    import hashlib
+    h = hashlib.sha256()
+    for rel in TRAFFIC_SOURCES:
+        with open(os.path.join(ROOT, rel), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
 def workload_config(args, world):
     """The `config` of both arms' JSON lines: the workload the metric is quoted on."""
     n = args.n
@@ -177,16 +296,26 @@ def run_reference(args, rank, world):
     value = (flops_lu(args.cpu_n) + flops_chol(args.cpu_n)) * len(times) / sum(times) / 1e12
     sample = (f"tiled LU + Cholesky, N={args.cpu_n} (tile {args.cpu_tile}) per step instead of N={args.n}: "
               f"the oracle's restatement of the reference's task list with scipy/OpenBLAS tile calls")
+    config = workload_config(args, world)
+    config.update({"workload": f"plain FP64 tiled LU + Cholesky, sampled at N={args.cpu_n} per step "
+                               f"(the metric's workload is N={args.n})",
+                   "n": args.cpu_n, "tile_lu": args.cpu_tile, "tile_chol": args.cpu_tile, "metric_n": args.n,
+                   "l2": "host run"})
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": workload_config(args, world),
+        "data": "synthetic", "config": config,
         "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
+
+# The ncu capture behind roofline.traffic (profiles/dram_traffic_bench_n24000_t1536.md):
+# DRAM read + write bytes of one step's two launches, and the hash of the FP64 kernel
+# sources it measured.
+TRAFFIC_CAPTURE = {"sources_sha16": "", "bytes": 76424422400 + 35419470336 + 39205473280 + 17637506560}
 
 METRIC = "FP64-accurate LU/Cholesky TFLOP/s, N=24000, 1 B200: mixed+IR vs plain FP64"
 
@@ -204,7 +333,13 @@ def main():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-n", type=int, default=12000)
     ap.add_argument("--cpu-tile", type=int, default=1000)
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the host LAPACK baseline")
+    ap.add_argument("--cpu-runs", type=int, default=3, help="timed host LAPACK runs (mean reported)")
+    ap.add_argument("--cpu-budget", type=float, default=60.0,
+                    help="stop the LAPACK runs once this many seconds are spent (at least one run)")
+    ap.add_argument("--no-parity", action="store_true", help="skip the parity checks after the timed steps")
+    ap.add_argument("--reference-gpu", action="store_true",
+                    help="also time the reference's own 1-rank build on this GPU (oracle/_ref)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer measurement")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision + IR comparison")
     ap.add_argument("--mixed-kappa", type=float, default=1e2)
@@ -377,12 +512,16 @@ def main():
     achieved = flops_step / (dev_ms * 1e-3) / 1e12
     # DRAM bytes (read + write) of the two launches of one step, from one ncu capture of
     # dram__bytes_read.sum / dram__bytes_write.sum (a single-pass metric pair) on exactly this
-    # workload: profiles/dram_traffic_bench_n24000_t1536.md.  Other workloads report null.
+    # workload: profiles/dram_traffic_bench_n24000_t1536.md.  Reported only for this workload
+    # and while the FP64 kernel's sources hash to the state that capture measured.
     measured = n == 24000 and args.tile_lu == 1536 and args.tile_chol == 1536 and args.only is None
-    traffic = (76424422400 + 35419470336 + 39205473280 + 17637506560) if measured else None
+    sources_sha = kernel_sources_sha16()
+    traffic = (TRAFFIC_CAPTURE["bytes"] if measured and sources_sha == TRAFFIC_CAPTURE["sources_sha16"] else None)
     roofline = {
         "bound": "tensor", "achieved": achieved, "peak": peak_meas, "unit": "TFLOP/s",
         "frac": achieved / peak_meas if peak_meas else None, "traffic": traffic,
+        "traffic_source": (f"ncu capture of this workload, kernel sources {TRAFFIC_CAPTURE['sources_sha16']}"
+                           if traffic else f"none for kernel sources {sources_sha}"),
         "traffic_unit": "bytes per step (LU launch + Cholesky launch)",
         "traffic_bytes_per_flop": traffic / flops_step if traffic else None,
         "kernel": "mtd::persistent_kernel<2> (scheduler + all FP64 tile operations)",
@@ -392,14 +531,40 @@ def main():
         "chol_tflops": flops_chol(n) / (t_ch / args.steps * 1e-3) / 1e12 if args.only != "lu" else None,
     }
 
+    # --- parity of the measured workload (rank 0, after the timed steps) -------------
+    # One more LU and Cholesky of the same inputs: the device probe residual of each, and
+    # (with the host LAPACK baseline below) the factors against LAPACK's.
+    parity, h_f = None, {}
+    if rank == 0 and not args.no_parity and args.only is None:
+        from mustard_b200 import verify
+        parity = {"workload": f"the timed inputs, N={n}, tiles {args.tile_lu}/{args.tile_chol}",
+                  "probe": "||(A - LU) X||_F / ||A X||_F, 8 random columns, FP64 on the device"}
+        for kind, g, src in (("lu", g_lu, src_lu), ("chol", g_ch, src_ch)):
+            work.copy_(src)
+            g.run(work, stream=stream)  # synchronous: raises on a failed run
+            parity[f"{kind}_resid"] = verify.probe_residual(src, work, kind)
+            h_f[kind] = to_host(work)
+        parity["bar"] = "resid <= 1e-15; factors within 1e-12 (max |diff| / max |LAPACK|) of LAPACK's"
+
     cpu = None
-    if rank == 0 and not args.no_cpu:
-        os.environ.setdefault("OPENBLAS_NUM_THREADS", str(cpu_cores()))
-        v, tlu, tch, _ = cpu_sample(args.cpu_n, args.cpu_tile, args.seed)
-        cpu = {"value": v, "unit": "TFLOP/s", "cores": cpu_cores(), "kind": "port",
-               "sample": (f"tiled LU + Cholesky at N={args.cpu_n}, tile {args.cpu_tile} "
-                          f"({tlu:.1f} s + {tch:.1f} s): the oracle's restatement of the reference's "
-                          "task list with scipy/OpenBLAS tile calls, all host cores")}
+    if rank == 0 and not args.no_cpu and args.only is None:
+        import numpy as np
+        h_lu, h_ch = to_host(src_lu), to_host(src_ch)
+        cpu, lap_lu, lap_ch = lapack_baseline(h_lu, h_ch, args.cpu_runs, args.cpu_budget)
+        del h_lu, h_ch
+        if parity is not None:
+            from mustard_b200 import verify
+
+            def rel(x, y):
+                return float(np.abs(x - y).max() / np.abs(y).max())
+
+            parity["lu_rel_vs_lapack"] = rel(h_f["lu"], lap_lu)
+            parity["chol_rel_vs_lapack"] = rel(np.tril(h_f["chol"]), np.tril(lap_ch))
+            for kind, lap, src in (("lu", lap_lu, src_lu), ("chol", lap_ch, src_ch)):
+                work.copy_(torch.from_numpy(np.ascontiguousarray(lap.T)).to(dev).t())
+                parity[f"lapack_{kind}_resid"] = verify.probe_residual(src, work, kind)
+        del lap_lu, lap_ch
+    h_f.clear()
 
     # FP64-accurate solve of A x = b at the same N: plain FP64 Cholesky + one solve against a
     # TF32 factor + FP64 iterative refinement to backward error 1e-13 (wall time with the
@@ -436,17 +601,25 @@ def main():
         except Exception as e:  # a side report: the line above stands without it
             mixed["bf16_ir"] = {"error": f"{type(e).__name__}: {e}"}
 
+    ref_gpu = None
+    if rank == 0 and args.reference_gpu:
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()  # the reference's process needs its own device memory
+        ref_gpu = reference_gpu_baseline(n, timeout=300)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(args, world),
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "mixed_ir": mixed,
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "mixed_ir": mixed,
             "clocks": clocks.summary(),
             "gpu_launches": args.steps * (1 if args.only else 2) * launches_per_run,
             "wall_s_timed": wall1 - wall0,
         }
+        if ref_gpu is not None:
+            line["reference_gpu"] = ref_gpu
         if args.trace:
             line["scheduler"] = {"lu": stats_lu, "chol": stats_ch}
         print(json.dumps(line), flush=True)

@@ -113,7 +113,8 @@ int mtd_graph_create(mtd_graph **out, int kind, int64_t n, int64_t tile);
 int mtd_graph_add_task(mtd_graph *g, int op, int wi, int wj, const int *reads, int nreads);
 
 /* Emit the reference's whole task list for the graph's kind, in its loop order
- * (cholesky_mustard.cu:224-395 or lu_mustard.cu:345-533). */
+ * (cholesky_mustard.cu:224-395 or lu_mustard.cu:345-533).  MTD_ERR_INVALID_ARG when the
+ * list would exceed 2^25 tasks (the count is cubic in the tile count). */
 int mtd_graph_build_tiled(mtd_graph *g);
 
 /* Number of tasks recorded so far. */
@@ -205,11 +206,10 @@ int mtd_tiled_lu(double *dA, int64_t n, int64_t lda, int64_t tile, void *stream,
  *
  * No counterpart in the reference.  Every other entry point gets its task table, ready
  * queues, counters and inverse workspace from cudaMalloc.  Some callers cannot do that:
- * code that runs while a stream is being captured into a CUDA graph (a cudaMalloc there
- * breaks the capture), applications whose device memory is owned entirely by a pool
- * allocator (PyTorch's caching allocator, RAPIDS RMM) that must not see raw allocations,
- * and latency-critical services that cannot afford an allocation, or its failure, on the
- * request path.  This entry point serves them: it runs the same tiled LU (kind
+ * applications whose device memory is owned entirely by a pool allocator (PyTorch's
+ * caching allocator, RAPIDS RMM) that must not see raw allocations, and latency-critical
+ * services that cannot afford an allocation, or its failure, on the request path.  This
+ * entry point serves them: it runs the same tiled LU (kind
  * MTD_KIND_LU) or Cholesky (MTD_KIND_CHOLESKY) as mtd_tiled_lu / mtd_tiled_cholesky, but
  * all of its device scratch lives in one fixed, file-scope device array of 24 MiB inside
  * this library (every GPU that loads the library holds it until the process exits).  It
@@ -217,13 +217,16 @@ int mtd_tiled_lu(double *dA, int64_t n, int64_t lda, int64_t tile, void *stream,
  * list is assembled in ordinary host memory and copied into the array.
  *
  * Limits: n <= 16384 and, for the chosen tile, at most 32768 device tasks, 131072
- * dependency edges and 262144 work items; larger problems return MTD_ERR_TOO_LARGE.
+ * dependency edges and 262144 work items; larger problems return MTD_ERR_TOO_LARGE (a tile
+ * so small that the task list alone is too long is rejected before the list is built).
  * The first call on a device looks up the array's device address (and sets the kernel's
- * shared-memory limit); make that first call before any stream capture.
+ * shared-memory limit).
  * All calls share the one array: calls whose work overlaps on the GPU (different streams,
  * host threads, or graphs) race and corrupt each other's results; serialise them.  The
- * call waits for its stream and returns the run's status; info_out (may be NULL)
- * receives LAPACK-style info as with mtd_run. */
+ * call copies the task list from ordinary (pageable) host memory into the array, waits
+ * for its stream and returns the run's status, so it cannot be called while its stream
+ * is being captured into a CUDA graph; info_out (may be NULL) receives LAPACK-style info
+ * as with mtd_run. */
 int mtd_factor_noalloc(int kind, double *dA, int64_t n, int64_t lda, int64_t tile, void *stream,
                        int *info_out);
 

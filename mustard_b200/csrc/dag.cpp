@@ -103,8 +103,17 @@ int Dag::add_task(int op, int wi, int wj, const int *reads, int nreads) {
     return idx;
 }
 
+int64_t Dag::reference_task_count(int kind, int64_t T) {
+    // Cholesky: per step with m = T-k-1 trailing tiles, m TRSM + m SYRK + m(m-1)/2 GEMM;
+    // LU: m TRSM-L + m TRSM-R + m^2 GEMM; plus one diagonal factorisation per step.
+    int64_t total = T;
+    for (int64_t m = 0; m < T; ++m) total += kind == MTD_KIND_CHOLESKY ? 2 * m + m * (m - 1) / 2 : 2 * m + m * m;
+    return total;
+}
+
 int Dag::build_reference_order() {
     const int T = tiles_;
+    if (reference_task_count(kind_, T) > kMaxReferenceTasks) return MTD_ERR_INVALID_ARG;
     auto add = [&](int op, int wi, int wj, std::initializer_list<int> r) {
         std::vector<int> v(r);
         int rc = add_task(op, wi, wj, v.data(), static_cast<int>(v.size() / 2));
@@ -151,9 +160,7 @@ int items_of(const DevTask &t) {
         return static_cast<int>(ceil_div(t.m, kPanelRows));
     case MTD_OP_TRSM_LLNU:
         return static_cast<int>(ceil_div(t.n, kPanelRows));
-    case kOpJoin:
-        return 0;
-    default:
+    default:  // diagonal factorisations, and a join's one no-op item
         return 1;
     }
 }

@@ -44,7 +44,13 @@ public:
 
     // Returns the new task index, or a negative mtd_status.
     int add_task(int op, int wi, int wj, const int *reads, int nreads);
+    // The reference's whole task list for this kind; MTD_ERR_INVALID_ARG when it would
+    // exceed kMaxReferenceTasks (checked in closed form before anything is built).
     int build_reference_order();
+    // Tasks of the reference's list for `kind` over T x T tiles (cholesky_mustard.cu:200-204,
+    // lu_mustard.cu:322-326), in 64 bits.
+    static int64_t reference_task_count(int kind, int64_t T);
+    static constexpr int64_t kMaxReferenceTasks = int64_t(1) << 25;
 
     int num_tasks() const { return static_cast<int>(tasks_.size()); }
     const std::vector<int> &deps(int t) const { return deps_[t]; }

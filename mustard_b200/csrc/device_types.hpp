@@ -18,7 +18,7 @@ constexpr int kPanelRows = 64;  // rows (or columns) of one TRSM work item
 constexpr int kNB = 64;         // diagonal block edge inside POTRF / GETRF (and inverse blocks)
 constexpr int kNestTile = 128;  // default sub-tile edge of a nested diagonal factorisation
 
-// Device-side operation codes: the public mtd_op values plus a zero-work join.
+// Device-side operation codes: the public mtd_op values plus a join (one no-op work item).
 constexpr int kOpJoin = 100;
 
 // Cholesky adjoint operations (device tasks of the reverse sweep; see adjoint_ops.cuh).
@@ -47,7 +47,7 @@ constexpr bool is_adjoint_op(int op) { return op >= kOpAdjTrsm && op <= kOpAdjPo
 struct alignas(16) DevTask {
     int32_t op;
     int32_t queue;       // ready queue, 0 .. kNumQueues - 1
-    int32_t n_items;     // 0 for a join
+    int32_t n_items;     // >= 1 (a join has one no-op item)
     int32_t cr, cc;      // output block origin
     int32_t ar, ac;      // first operand (triangular block for TRSM)
     int32_t br, bc;      // second operand (GEMM)

@@ -105,9 +105,11 @@ int smem_setup(int device) {
     return MTD_OK;
 }
 
-// Leading dimension of the inverse workspace: N rounded up to a multiple of 4 so every
-// 64-column block starts on a 16-byte boundary for either element size.
-int64_t ws_ld(const mtd_graph *g) { return (g->dag.n() + 3) & ~int64_t(3); }
+// Leading dimension of the inverse workspace of an n x n factorisation: n rounded up to a
+// multiple of 4 so every 64-column block starts on a 16-byte boundary for either element
+// size.  Every entry point that lays out a workspace uses this one rule.
+int64_t ws_ld_for(int64_t n) { return (n + 3) & ~int64_t(3); }
+int64_t ws_ld(const mtd_graph *g) { return ws_ld_for(g->dag.n()); }
 
 size_t elem_size(const mtd_graph *g) { return g->prec == MTD_PREC_FP64 ? sizeof(double) : sizeof(float); }
 
@@ -751,6 +753,10 @@ extern "C" int mtd_factor_noalloc(int kind, double *dA, int64_t n, int64_t lda, 
     if (kind != MTD_KIND_LU && kind != MTD_KIND_CHOLESKY) return MTD_ERR_INVALID_ARG;
     if (!dA || n <= 0 || tile <= 0 || tile > n || lda < n) return MTD_ERR_INVALID_ARG;
     if (n > kNoAllocMaxN) return MTD_ERR_TOO_LARGE;
+    // Every host task becomes at least one device task: reject a tile so small that the
+    // task list alone exceeds the task table before building anything (the count is cubic
+    // in the tile count).
+    if (Dag::reference_task_count(kind, (n + tile - 1) / tile) > kNoAllocMaxTasks) return MTD_ERR_TOO_LARGE;
 
     // The task graph: host memory only.
     Dag dag(kind, n, tile);
@@ -779,7 +785,7 @@ extern "C" int mtd_factor_noalloc(int kind, double *dA, int64_t n, int64_t lda, 
     rc = noalloc_scratch(device, &scratch);
     if (rc) return rc;
 
-    const int64_t wld = n + (n & 1);
+    const int64_t wld = ws_ld_for(n);
     ScratchCarver sc{scratch};
     RunArgs a{};
     DevTask *d_tasks = sc.take<DevTask>(nt);

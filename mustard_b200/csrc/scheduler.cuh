@@ -50,44 +50,22 @@ __device__ __forceinline__ long long add_avail(long long *c, long long v) {
         atomicAdd(reinterpret_cast<unsigned long long *>(c), static_cast<unsigned long long>(v)));
 }
 
-// One thread of a CTA: `task` has no predecessors left.  Push every work item of it; a
-// join (no work items) completes on the spot, releasing its own successors.
+// One thread of a CTA: `task` has no predecessors left.  Push its work items.  Every task
+// has at least one: a join (the stand-in of a nested factorisation with several sinks) has
+// one no-op item, so a release never recurses and a chain of joins needs no stack.
 __device__ __forceinline__ void release_task(const RunArgs &p, int task) {
-    int stack[8];
-    int top = 0;
-    stack[top++] = task;
-    while (top > 0) {
-        const int tk = stack[--top];
-        const int q = __ldg(&p.tasks[tk].queue);
-        const int n_items = __ldg(&p.tasks[tk].n_items);
-        if (n_items > 0) {
-            const unsigned long long n = static_cast<unsigned long long>(n_items);
-            const unsigned long long base = atomicAdd(&p.qctl[q].tail, n);
-            if (base + n > static_cast<unsigned long long>(p.queue_cap[q])) {
-                report_error(p.ctl, MTD_ERR_QUEUE, 0);
-                return;
-            }
-            volatile unsigned long long *slots = p.queue[q];
-            for (unsigned long long i = 0; i < n; ++i)
-                slots[base + i] = (static_cast<unsigned long long>(tk) << 32) | i;
-            __threadfence();  // the slots before the count that lets consumers claim them
-            add_avail(&p.qctl[q].avail, static_cast<long long>(n));
-            continue;
-        }
-        const int sb = __ldg(&p.tasks[tk].succ_begin), sc = __ldg(&p.tasks[tk].succ_count);
-        for (int s = 0; s < sc; ++s) {
-            const int succ = __ldg(&p.succ[sb + s]);
-            if (atomicSub(&p.deps[succ], 1) == 1) {
-                if (top == 8) {
-                    report_error(p.ctl, MTD_ERR_QUEUE, 0);
-                    return;
-                }
-                stack[top++] = succ;
-            }
-        }
-        __threadfence();
-        atomicAdd(&p.ctl->tasks_done, 1);
+    const int q = __ldg(&p.tasks[task].queue);
+    const int n_items = __ldg(&p.tasks[task].n_items);
+    const unsigned long long n = static_cast<unsigned long long>(n_items);
+    const unsigned long long base = atomicAdd(&p.qctl[q].tail, n);
+    if (n_items <= 0 || base + n > static_cast<unsigned long long>(p.queue_cap[q])) {
+        report_error(p.ctl, MTD_ERR_QUEUE, 0);
+        return;
     }
+    volatile unsigned long long *slots = p.queue[q];
+    for (unsigned long long i = 0; i < n; ++i) slots[base + i] = (static_cast<unsigned long long>(task) << 32) | i;
+    __threadfence();  // the slots before the count that lets consumers claim them
+    add_avail(&p.qctl[q].avail, static_cast<long long>(n));
 }
 
 // One thread of a CTA: one attempt to claim a work item.  The exit flags and every queue's
@@ -263,6 +241,7 @@ __device__ __forceinline__ int op_update_tc(const RunArgs &p, const MatCtx &m, c
 template <int VEC, typename T, int SPLIT = 1, bool ADJ = false>
 __device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int item, void *smem,
                                         tc::State *tcs = nullptr) {
+    if (t.op == kOpJoin) return 0;  // a join's one item: nothing to compute
     if constexpr (ADJ) return dispatch_adjoint<T, VEC, SPLIT>(p, t, item, smem);
     const MatCtx m = mat_ctx<T>(p, t);
     if constexpr (uses_tcgen05<VEC, T, SPLIT, ADJ>())

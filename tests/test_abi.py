@@ -108,6 +108,34 @@ def test_invalid_graph_arguments(mtd):
     assert e.value.status == 2
 
 
+def test_oversized_task_lists_rejected_before_they_are_built(mtd):
+    """The reference's task count is cubic in the tile count: a list past 2^25 tasks is
+    refused from the closed form, before anything is built (40960 / 10 -> 4096 tiles,
+    ~2.3e10 tasks), and the no-allocation entry point refuses a list longer than its task
+    table the same way, before any device work (the pointer is never dereferenced)."""
+    import time
+    for kind in (mtd.KIND_LU, mtd.KIND_CHOLESKY):
+        g = mtd.TaskGraph(kind, 40960, 10)
+        t0 = time.perf_counter()
+        with pytest.raises(mtd.MtdError) as e:
+            g.build_tiled()
+        assert e.value.status == 1 and time.perf_counter() - t0 < 1.0
+        g.close()
+    info = ctypes.c_int(-1)
+    t0 = time.perf_counter()
+    rc = mtd.lib().mtd_factor_noalloc(mtd.KIND_LU, ctypes.c_void_p(0x1000), 16000, 16000, 8, None,
+                                      ctypes.byref(info))
+    assert rc == 11 and info.value == 0 and time.perf_counter() - t0 < 1.0
+    # the closed form agrees with the oracle's count of the reference's loops
+    for t in (1, 2, 6, 8, 47):
+        g = mtd.TaskGraph(mtd.KIND_CHOLESKY, 64 * t, 64).build_tiled()
+        assert g.num_tasks == tiled.cholesky_task_count(t)
+        g.close()
+        g = mtd.TaskGraph(mtd.KIND_LU, 64 * t, 64).build_tiled()
+        assert g.num_tasks == tiled.lu_task_count(t)
+        g.close()
+
+
 def test_finalize_without_gpu_reports_no_device(mtd):
     import torch
     if torch.cuda.is_available():

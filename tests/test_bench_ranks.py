@@ -73,8 +73,9 @@ def test_reference_arm_line_and_other_ranks():
     (line,) = _reference_arm({"RANK": "0", "WORLD_SIZE": "1"})
     assert line["impl"] == "reference" and line["metric"] == bench.METRIC and line["unit"] == "TFLOP/s"
     assert line["higher_is_better"] is True and line["value"] > 0
-    # the workload of the measured arm; the CPU sample is described in cpu_baseline
-    assert line["config"]["workload"] == "plain FP64 tiled LU + Cholesky, N=24000"
+    # the config states the sample it ran and the metric's workload size
+    cfg = line["config"]
+    assert cfg["n"] == 600 and cfg["metric_n"] == 24000 and "sampled at N=600" in cfg["workload"]
     cb = line["cpu_baseline"]
     assert cb["kind"] == "port" and cb["value"] == line["value"] and cb["cores"] >= 1 and "N=600" in cb["sample"]
     assert line["e2e"] == {"value": line["value"], "unit": "TFLOP/s", "h2d_bytes_per_step": 0,

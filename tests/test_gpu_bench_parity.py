@@ -1,0 +1,62 @@
+"""Parity at the configuration the headline number is quoted on: FP64 tiled LU of
+U[-1,1) + N I and tiled Cholesky of B B^T / N + I at N = 24000, tile 1536 (15 full tiles and
+a 960-wide ragged one), on the benchmark's own seeded device inputs.
+
+Checked, per factorisation:
+  - the device probe residual ||(A - L U) X|| / ||A X|| over 8 random columns, and the
+    same for LAPACK's factor of the same input (host, all cores): ours within 25 % of
+    LAPACK's and below 1e-15;
+  - the whole factor against LAPACK's (dpotrf; dgetrf with an identity-pivot assertion,
+    the input being column diagonally dominant) within the FP64 bar of 1e-12 relative
+    (max |diff| / max |LAPACK|);
+  - Cholesky: the strict upper triangle is the input's, bit for bit.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import tiled
+from tests.gpu_util import device_probe_residual, from_dev, rel_diff
+
+pytestmark = pytest.mark.gpu
+N, TILE, SEED = 24000, 1536, 2024  # bench.py's defaults
+
+
+def _host_probe(a, f, kind):
+    import torch
+    return device_probe_residual(torch.from_numpy(np.ascontiguousarray(a.T)).cuda().t(),
+                                 torch.from_numpy(np.ascontiguousarray(f.T)).cuda().t(), kind)
+
+
+@pytest.mark.parametrize("kind", ["lu", "chol"])
+def test_bench_workload_parity_n24000(mtd, kind):
+    import torch
+    from scipy.linalg import lapack
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", str(len(os.sched_getaffinity(0))))
+    src = mtd.colmajor(torch.empty((N, N), dtype=torch.float64, device="cuda"))
+    if kind == "lu":
+        mtd.generate(src, mtd.GEN_UNIFORM_DIAG, seed=SEED)
+    else:
+        mtd.generate(src, mtd.GEN_SPD, seed=SEED, alpha=1.0)
+    work = src.clone(memory_format=torch.preserve_format)
+    assert work.stride() == src.stride()
+    g = mtd.TaskGraph(mtd.KIND_LU if kind == "lu" else mtd.KIND_CHOLESKY, N, TILE).build_tiled().finalize()
+    assert g.run(work) == 0
+    g.close()
+    ours_resid = device_probe_residual(src, work, kind)
+    a = from_dev(src)
+    ours = from_dev(work)
+    del src, work
+    torch.cuda.empty_cache()
+    if kind == "lu":
+        ref = tiled.lu_nopiv_lapack(a)  # asserts identity pivots
+    else:
+        ref, info = lapack.dpotrf(a, lower=1, clean=0, overwrite_a=0)
+        assert info == 0
+        assert np.array_equal(np.triu(ours, 1), np.triu(a, 1))
+        ours, ref = np.tril(ours), np.tril(ref)
+    rel = rel_diff(ours, ref)
+    assert rel <= 1e-12, rel
+    lapack_resid = _host_probe(a, ref, kind)
+    assert ours_resid <= 1e-15 and ours_resid <= 1.25 * lapack_resid, (ours_resid, lapack_resid)

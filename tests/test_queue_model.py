@@ -9,8 +9,9 @@ operation, so a random scheduler explores interleavings the GPU may produce:
 - run the item, then complete it (complete_item): decrement the task's items-left counter;
   the last item decrements each successor's predecessor counter, and a successor that
   reaches zero is pushed (release_task): fetch-and-add on `tail`, write the slots, then
-  fetch-and-add their number on `avail`.  A task without items (a join) completes on the
-  spot and releases its own successors.
+  fetch-and-add their number on `avail`.  Every task has at least one item: a join (the
+  stand-in of a nested factorisation with several sinks) has one no-op item, so a release
+  never recurses.
 
 The tcgen05 kernel's variant (`deferred`): a GEMM / SYRK item is completed only during the
 CTA's next claim, the completion and the claim interleaving step by step.
@@ -36,7 +37,8 @@ class Queue:
 
 class Model:
     def __init__(self, n_items, succ, deps, queue_of, n_queues):
-        self.n_items = n_items                 # per task (0: a join)
+        assert all(n >= 1 for n in n_items)    # a join is one no-op item
+        self.n_items = n_items                 # per task
         self.succ = succ
         self.deps = list(deps)                 # predecessor counters
         self.items_left = list(n_items)
@@ -51,33 +53,18 @@ class Model:
         self.runs = []                         # (task, item) in execution order
         self.started = {}
 
-    # release_task: a stack of tasks whose counters reached zero (joins complete on the spot)
+    # release_task: reserve slots on `tail`, write them, then publish them on `avail`
     def release(self, task):
-        stack = [task]
-        while stack:
-            tk = stack.pop()
-            n = self.n_items[tk]
-            if n > 0:
-                q = self.queues[self.queue_of[tk]]
-                base = q.tail
-                q.tail += n
-                yield
-                for i in range(n):
-                    q.slots[base + i] = (tk, i)
-                    yield
-                q.avail += n                   # after the slots (the device fences in between)
-                yield
-                continue
-            self.data_done.add(tk)             # a join: nothing to run
-            for s in self.succ[tk]:
-                self.deps[s] -= 1
-                left = self.deps[s]
-                yield
-                if left == 0:
-                    stack.append(s)
-            self.done_tasks.add(tk)
-            self.tasks_done += 1
+        n = self.n_items[task]
+        q = self.queues[self.queue_of[task]]
+        base = q.tail
+        q.tail += n
+        yield
+        for i in range(n):
+            q.slots[base + i] = (task, i)
             yield
+        q.avail += n                           # after the slots (the device fences in between)
+        yield
 
     def complete(self, task):
         self.items_left[task] -= 1
@@ -225,8 +212,8 @@ def run_model(tasks, preds, succ, n_items, n_ctas, seed, deferred=False, max_ste
 def test_cholesky_dag_runs_each_item_once_in_dependency_order(t, n_ctas, seed, deferred):
     tasks, preds, succ = cholesky_dag(t)
     rng = random.Random(seed)
-    # a few items per task, and some joins (no items) like the nested factorisations' joins
-    n_items = [0 if (idx % 7 == 3 and preds[idx]) else rng.randint(1, 3) for idx in range(len(tasks))]
+    # a few items per task (a join's single no-op item is one of them)
+    n_items = [1 if (idx % 7 == 3 and preds[idx]) else rng.randint(1, 3) for idx in range(len(tasks))]
     m = run_model(tasks, preds, succ, n_items, n_ctas, seed, deferred=deferred)
     want = sorted((tk, i) for tk, n in enumerate(n_items) for i in range(n))
     assert sorted(m.runs) == want                       # every item exactly once

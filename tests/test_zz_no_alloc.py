@@ -1,14 +1,15 @@
 """mtd_factor_noalloc: the factorisation entry point for callers that cannot allocate
 device memory.
 
-Callers that run while a stream is being captured into a CUDA graph, callers whose device
-memory belongs entirely to a pool allocator (PyTorch's caching allocator, RMM), and
-latency-critical request paths cannot call cudaMalloc.  mtd_factor_noalloc keeps all of
-its device scratch in one fixed 24 MiB array inside the library instead.  These tests call
+Callers whose device memory belongs entirely to a pool allocator (PyTorch's caching
+allocator, RMM) and latency-critical request paths cannot call cudaMalloc.
+mtd_factor_noalloc keeps all of its device scratch in one fixed 24 MiB array inside the
+library instead.  These tests call
 it through the C ABI and check that it gives what the allocating entry points
 (mtd_tiled_cholesky / mtd_tiled_lu) give, within the FP64 parity tolerance of the other
 tests, on consecutive calls that reuse the same array -- including a call after a larger
-problem of the other kind left its own contents there.  This file runs last in the
+problem of the other kind left its own contents there -- and that a warm call leaves the
+device's free memory exactly as it found it.  This file runs last in the
 suite (pytest orders files by name), after every other test has run.
 """
 import ctypes
@@ -85,6 +86,27 @@ def test_noalloc_rejects_problems_beyond_its_scratch(mtd):
                                 ctypes.byref(info))
     assert rc == 11
     assert b"scratch" in lib.mtd_strerror(rc)
+    # a tiny tile (2000 x 2000 tiles, ~2.7e9 tasks) is rejected from the closed-form task
+    # count, before any task list is built
+    import time
+    t0 = time.perf_counter()
+    rc = lib.mtd_factor_noalloc(mtd.KIND_LU, ctypes.c_void_p(d.data_ptr()), 16000, 16000, 8, None,
+                                ctypes.byref(info))
+    assert rc == 11 and time.perf_counter() - t0 < 1.0
+
+
+def test_noalloc_allocates_no_device_memory(mtd):
+    import torch
+    a = gen.spd_input(2048, 5)
+    d1, d2 = to_dev(a), to_dev(a)
+    assert _noalloc(mtd, mtd.KIND_CHOLESKY, d1, 512) == (0, 0)  # warm: per-device set-up done
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    assert _noalloc(mtd, mtd.KIND_CHOLESKY, d2, 512) == (0, 0)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert np.array_equal(from_dev(d1), from_dev(d2))
 
 
 def test_noalloc_reports_non_spd_info(mtd):
