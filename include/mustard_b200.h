@@ -124,6 +124,13 @@ int mtd_graph_num_tasks(const mtd_graph *g);
  * mustard/mustard.h:137) into out[0..cap); returns the full count or a negative status. */
 int mtd_graph_get_deps(const mtd_graph *g, int task, int *out, int cap);
 
+/* Task `task` as recorded: its operation (mtd_op), the tile it writes, and up to `cap` of
+ * the tiles it reads as (row, col) pairs in reads_out[0..2*cap) -- the arguments of the
+ * reference's beginCaptureOperation (mustard/mustard.h:148-167).  Returns the number of
+ * tiles read or a negative status.  Used to plan how a graph's tasks and tiles are spread
+ * over several GPUs (mustard_b200/distribution.py). */
+int mtd_graph_task_info(const mtd_graph *g, int task, int *op_out, int *wi_out, int *wj_out, int *reads_out, int cap);
+
 /* Number of device tasks after mtd_graph_finalize: the host tasks, with every nested
  * diagonal factorisation counted as its sub-tasks (0 before finalize). */
 int mtd_graph_num_device_tasks(const mtd_graph *g);

@@ -117,6 +117,15 @@ class TaskGraph:
         self._lib.mtd_graph_get_deps(self._h, task, buf, cnt)
         return list(buf[:cnt])
 
+    def task_info(self, task):
+        """(op, write tile, read tiles) of host task ``task``, as it was recorded."""
+        op, wi, wj = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        buf = (ctypes.c_int * 16)()
+        nr = self._lib.mtd_graph_task_info(self._h, task, ctypes.byref(op), ctypes.byref(wi), ctypes.byref(wj), buf, 8)
+        if nr < 0:
+            raise MtdError(-nr)
+        return op.value, (wi.value, wj.value), [(buf[2 * r], buf[2 * r + 1]) for r in range(nr)]
+
     def items(self, task):
         return self._lib.mtd_graph_task_items(self._h, task)
 

@@ -78,6 +78,8 @@ SIGNATURES = {
     "mtd_graph_build_tiled": (_i, [_vp]),
     "mtd_graph_num_tasks": (_i, [_vp]),
     "mtd_graph_get_deps": (_i, [_vp, _i, ctypes.POINTER(_i), _i]),
+    "mtd_graph_task_info": (_i, [_vp, _i, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i),
+                                 ctypes.POINTER(_i), _i]),
     "mtd_graph_task_items": (_i, [_vp, _i]),
     "mtd_graph_device_task_op": (_i, [_vp, _i]),
     "mtd_graph_device_task_deps": (_i, [_vp, _i, ctypes.POINTER(ctypes.c_int), _i]),

@@ -303,6 +303,21 @@ int mtd_graph_get_deps(const mtd_graph *g, int task, int *out, int cap) {
     return static_cast<int>(d.size());
 }
 
+int mtd_graph_task_info(const mtd_graph *g, int task, int *op_out, int *wi_out, int *wj_out, int *reads_out,
+                        int cap) {
+    if (!g || task < 0 || task >= g->dag.num_tasks() || cap < 0 || (cap > 0 && !reads_out)) return -MTD_ERR_INVALID_ARG;
+    const HostTask &t = g->dag.task(task);
+    if (op_out) *op_out = t.op;
+    if (wi_out) *wi_out = t.write.first;
+    if (wj_out) *wj_out = t.write.second;
+    const int nr = static_cast<int>(t.reads.size());
+    for (int r = 0; r < nr && r < cap; ++r) {
+        reads_out[2 * r] = t.reads[r].first;
+        reads_out[2 * r + 1] = t.reads[r].second;
+    }
+    return nr;
+}
+
 int mtd_graph_num_device_tasks(const mtd_graph *g) { return g ? (g->finalized ? g->n_dev : 0) : -MTD_ERR_INVALID_ARG; }
 
 int mtd_graph_task_items(const mtd_graph *g, int task) {
