@@ -544,7 +544,8 @@ def main():
             g.run(work, stream=stream)  # synchronous: raises on a failed run
             parity[f"{kind}_resid"] = verify.probe_residual(src, work, kind)
             h_f[kind] = to_host(work)
-        parity["bar"] = "resid <= 1e-15; factors within 1e-12 (max |diff| / max |LAPACK|) of LAPACK's"
+        parity["bar"] = ("resid within 25 % of LAPACK's on the same input and <= 1e-14; factors within 1e-12 "
+                         "(max |diff| / max |LAPACK|) of LAPACK's")
 
     cpu = None
     if rank == 0 and not args.no_cpu and args.only is None:

@@ -5,7 +5,7 @@ a 960-wide ragged one), on the benchmark's own seeded device inputs.
 Checked, per factorisation:
   - the device probe residual ||(A - L U) X|| / ||A X|| over 8 random columns, and the
     same for LAPACK's factor of the same input (host, all cores): ours within 25 % of
-    LAPACK's and below 1e-15;
+    LAPACK's (both grow like sqrt(N) u: about 3e-15 for LU at this N) and below 1e-14;
   - the whole factor against LAPACK's (dpotrf; dgetrf with an identity-pivot assertion,
     the input being column diagonally dominant) within the FP64 bar of 1e-12 relative
     (max |diff| / max |LAPACK|);
@@ -59,4 +59,4 @@ def test_bench_workload_parity_n24000(mtd, kind):
     rel = rel_diff(ours, ref)
     assert rel <= 1e-12, rel
     lapack_resid = _host_probe(a, ref, kind)
-    assert ours_resid <= 1e-15 and ours_resid <= 1.25 * lapack_resid, (ours_resid, lapack_resid)
+    assert ours_resid <= 1e-14 and ours_resid <= 1.25 * lapack_resid, (ours_resid, lapack_resid)
