@@ -127,6 +127,13 @@ struct RunArgs {
     int64_t bf16_ld;
     int tma_bf16;
     alignas(64) unsigned char tmap_bf16[128];
+    // FP64 single-matrix runs: TMA tensor maps of the matrix for the GEMM / SYRK items
+    // (tma64.cuh) when tma64 != 0: a 3D map {16 rows of an atom, columns, atoms}, box
+    // {16, 16, 8}, for m- and n-contiguous operands, and a 2D map {rows, columns}, box
+    // {16, 128}, for the k-contiguous operand of GEMM_NN; both with the 128-byte swizzle.
+    int tma64;
+    alignas(64) unsigned char tmap64_mn[128];
+    alignas(64) unsigned char tmap64_k[128];
 };
 
 }  // namespace mtd

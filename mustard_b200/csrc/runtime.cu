@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -36,6 +37,9 @@ struct mtd_graph {
     bool trace = false;
     double timeout_s = 10.0;
     int nest = kNestTile;
+    // FP64 GEMM / SYRK items fed by TMA when the geometry allows; the environment variable
+    // MTD_TMA64=0, read when the graph is finalised, keeps them on the cp.async engine
+    bool use_tma64 = true;
     int prec = MTD_PREC_FP64;  // element type of the matrix runs factor
     unsigned short *d_bf16 = nullptr;  // MTD_PREC_BF16: BF16 copy of the panels (bf16_ld x n)
     int64_t bf16_ld = 0;
@@ -368,6 +372,10 @@ int mtd_graph_finalize(mtd_graph *g) {
 
     rc = g->dag.lower(g->nest, g->low);
     if (rc) return rc;
+    {
+        const char *e = std::getenv("MTD_TMA64");
+        g->use_tma64 = !(e && e[0] == '0');
+    }
     const std::vector<DevTask> &tasks = g->low.tasks;
     const std::vector<int> &succ = g->low.succ;
     const int64_t *cap = g->low.queue_cap;
@@ -520,6 +528,37 @@ void encode_tmap_bf16(RunArgs &a, void *d16, int64_t n, int64_t ld) {
     a.tma_bf16 = 1;
 }
 
+// TMA tensor maps of an FP64 n x n column-major matrix (ld elements) for the FP64 GEMM /
+// SYRK items (tma64.cuh): 3D {16 rows of an atom, columns, atoms} with box {16, 16, 8} for
+// m- / n-contiguous operands, 2D {rows, columns} with box {16, 128} for the k-contiguous
+// operand of GEMM_NN; 128-byte swizzle, zero fill past the matrix.  Needs n a multiple of
+// 16 (whole atoms) and 16-byte aligned columns; without the encoder, or on an encoding
+// error, the run keeps the cp.async engine for every item.
+void encode_tmap64(RunArgs &a, void *dA, int64_t n, int64_t ld) {
+    static_assert(sizeof(CUtensorMap) == sizeof(a.tmap64_mn), "tensor map storage");
+    const PFN_cuTensorMapEncodeTiled_v12000 encode = tmap_encoder();
+    a.tma64 = 0;
+    if (!encode || n % 16 != 0 || ld % 2 != 0 || reinterpret_cast<uintptr_t>(dA) % 16 != 0) return;
+    CUtensorMap mn, kc;
+    const cuuint64_t dims3[3] = {16, cuuint64_t(n), cuuint64_t(n / 16)};
+    const cuuint64_t strides3[2] = {cuuint64_t(ld) * sizeof(double), 16 * sizeof(double)};
+    const cuuint32_t box3[3] = {16, t64::kBK, 8}, elem3[3] = {1, 1, 1};
+    if (encode(&mn, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, dA, dims3, strides3, box3, elem3, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return;
+    const cuuint64_t dims2[2] = {cuuint64_t(n), cuuint64_t(n)};
+    const cuuint64_t strides2[1] = {cuuint64_t(ld) * sizeof(double)};
+    const cuuint32_t box2[2] = {16, 128}, elem2[2] = {1, 1};
+    if (encode(&kc, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, dA, dims2, strides2, box2, elem2, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return;
+    std::memcpy(a.tmap64_mn, &mn, sizeof(mn));
+    std::memcpy(a.tmap64_k, &kc, sizeof(kc));
+    a.tma64 = 1;
+}
+
 // Reset, seed and launch one persistent run (shared by graphs, batches and the
 // no-allocation entry point's sibling paths).  Stream-ordered; no host synchronisation.
 int launch_run(const RunArgs &a, const int *deps_init, const int *roots, int n_roots, long long total_items,
@@ -573,6 +612,10 @@ static int run_persistent(mtd_graph *g, void *dA, int64_t lda, void *stream, int
     // the others keep the TF32 path on the FP32 matrix
     if (g->prec == MTD_PREC_BF16 && vec2 && g->dag.tile() % 64 == 0 && g->nest % 64 == 0)
         mtd::encode_tmap_bf16(a, g->d_bf16, g->dag.n(), g->bf16_ld);
+    // FP64 GEMM / SYRK items read their operands by TMA when every operand block starts on a
+    // 16-row atom (tile and nested sub-tile edges multiples of 16)
+    if (g->prec == MTD_PREC_FP64 && vec2 && g->dag.tile() % 16 == 0 && g->nest % 16 == 0 && g->use_tma64)
+        mtd::encode_tmap64(a, dA, g->dag.n(), lda);
     const int grid = g->num_sms;
     g->last_grid = grid;
     const int rc = launch_run(a, g->d_deps_init, g->d_roots, g->n_roots, g->total_items, g->prec, vec2, grid, s,

@@ -240,7 +240,7 @@ __device__ __forceinline__ int op_update_tc(const RunArgs &p, const MatCtx &m, c
 
 template <int VEC, typename T, int SPLIT = 1, bool ADJ = false>
 __device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int item, void *smem,
-                                        tc::State *tcs = nullptr) {
+                                        tc::State *tcs = nullptr, t64::State *s64 = nullptr) {
     if (t.op == kOpJoin) return 0;  // a join's one item: nothing to compute
     if constexpr (ADJ) return dispatch_adjoint<T, VEC, SPLIT>(p, t, item, smem);
     const MatCtx m = mat_ctx<T>(p, t);
@@ -250,12 +250,12 @@ __device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int 
         switch (t.op) {
         case MTD_OP_POTRF: return op_potrf<T, VEC>(p, m, t, smem);
         case MTD_OP_TRSM_RLT: return op_trsm_rlt<T, VEC>(p, m, t, item, smem);
-        case MTD_OP_SYRK_LN: return op_syrk_ln<T, VEC>(p, m, t, item, smem);
-        case MTD_OP_GEMM_NT: return op_gemm_nt<T, VEC>(p, m, t, item, smem);
+        case MTD_OP_SYRK_LN: return op_syrk_ln<T, VEC>(p, m, t, item, smem, s64);
+        case MTD_OP_GEMM_NT: return op_gemm_nt<T, VEC>(p, m, t, item, smem, s64);
         case MTD_OP_GETRF: return op_getrf<VEC>(p, m, t, smem);
         case MTD_OP_TRSM_LLNU: return op_trsm_llnu<VEC>(p, m, t, item, smem);
         case MTD_OP_TRSM_RUN: return op_trsm_run<VEC>(p, m, t, item, smem);
-        case MTD_OP_GEMM_NN: return op_gemm_nn<VEC>(p, m, t, item, smem);
+        case MTD_OP_GEMM_NN: return op_gemm_nn<VEC>(p, m, t, item, smem, s64);
         default: break;
         }
     } else {
@@ -383,6 +383,11 @@ __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const __grid_co
         return;
     } else {
         __shared__ int s_cmd, s_task, s_item;
+        // FP64 factorisations: barriers of the TMA-fed GEMM / SYRK items (tma64.cuh), kept
+        // for the whole run (the items use them only when the run carries tensor maps)
+        __shared__ t64::State s64;
+        constexpr bool kT64 = sizeof(T) == 8 && !ADJ;
+        if constexpr (kT64) t64::init(&s64);
         while (true) {
             if (threadIdx.x == 0) {
                 int tk = 0, it = 0;
@@ -396,7 +401,7 @@ __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const __grid_co
             const unsigned long long t_start = p.trace ? global_ns() : 0ull;
             DevTask t;
             load_task(p, task, &t);
-            const int st = dispatch<VEC, T, SPLIT, ADJ>(p, t, item, smem);
+            const int st = dispatch<VEC, T, SPLIT, ADJ>(p, t, item, smem, nullptr, kT64 ? &s64 : nullptr);
             __syncthreads();
             if (threadIdx.x == 0) finish_item(p, task, item, t_start, st == 0);
         }

@@ -332,6 +332,7 @@ __device__ bool mainloop_tma(State *st, uint8_t *smem, const void *map, int map_
         // the operands were written by other CTAs with generic stores (released and acquired
         // through the scheduler's counters): order them before this thread's async-proxy loads
         asm volatile("fence.proxy.async.global;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // after generic use of the stages
         auto issue = [&](int s, int kt) {
             const uint32_t bar = smem_addr(&st->full[s]), base = smem_addr(smem + s * kTmaStageBytes);
             const int k = k0 + kt * kTmaBK;
@@ -417,6 +418,7 @@ __device__ bool mainloop_tma_bf16(State *st, uint8_t *smem, const void *map, int
         const int nk = K / kBfBK;
         uint32_t ph = st->phases, fph = st->fphases;
         asm volatile("fence.proxy.async.global;" ::: "memory");  // see mainloop_tma
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         auto issue = [&](int s, int kt) {
             const uint32_t bar = smem_addr(&st->full[s]), base = smem_addr(smem + s * kBfStageBytes);
             const int k = k0 + kt * kBfBK;

@@ -17,6 +17,7 @@
 
 #include "device_types.hpp"
 #include "mma.cuh"
+#include "tma64.cuh"
 #include "../../include/mustard_b200.h"
 
 namespace mtd {
@@ -642,13 +643,42 @@ __device__ int op_trsm_llnu(const RunArgs &p, const MatCtx &m, const DevTask &t,
 // Update work items: one kGemmTile x kGemmTile output block each.
 // ---------------------------------------------------------------------------------
 
+// FP64 update items whose operands come by TMA (tma64.cuh): the run carries the tensor maps
+// (single-matrix FP64 runs of suitable geometry), the depth is whole k-slices and both
+// operand blocks start on 16-row atoms.
+__device__ __forceinline__ bool tma64_ok(const RunArgs &p, const t64::State *s64, int k, int a_row, int b_row) {
+    return s64 != nullptr && p.tma64 != 0 && p.mats == nullptr && k % t64::kBK == 0 && (a_row & 15) == 0 &&
+           (b_row & 15) == 0;
+}
+
+template <int BL>
+__device__ __noinline__ int update_tma64(const RunArgs &p, t64::State *s64, void *smem, const t64::Coords &c, double *C,
+                                         int64_t ldc,
+                            int mm, int nn, bool lower) {
+    t64::Engine<BL> e;
+    e.zero();
+    uint8_t *ring = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem) + 1023) & ~uintptr_t(1023));
+    // the tensor maps' addresses are taken on the kernel parameter itself
+    if (!e.run(s64, ring, p.tmap64_mn, p.tmap64_k, c, p.timeout_ns)) {
+        if (threadIdx.x == 0) report_error(p.ctl, MTD_ERR_TIMEOUT, 0);
+        return MTD_ERR_TIMEOUT;
+    }
+    e.sub_from(C, ldc, mm, nn, lower);
+    return 0;
+}
+
 // C -= A B^T   (cublasGemmEx N, T; cholesky_mustard.cu:376)
 template <typename T, int VEC, int SPLIT = 1>
-__device__ int op_gemm_nt(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
+__device__ int op_gemm_nt(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem,
+                          t64::State *s64 = nullptr) {
     using Mg = GemmMma<kBNContig, VEC, T, SPLIT>;
     const int nbn = (t.n + kGemmTile - 1) / kGemmTile;
     const int r0 = (item / nbn) * kGemmTile, c0 = (item % nbn) * kGemmTile;
     const int mm = min(kGemmTile, t.m - r0), nn = min(kGemmTile, t.n - c0);
+    if constexpr (sizeof(T) == 8 && VEC == 2)
+        if (tma64_ok(p, s64, t.k, t.ar + r0, t.br + c0))
+            return update_tma64<kBNContig>(p, s64, smem, t64::Coords{t.ar + r0, t.ac, t.br + c0, t.bc, t.k},
+                                           at<double>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn, false);
     Mg e;
     e.zero();
     e.run(smem, at<T>(m, t.ar + r0, t.ac), m.lda, at<T>(m, t.br + c0, t.bc), m.lda, mm, nn, t.k);
@@ -658,11 +688,16 @@ __device__ int op_gemm_nt(const RunArgs &p, const MatCtx &m, const DevTask &t, i
 
 // C -= A B   (cublasGemmEx N, N; lu_mustard.cu:511)
 template <int VEC>
-__device__ int op_gemm_nn(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
+__device__ int op_gemm_nn(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem,
+                          t64::State *s64 = nullptr) {
     using Mg = GemmMma<kBKContig, VEC>;
     const int nbn = (t.n + kGemmTile - 1) / kGemmTile;
     const int r0 = (item / nbn) * kGemmTile, c0 = (item % nbn) * kGemmTile;
     const int mm = min(kGemmTile, t.m - r0), nn = min(kGemmTile, t.n - c0);
+    if constexpr (VEC == 2)
+        if (tma64_ok(p, s64, t.k, t.ar + r0, t.br))  // B: k range from row br, columns bc + c0 ..
+            return update_tma64<kBKContig>(p, s64, smem, t64::Coords{t.ar + r0, t.ac, t.br, t.bc + c0, t.k},
+                                           at<double>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn, false);
     Mg e;
     e.zero();
     e.run(smem, at<double>(m, t.ar + r0, t.ac), m.lda, at<double>(m, t.br, t.bc + c0), m.lda, mm, nn, t.k);
@@ -672,13 +707,18 @@ __device__ int op_gemm_nn(const RunArgs &p, const MatCtx &m, const DevTask &t, i
 
 // C -= A A^T, lower triangle only   (cublasDsyrk L, N; cholesky_mustard.cu:327)
 template <typename T, int VEC, int SPLIT = 1>
-__device__ int op_syrk_ln(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
+__device__ int op_syrk_ln(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem,
+                          t64::State *s64 = nullptr) {
     using Mg = GemmMma<kBNContig, VEC, T, SPLIT>;
     int pb = 0;
     while ((pb + 1) * (pb + 2) / 2 <= item) ++pb;
     const int qb = item - pb * (pb + 1) / 2;
     const int r0 = pb * kGemmTile, c0 = qb * kGemmTile;
     const int mm = min(kGemmTile, t.m - r0), nn = min(kGemmTile, t.m - c0);
+    if constexpr (sizeof(T) == 8 && VEC == 2)
+        if (tma64_ok(p, s64, t.k, t.ar + r0, t.ar + c0))
+            return update_tma64<kBNContig>(p, s64, smem, t64::Coords{t.ar + r0, t.ac, t.ar + c0, t.ac, t.k},
+                                           at<double>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn, pb == qb);
     Mg e;
     e.zero();
     e.run(smem, at<T>(m, t.ar + r0, t.ac), m.lda, at<T>(m, t.ar + c0, t.ac), m.lda, mm, nn, t.k);
@@ -702,6 +742,7 @@ constexpr int kOpSmemBytes() {
     constexpr int m12 = (g1 > g2 ? g1 : g2) > pn ? (g1 > g2 ? g1 : g2) : pn;
     constexpr int m = m12 > g3 ? m12 : g3;
     constexpr int d = diag > chol ? diag : chol;
+    static_assert(t64::kSmemBytes <= (m > d ? m : d), "the FP64 TMA ring fits the engines' shared memory");
     return m > d ? m : d;
 }
 
