@@ -542,7 +542,7 @@ void encode_tmap64(RunArgs &a, void *dA, int64_t n, int64_t ld) {
     CUtensorMap mn, kc;
     const cuuint64_t dims3[3] = {16, cuuint64_t(n), cuuint64_t(n / 16)};
     const cuuint64_t strides3[2] = {cuuint64_t(ld) * sizeof(double), 16 * sizeof(double)};
-    const cuuint32_t box3[3] = {16, t64::kBK, 8}, elem3[3] = {1, 1, 1};
+    const cuuint32_t box3[3] = {16, cuuint32_t(t64::kBK), 8}, elem3[3] = {1, 1, 1};
     if (encode(&mn, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, dA, dims3, strides3, box3, elem3, CU_TENSOR_MAP_INTERLEAVE_NONE,
                CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)

@@ -651,8 +651,16 @@ __device__ __forceinline__ bool tma64_ok(const RunArgs &p, const t64::State *s64
            (b_row & 15) == 0;
 }
 
+#ifndef MTD_T64_NOINLINE
+#define MTD_T64_NOINLINE 1
+#endif
+#if MTD_T64_NOINLINE
+#define MTD_T64_INLINE __noinline__
+#else
+#define MTD_T64_INLINE __forceinline__
+#endif
 template <int BL>
-__device__ __noinline__ int update_tma64(const RunArgs &p, t64::State *s64, void *smem, const t64::Coords &c, double *C,
+__device__ MTD_T64_INLINE int update_tma64(const RunArgs &p, t64::State *s64, void *smem, const t64::Coords &c, double *C,
                                          int64_t ldc,
                             int mm, int nn, bool lower) {
     t64::Engine<BL> e;

@@ -16,8 +16,9 @@
 //     {16 rows of an atom, columns, atoms of 16 rows}, box {16, kBK, 8}: one load brings 128
 //     rows x kBK columns, element (m, k) at (m / 16) kBK 128 + k 128 + (((m % 16) / 2) ^ (k % 8)) 16
 //     + (m % 2) 8 bytes;
-//   - k-contiguous operands (B of GEMM_NN) through a 2D map {rows, columns}, box {16, 128}:
-//     element (k, n) at n 128 + ((k / 2) ^ (n % 8)) 16 + (k % 2) 8 bytes.
+//   - k-contiguous operands (B of GEMM_NN) through a 2D map {rows, columns}, box {16, 128},
+//     kBK / 16 boxes per slice: element (k, n) at (k / 16) 16384 + n 128 + (((k % 16) / 2) ^
+//     (n % 8)) 16 + (k % 2) 8 bytes.
 // Fragment loads of mma.sync.m16n8k8.f64 from these layouts are bank-conflict-free when the
 // logical rows of each 16-row fragment group are mapped to physical rows by
 //   P16(l) = (l & 1) | ((l >> 1) & 1) << 3 | ((l >> 2) & 1) << 1 | ((l >> 3) & 1) << 2
@@ -41,14 +42,28 @@
 namespace mtd {
 namespace t64 {
 
-constexpr int kBK = 16;                          // k per stage
-constexpr int kStages = 6;
-constexpr int kLag = 2;                          // stage of slice kt - kLag is refilled at slice kt
-constexpr int kOperandBytes = 128 * kBK * 8;     // 16 KB
+#ifndef MTD_T64_BK
+#define MTD_T64_BK 16
+#endif
+#ifndef MTD_T64_STAGES
+#define MTD_T64_STAGES 6
+#endif
+#ifndef MTD_T64_LAG
+#define MTD_T64_LAG 2
+#endif
+// 1: one arrival per warp on `empty` (lane 0, after the warp's reads); 0: one per thread
+#ifndef MTD_T64_WARP_ARRIVE
+#define MTD_T64_WARP_ARRIVE 1
+#endif
+constexpr int kBK = MTD_T64_BK;                  // k per stage (a multiple of 16)
+constexpr int kStages = MTD_T64_STAGES;
+constexpr int kLag = MTD_T64_LAG;                // stage of slice kt - kLag is refilled at slice kt
+constexpr int kArrivals = MTD_T64_WARP_ARRIVE ? kThreads / 32 : kThreads;
+constexpr int kOperandBytes = 128 * kBK * 8;     // 16 KB at kBK = 16
 constexpr int kStageBytes = 2 * kOperandBytes;   // 32 KB
 constexpr int kSmemBytes = kStages * kStageBytes + 1024;  // + alignment of the stage ring
 static_assert(kLag >= 1 && kLag < kStages, "refill lag");
-static_assert(kBK % 8 == 0, "swizzle rows repeat every 8 columns");
+static_assert(kBK % 16 == 0, "whole 16-deep boxes of the k-contiguous operand");
 
 struct State {
     uint64_t full[kStages];   // stage loaded (TMA complete_tx)
@@ -70,7 +85,7 @@ __device__ __forceinline__ void init(State *st) {
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(&st->full[s])), "r"(1));
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(&st->empty[s])), "r"(kThreads));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(&st->empty[s])), "r"(kArrivals));
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         st->fbase = 0;
@@ -95,8 +110,15 @@ __device__ __forceinline__ bool wait_parity(uint64_t *bar, uint32_t parity, unsi
     }
 }
 
-__device__ __forceinline__ void arrive(uint64_t *bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(bar)) : "memory");
+// This thread (or warp) has read the stage: every DMMA that used its fragments is issued,
+// so those shared-memory loads have returned.
+__device__ __forceinline__ void release(uint64_t *bar) {
+    if (MTD_T64_WARP_ARRIVE) {
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(bar)) : "memory");
+    } else {
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(bar)) : "memory");
+    }
 }
 
 __device__ __forceinline__ void load_3d(uint32_t dst, const void *map, int x, int y, int z, uint32_t bar) {
@@ -135,7 +157,9 @@ static_assert(maps_are_permutations(), "fragment row / column maps");
 __device__ __forceinline__ int off_mn(int m, int k) {
     return (m >> 4) * (kBK * 128) + k * 128 + ((((m & 15) >> 1) ^ (k & 7)) << 4) + ((m & 1) << 3);
 }
-__device__ __forceinline__ int off_k(int k, int n) { return n * 128 + ((((k & 15) >> 1) ^ (n & 7)) << 4) + ((k & 1) << 3); }
+__device__ __forceinline__ int off_k(int k, int n) {
+    return (k >> 4) * (128 * 128) + n * 128 + ((((k & 15) >> 1) ^ (n & 7)) << 4) + ((k & 1) << 3);
+}
 
 // Where one item's operands start.  A: rows a_row .. a_row + 127, columns a_col .. (3D map).
 // B of GEMM_NT / SYRK (kBNContig): rows b_row .., columns b_col .. (3D map).  B of GEMM_NN
@@ -210,8 +234,13 @@ struct Engine {
         const uint32_t bar = saddr(&st->full[s]), dst = saddr(ring + s * kStageBytes);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kStageBytes) : "memory");
         load_3d(dst, map_mn, 0, c.a_col + kt * kBK, c.a_row >> 4, bar);
-        if (BL == kBNContig) load_3d(dst + kOperandBytes, map_mn, 0, c.b_col + kt * kBK, c.b_row >> 4, bar);
-        else load_2d(dst + kOperandBytes, map_k, c.b_row + kt * kBK, c.b_col, bar);
+        if (BL == kBNContig) {
+            load_3d(dst + kOperandBytes, map_mn, 0, c.b_col + kt * kBK, c.b_row >> 4, bar);
+        } else {
+#pragma unroll
+            for (int kb = 0; kb < kBK / 16; ++kb)  // 16-deep boxes of 128 columns, 16 KB each
+                load_2d(dst + kOperandBytes + kb * 16384, map_k, c.b_row + kt * kBK + 16 * kb, c.b_col, bar);
+        }
     }
 
     // acc = A B over c.K (all threads of the CTA).  `ring`: kStages x kStageBytes, 1024-byte
@@ -249,7 +278,7 @@ struct Engine {
             ok = wait_parity(&st->full[s], fpar, deadline);
             if (!ok) break;
             compute_stage(ring + s * kStageBytes);
-            arrive(&st->empty[s]);
+            release(&st->empty[s]);
         }
         if (!ok) {
             // thread 0: let the loads it issued and did not consume land before leaving
