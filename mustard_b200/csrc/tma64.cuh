@@ -52,8 +52,17 @@ namespace t64 {
 #define MTD_T64_LAG 2
 #endif
 // 1: one arrival per warp on `empty` (lane 0, after the warp's reads); 0: one per thread
+// 1: fragment offsets precomputed once per item (Engine::offsets); 0: computed per load
+#ifndef MTD_T64_PRECOMP
+#define MTD_T64_PRECOMP 0
+#endif
 #ifndef MTD_T64_WARP_ARRIVE
-#define MTD_T64_WARP_ARRIVE 1
+#define MTD_T64_WARP_ARRIVE 0
+#endif
+// 1: B fragments loaded per column fragment inside the row loop (12 live fragment registers
+// instead of 24, twice the B loads)
+#ifndef MTD_T64_BINNER
+#define MTD_T64_BINNER 0
 #endif
 constexpr int kBK = MTD_T64_BK;                  // k per stage (a multiple of 16)
 constexpr int kStages = MTD_T64_STAGES;
@@ -197,6 +206,89 @@ struct Engine {
         return wn0 + j * 8 + r8(l8);
     }
 
+    // This thread's fragment offsets at k = t (t = lane % 4) inside a stage: A rows of the
+    // fragments (i, g) and (i, g + 8), B columns of fragment j.  Every other k of a slice
+    // follows by one add and one XOR: for k = ks + t (+ 4), ks a multiple of 8, the swizzled
+    // chunk of an m- / n-contiguous operand is ((m % 16) / 2) ^ t (^ 4), i.e. +ks 128
+    // (+ 512, ^ 64); of the k-contiguous operand ((k % 16) / 2) ^ (n % 8) = (t / 2 ^ n % 8)
+    // ^ ((ks % 16 + 4c) / 2), i.e. ^ (ks % 16 + 4c) 8, plus (ks / 16) 16384.
+    struct Offsets {
+        int a[FM][2];
+        int b[FN];
+    };
+    __device__ __forceinline__ static Offsets offsets() {
+        Offsets o;
+        const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+        for (int i = 0; i < FM; ++i) {
+            o.a[i][0] = off_mn(prow(i, g), t);
+            o.a[i][1] = off_mn(prow(i, g + 8), t);
+        }
+#pragma unroll
+        for (int j = 0; j < FN; ++j) o.b[j] = BL == kBNContig ? off_mn(pcol(j, g), t) : off_k(t, pcol(j, g));
+        return o;
+    }
+
+    __device__ __forceinline__ static void load_b(const uint8_t *Bs, int ob, int ks, double (&b)[2]) {
+        if (BL == kBNContig) {
+            b[0] = *reinterpret_cast<const double *>(Bs + ob + ks * 128);
+            b[1] = *reinterpret_cast<const double *>(Bs + ((ob + ks * 128 + 512) ^ 64));
+        } else {
+            const int kb = (ks >> 4) * 16384, x0 = (ks & 15) * 8, x1 = ((ks & 15) + 4) * 8;
+            b[0] = *reinterpret_cast<const double *>(Bs + kb + (ob ^ x0));
+            b[1] = *reinterpret_cast<const double *>(Bs + kb + (ob ^ x1));
+        }
+    }
+
+    __device__ __forceinline__ void compute_stage_pre(const uint8_t *st_base, const Offsets &o) {
+        const uint8_t *As = st_base, *Bs = st_base + kOperandBytes;
+#if MTD_T64_BINNER
+#pragma unroll
+        for (int ks = 0; ks < kBK; ks += 8) {
+#pragma unroll
+            for (int i = 0; i < FM; ++i) {
+                double af[4];
+                af[0] = *reinterpret_cast<const double *>(As + o.a[i][0] + ks * 128);
+                af[1] = *reinterpret_cast<const double *>(As + o.a[i][1] + ks * 128);
+                af[2] = *reinterpret_cast<const double *>(As + ((o.a[i][0] + ks * 128 + 512) ^ 64));
+                af[3] = *reinterpret_cast<const double *>(As + ((o.a[i][1] + ks * 128 + 512) ^ 64));
+#pragma unroll
+                for (int j = 0; j < FN; ++j) {
+                    double bf[2];
+                    load_b(Bs, o.b[j], ks, bf);
+                    dmma_16x8x8(acc[i][j], af, bf);
+                }
+            }
+        }
+        return;
+#endif
+#pragma unroll
+        for (int ks = 0; ks < kBK; ks += 8) {
+            double bf[FN][2];
+#pragma unroll
+            for (int j = 0; j < FN; ++j) {
+                if (BL == kBNContig) {
+                    bf[j][0] = *reinterpret_cast<const double *>(Bs + o.b[j] + ks * 128);
+                    bf[j][1] = *reinterpret_cast<const double *>(Bs + ((o.b[j] + ks * 128 + 512) ^ 64));
+                } else {
+                    const int kb = (ks >> 4) * 16384, x0 = (ks & 15) * 8, x1 = ((ks & 15) + 4) * 8;
+                    bf[j][0] = *reinterpret_cast<const double *>(Bs + kb + (o.b[j] ^ x0));
+                    bf[j][1] = *reinterpret_cast<const double *>(Bs + kb + (o.b[j] ^ x1));
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < FM; ++i) {
+                double af[4];
+                af[0] = *reinterpret_cast<const double *>(As + o.a[i][0] + ks * 128);
+                af[1] = *reinterpret_cast<const double *>(As + o.a[i][1] + ks * 128);
+                af[2] = *reinterpret_cast<const double *>(As + ((o.a[i][0] + ks * 128 + 512) ^ 64));
+                af[3] = *reinterpret_cast<const double *>(As + ((o.a[i][1] + ks * 128 + 512) ^ 64));
+#pragma unroll
+                for (int j = 0; j < FN; ++j) dmma_16x8x8(acc[i][j], af, bf[j]);
+            }
+        }
+    }
+
     __device__ __forceinline__ void compute_stage(const uint8_t *st_base) {
         const uint8_t *As = st_base, *Bs = st_base + kOperandBytes;
         const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
@@ -262,6 +354,9 @@ struct Engine {
         }
         bool ok = true;
         int kt = 0;
+#if MTD_T64_PRECOMP
+        const Offsets offs = offsets();
+#endif
         for (; kt < nk; ++kt) {
             const int s = kt % kStages;
             if (threadIdx.x == 0 && kt >= kLag && issued < nk) {
@@ -277,7 +372,11 @@ struct Engine {
             const uint32_t fpar = ((fbase >> s) + kt / kStages) & 1u;
             ok = wait_parity(&st->full[s], fpar, deadline);
             if (!ok) break;
+#if MTD_T64_PRECOMP
+            compute_stage_pre(ring + s * kStageBytes, offs);
+#else
             compute_stage(ring + s * kStageBytes);
+#endif
             release(&st->empty[s]);
         }
         if (!ok) {
