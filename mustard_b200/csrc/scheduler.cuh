@@ -370,6 +370,127 @@ __device__ __forceinline__ void persistent_loop_tc(const RunArgs &p, double *sme
     }
 }
 
+// Named barrier 2 over warps 2 .. 15 (the warp-specialised loop's drain warps).
+__device__ __forceinline__ void sync_ws_drain_warps() { asm volatile("bar.sync 2, %0;" ::"r"(kThreads - 64) : "memory"); }
+
+// The persistent loop of the tcgen05 kernel on the warp-specialised pipeline (tcgen05.cuh,
+// ws_*).  One item per round, taken from one of two claim slots:
+//   - a TMA item (GEMM_NT / SYRK_LN with TMA operands): thread 0 loads its slices and then
+//     claims the next item into the other slot; thread 32 issues its MMAs into accumulator
+//     `buf`; warps 2 .. 15 first update C from the previous TMA item's accumulator (waiting on
+//     its accf barrier; thread 64 then completes that item) and then prefetch this item's C.
+//     The round ends when all three are done, so the previous item's C update and this
+//     item's loads and MMAs overlap, and the next item's loads queue behind this item's MMAs;
+//   - any other item: warps 2 .. 15 finish the pending TMA item first (its MMAs are then done,
+//     so the ring's shared memory is free), then all threads run the item as the plain loop
+//     does, and thread 0 completes it and claims the next.
+// Every wait is bounded by the run's timeout; an expired wait raises the error (abort) and
+// the loop drains what it has started before leaving.
+template <int VEC, typename T, int SPLIT>
+__device__ __forceinline__ void persistent_loop_ws(const RunArgs &p, double *smem, tc::State &tcs, tc::WsState &ws) {
+    __shared__ int s_cmd[2], s_task[2], s_item[2];
+    float cv[tc::kWsDrainChunks][16];  // warps 2 .. 15: the pending item's C values
+    // warps 2 .. 15: the pending TMA item (its accumulator is being computed or is final)
+    bool pv = false;
+    float *pC = nullptr;
+    int64_t pld = 0;
+    int pM = 0, pN = 0, plower = 0, ptask = 0, pitem = 0, pbuf = 0;
+    unsigned long long pt0 = 0;
+    uint32_t uses0 = 0, uses1 = 0;  // items drained from each accumulator (accf parities)
+    int buf = 0;
+    const int warp = threadIdx.x >> 5;
+    uint8_t *ring = tc_stages(smem);
+    auto drain_pending = [&]() {  // warps 2 .. 15
+        if (!pv) return;
+        const uint32_t par = (pbuf ? uses1 : uses0) & 1u;
+        const bool ok = tc::wait_bar(&ws.accf[pbuf], par, global_ns() + p.timeout_ns);
+        if (pbuf) ++uses1;
+        else ++uses0;
+        if (ok) tc::ws_drain(tcs.taddr + tc::kAccCols * pbuf, pC, pld, pM, pN, plower != 0, cv);
+        sync_ws_drain_warps();
+        if (threadIdx.x == 64) {
+            if (!ok) report_error(p.ctl, MTD_ERR_TIMEOUT, 0);
+            finish_item(p, ptask, pitem, pt0, ok);
+        }
+        pv = false;
+    };
+    if (threadIdx.x == 0) {
+        int tk = 0, it = 0;
+        s_cmd[0] = pop_item(p, &tk, &it);
+        s_task[0] = tk;
+        s_item[0] = it;
+    }
+    __syncthreads();
+    for (int r = 0;; ++r) {
+        const int slot = r & 1, cmd = s_cmd[slot], task = s_task[slot], item = s_item[slot];
+        if (cmd != kCmdWork) {
+            if (warp >= 2) drain_pending();
+            break;
+        }
+        const unsigned long long t_start = p.trace ? global_ns() : 0ull;
+        DevTask t;
+        load_task(p, task, &t);
+        const UpdateGeom g = update_geom(t, item);
+        const int path = tc_path(p, t, g, p.tma != 0);
+        if (path != kTcStaged) {
+            const MatCtx m = mat_ctx<T>(p, t);
+            float *C = at<float>(m, t.cr + g.r0, t.cc + g.c0);
+            const int kind = path == kTcTmaBf16 ? tc::kWsBf16 : (p.tma == tc::kTmaMap3D ? tc::kWsTf32Map3D : tc::kWsTf32Map2D);
+            if (threadIdx.x == 0) {
+                const void *map = path == kTcTmaBf16 ? static_cast<const void *>(p.tmap_bf16) : static_cast<const void *>(p.tmap);
+                if (!tc::ws_load(&ws, ring, map, kind, t.ar + g.r0, g.brow, t.ac, t.k, global_ns() + p.timeout_ns))
+                    report_error(p.ctl, MTD_ERR_TIMEOUT, 0);
+                int tk = 0, it = 0;
+                s_cmd[slot ^ 1] = pop_item(p, &tk, &it);
+                s_task[slot ^ 1] = tk;
+                s_item[slot ^ 1] = it;
+            } else if (threadIdx.x == 32) {
+                if (!tc::ws_mma(&ws, ring, kind, t.k, tcs.taddr + tc::kAccCols * buf, buf, global_ns() + p.timeout_ns))
+                    report_error(p.ctl, MTD_ERR_TIMEOUT, 0);
+            } else if (warp >= 2) {
+                drain_pending();
+                tc::ws_prefetch_c(C, m.lda, g.mm, g.nn, g.lower, cv);
+                pv = true;
+                pC = C;
+                pld = m.lda;
+                pM = g.mm;
+                pN = g.nn;
+                plower = g.lower ? 1 : 0;
+                ptask = task;
+                pitem = item;
+                pt0 = t_start;
+                pbuf = buf;
+            }
+            buf ^= 1;
+            __syncthreads();
+            continue;
+        }
+        if (warp >= 2) drain_pending();
+        __syncthreads();
+        const int st = dispatch<VEC, T, SPLIT, false>(p, t, item, smem, &tcs);
+        // nothing is pending here: redefining cv after the tile operation frees its registers
+#pragma unroll
+        for (int c = 0; c < tc::kWsDrainChunks; ++c)
+#pragma unroll
+            for (int j = 0; j < 16; ++j) cv[c][j] = 0.f;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            finish_item(p, task, item, t_start, st == 0);
+            int tk = 0, it = 0;
+            s_cmd[slot ^ 1] = pop_item(p, &tk, &it);
+            s_task[slot ^ 1] = tk;
+            s_item[slot ^ 1] = it;
+        }
+        __syncthreads();
+    }
+    // leave nothing in flight: thread 0 waits (bounded) for loads no MMA consumed
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned long long grace = global_ns() + 1000000ull;
+        for (uint32_t g = ws.cons; g < ws.prod; ++g) tc::wait_bar(&ws.full[g % tc::kWsStages], (g / tc::kWsStages) & 1u, grace);
+    }
+}
+
 template <int VEC, typename T, int SPLIT = 1, bool ADJ = false>
 __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const __grid_constant__ RunArgs p) {
     extern __shared__ __align__(128) double smem[];
@@ -377,8 +498,15 @@ __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const __grid_co
     if (threadIdx.x == 0) atomicMin(&p.ctl->start_ns, global_ns());
     if constexpr (kTc) {
         __shared__ tc::State tcs;
-        tc::init(&tcs);  // TMEM accumulators and barriers, held for the whole run
-        persistent_loop_tc<VEC, T, SPLIT>(p, smem, tcs);
+        if (MTD_TC_WS) {
+            __shared__ tc::WsState ws;
+            tc::ws_init(&ws);
+            tc::init(&tcs);  // TMEM accumulators and the staged items' barriers; its barrier publishes ws
+            persistent_loop_ws<VEC, T, SPLIT>(p, smem, tcs, ws);
+        } else {
+            tc::init(&tcs);  // TMEM accumulators and barriers, held for the whole run
+            persistent_loop_tc<VEC, T, SPLIT>(p, smem, tcs);
+        }
         tc::release(&tcs);
         return;
     } else {

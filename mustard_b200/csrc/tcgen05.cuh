@@ -298,13 +298,21 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const void *map, int x
         : "memory");
 }
 
-// TMA pipeline geometry: 64-deep k-slices, 3 stages of 64 KB (A then B).  An operand slice is
-// 4 MN atoms of 32 rows, each atom 64 K-rows of 128 bytes (8 KB), K-rows 128 bytes apart.
-constexpr int kTmaBK = 64;
+// 1: TMA items run on the warp-specialised pipeline (thread 0 loads, thread 32 issues MMAs,
+// warps 2 .. 15 drain accumulators; ws_* below), with 32-deep TF32 / 64-deep BF16 slices of
+// 32 KB in a ring of six stages; 0: the single-thread pipeline (mainloop_tma*) with 64-deep /
+// 128-deep slices of 64 KB in three stages.
+#ifndef MTD_TC_WS
+#define MTD_TC_WS 1
+#endif
+
+// TMA pipeline geometry: kTmaBK-deep k-slices (A then B).  An operand slice is 4 MN atoms of
+// 32 rows, each atom kTmaBK K-rows of 128 bytes, K-rows 128 bytes apart.
+constexpr int kTmaBK = MTD_TC_WS ? 32 : 64;
 constexpr int kTmaStages = 3;
-constexpr int kTmaAtomBytes = 32 * kTmaBK * 4;                // 8 KB
-constexpr int kTmaOperandBytes = 4 * kTmaAtomBytes;           // 32 KB
-constexpr int kTmaStageBytes = 2 * kTmaOperandBytes;          // 64 KB
+constexpr int kTmaAtomBytes = 32 * kTmaBK * 4;                // 4 KB (8 KB at kTmaBK = 64)
+constexpr int kTmaOperandBytes = 4 * kTmaAtomBytes;
+constexpr int kTmaStageBytes = 2 * kTmaOperandBytes;
 static_assert(kTmaStages * kTmaStageBytes <= kSmemBytes, "TMA stages fit the engine's shared memory");
 static_assert(kTmaStages <= kStages, "TMA stages use the engine's barriers");
 enum { kTmaNone = 0, kTmaMap2D = 1, kTmaMap3D = 2 };
@@ -400,11 +408,11 @@ __device__ bool mainloop_tma(State *st, uint8_t *smem, const void *map, int map_
 // (LBO), 8-row groups 1 KB apart (SBO), layout type 2 (128-byte swizzle); this layout was
 // checked bit-exact against a host product of the same BF16 values.  a_row, b_row multiples
 // of 64, K a multiple of kBfBK; otherwise as mainloop_tma (thread 0 alone, into `acc`).
-constexpr int kBfBK = 128;
+constexpr int kBfBK = MTD_TC_WS ? 64 : 128;
 constexpr int kBfStages = 3;
-constexpr int kBfAtomBytes = kBfBK * 128;                   // 64 BF16 x kBfBK rows: 16 KB
-constexpr int kBfOperandBytes = 2 * kBfAtomBytes;           // 32 KB
-constexpr int kBfStageBytes = 2 * kBfOperandBytes;          // 64 KB
+constexpr int kBfAtomBytes = kBfBK * 128;                   // 64 BF16 x kBfBK rows
+constexpr int kBfOperandBytes = 2 * kBfAtomBytes;
+constexpr int kBfStageBytes = 2 * kBfOperandBytes;
 static_assert(kBfStages * kBfStageBytes <= kSmemBytes, "BF16 stages fit the engine's shared memory");
 static_assert(kBfStages <= kStages, "BF16 stages use the engine's barriers");
 constexpr uint32_t kIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
@@ -466,6 +474,205 @@ __device__ bool mainloop_tma_bf16(State *st, uint8_t *smem, const void *map, int
         st->fphases = fph;
     }
     return ok;
+}
+
+// ---- warp-specialised pipeline ------------------------------------------------------------
+//
+// Thread 0 loads: one expect_tx and two (TF32 2D map: eight) TMA loads per slice into stage
+// g % kWsStages of a ring that runs on across items (g counts the CTA's slices), waiting for a
+// stage only while the MMAs of its previous slice are still reading it.  Thread 32 issues the
+// MMAs of each slice once it has landed, commits them to the stage's `empty` barrier, and
+// after the item's last slice commits to the accumulator's `accf` barrier.  Neither waits for
+// the other's work beyond the stage hand-offs, so loads run up to six slices ahead of the
+// MMAs and the MMA thread never waits for a reload.  Warps 2 .. 15 update C from the finished
+// accumulator (one of two in TMEM) while the next item's slices stream in.
+constexpr int kWsStages = 6;
+constexpr int kWsStageBytes = 32768;
+static_assert(kWsStages * kWsStageBytes <= kSmemBytes, "the ring fits the engine's shared memory");
+static_assert(!MTD_TC_WS || (kTmaStageBytes == kWsStageBytes && kBfStageBytes == kWsStageBytes),
+              "TF32 and BF16 slices share the ring");
+enum { kWsTf32Map3D = 0, kWsTf32Map2D = 1, kWsBf16 = 2 };
+
+struct WsState {
+    uint64_t full[kWsStages];   // slice g landed (TMA complete_tx); parity (g / kWsStages) & 1
+    uint64_t empty[kWsStages];  // MMAs of slice g done (tcgen05.commit)
+    uint64_t accf[2];           // an item's last MMAs into accumulator b done
+    uint32_t prod;              // slices loaded so far (thread 0)
+    uint32_t cons;              // slices whose MMAs were issued (thread 32)
+};
+
+// Once per CTA (thread 0 initialises; the caller's barrier publishes it).
+__device__ __forceinline__ void ws_init(WsState *w) {
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kWsStages; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&w->full[s])), "r"(1));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&w->empty[s])), "r"(1));
+        }
+        for (int b = 0; b < 2; ++b)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&w->accf[b])), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        w->prod = 0;
+        w->cons = 0;
+    }
+}
+
+__device__ __forceinline__ int ws_bk(int kind) { return kind == kWsBf16 ? kBfBK : kTmaBK; }
+
+// Thread 0: load the item's K / bk slices (A rows a_row .., B rows b_row .., columns k0 ..).
+// False if a wait for a free stage ran past the deadline.
+__device__ bool ws_load(WsState *w, uint8_t *ring, const void *map, int kind, int a_row, int b_row, int k0, int K,
+                        unsigned long long deadline) {
+    asm volatile("fence.proxy.async.global;" ::: "memory");       // operands other CTAs wrote
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the ring's earlier generic use
+    const int bk = ws_bk(kind), nk = K / bk;
+    uint32_t g = w->prod;
+    bool ok = true;
+    for (int kt = 0; kt < nk; ++kt, ++g) {
+        const int s = static_cast<int>(g % kWsStages);
+        if (g >= uint32_t(kWsStages) && !wait_bar(&w->empty[s], ((g / kWsStages) - 1) & 1u, deadline)) {
+            ok = false;
+            break;
+        }
+        const uint32_t bar = smem_addr(&w->full[s]), base = smem_addr(ring + s * kWsStageBytes);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kWsStageBytes)
+                     : "memory");
+        const int k = k0 + kt * bk;
+        if (kind == kWsBf16) {
+            tma_load_3d(base, map, 0, k, a_row >> 6, bar);
+            tma_load_3d(base + kWsStageBytes / 2, map, 0, k, b_row >> 6, bar);
+        } else if (kind == kWsTf32Map3D) {
+            tma_load_3d(base, map, 0, k, a_row >> 5, bar);
+            tma_load_3d(base + kWsStageBytes / 2, map, 0, k, b_row >> 5, bar);
+        } else {
+            for (int i = 0; i < 4; ++i) {
+                tma_load_2d(base + i * kTmaAtomBytes, map, a_row + 32 * i, k, bar);
+                tma_load_2d(base + kWsStageBytes / 2 + i * kTmaAtomBytes, map, b_row + 32 * i, k, bar);
+            }
+        }
+    }
+    w->prod = g;
+    return ok;
+}
+
+// Thread 32: acc(128 x 128) = A B^T over the item's slices as they land; commits each slice to
+// its stage's `empty` barrier and the whole item to accf[buf].  False on a timed-out wait.
+__device__ bool ws_mma(WsState *w, uint8_t *ring, int kind, int K, uint32_t acc, int buf,
+                       unsigned long long deadline) {
+    const int bk = ws_bk(kind), nk = K / bk;
+    uint32_t g = w->cons;
+    bool ok = true;
+    for (int kt = 0; kt < nk; ++kt, ++g) {
+        const int s = static_cast<int>(g % kWsStages);
+        if (!wait_bar(&w->full[s], (g / kWsStages) & 1u, deadline)) {
+            ok = false;
+            break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t a0 = smem_addr(ring + s * kWsStageBytes), b0 = a0 + kWsStageBytes / 2;
+        if (kind == kWsBf16) {
+#pragma unroll
+            for (int q = 0; q < kBfBK / 16; ++q) {
+                const uint64_t lead = uint64_t(kBfAtomBytes >> 4) << 16, stride = uint64_t(1024 >> 4) << 32;
+                const uint64_t ad = uint64_t(((a0 + q * 2048) >> 4) & 0x3fff) | lead | stride | (1ull << 46) | (2ull << 61);
+                const uint64_t bd = uint64_t(((b0 + q * 2048) >> 4) & 0x3fff) | lead | stride | (1ull << 46) | (2ull << 61);
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(acc),
+                    "l"(ad), "l"(bd), "r"(kIdescBf16), "r"((kt > 0 || q > 0) ? 1u : 0u)
+                    : "memory");
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < kTmaBK / 8; ++q) {
+                const uint64_t lead = uint64_t(kTmaAtomBytes >> 4) << 16, stride = uint64_t(512 >> 4) << 32;
+                const uint64_t ad = uint64_t(((a0 + q * 1024) >> 4) & 0x3fff) | lead | stride | (1ull << 46) | (1ull << 61);
+                const uint64_t bd = uint64_t(((b0 + q * 1024) >> 4) & 0x3fff) | lead | stride | (1ull << 46) | (1ull << 61);
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(acc),
+                    "l"(ad), "l"(bd), "r"(kIdescTf32), "r"((kt > 0 || q > 0) ? 1u : 0u)
+                    : "memory");
+            }
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_addr(&w->empty[s]))
+                     : "memory");
+    }
+    if (ok)
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_addr(&w->accf[buf]))
+                     : "memory");
+    w->cons = g;
+    return ok;
+}
+
+// The C update of a finished accumulator is shared by warps 2 .. 15.  Warp w covers TMEM lane
+// quarter q = w % 4; the quarter's 8 chunks of 16 columns go to its warps among 2 .. 15 --
+// three for q = 0, 1 (warps 4 + q, 8 + q, 12 + q), four for q = 2, 3 -- chunk rank + c * count.
+constexpr int kWsDrainChunks = 3;
+__host__ __device__ constexpr int ws_count(int q) { return q < 2 ? 3 : 4; }
+__host__ __device__ constexpr int ws_rank(int warp) { return (warp & 3) < 2 ? (warp >> 2) - 1 : (warp >> 2); }
+constexpr bool ws_drain_covers_once() {
+    for (int q = 0; q < 4; ++q)
+        for (int ch = 0; ch < kN / 16; ++ch) {
+            int owners = 0;
+            for (int w = 2; w < 16; ++w) {
+                if ((w & 3) != q) continue;
+                for (int c = 0; c < kWsDrainChunks; ++c)
+                    if (ws_rank(w) + c * ws_count(q) == ch) ++owners;
+            }
+            if (owners != 1) return false;
+        }
+    for (int w = 2; w < 16; ++w)
+        if (ws_rank(w) < 0 || ws_rank(w) >= ws_count(w & 3)) return false;
+    return true;
+}
+static_assert(ws_drain_covers_once(), "warps 2 .. 15 cover the accumulator once");
+
+// Warps 2 .. 15: this thread's C values of an item (row 32 q + lane of its chunks; 0 outside
+// the block or above the diagonal), all loads issued back to back.
+__device__ __forceinline__ void ws_prefetch_c(const float *C, int64_t ldc, int M, int N, bool lower,
+                                              float (&cv)[kWsDrainChunks][16]) {
+    const int warp = threadIdx.x >> 5, q = warp & 3, rank = ws_rank(warp), count = ws_count(q);
+    const int row = q * 32 + (threadIdx.x & 31);
+#pragma unroll
+    for (int c = 0; c < kWsDrainChunks; ++c) {
+        const int ch = rank + c * count;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int col = ch * 16 + j;
+            const bool in = ch < kN / 16 && row < M && col < N && (!lower || row >= col);
+            cv[c][j] = in ? __ldcg(C + row + int64_t(col) * ldc) : 0.f;
+        }
+    }
+}
+
+// Warps 2 .. 15, once accf[buf] says the item's MMAs are done: C = cv - accumulator.
+__device__ __forceinline__ void ws_drain(uint32_t acc, float *C, int64_t ldc, int M, int N, bool lower,
+                                         const float (&cv)[kWsDrainChunks][16]) {
+    const int warp = threadIdx.x >> 5, q = warp & 3, rank = ws_rank(warp), count = ws_count(q);
+    const int row = q * 32 + (threadIdx.x & 31);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+    for (int c = 0; c < kWsDrainChunks; ++c) {
+        const int ch = rank + c * count;
+        if (ch >= kN / 16) break;  // warp-uniform
+        uint32_t v[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(acc + (uint32_t(q * 32) << 16) + uint32_t(ch * 16)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int col = ch * 16 + j;
+            if (row < M && col < N && (!lower || row >= col)) C[row + int64_t(col) * ldc] = cv[c][j] - __uint_as_float(v[j]);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 }
 
 // A TMA item whose accumulator is final but whose update of C is still to be done.
