@@ -37,9 +37,11 @@ struct mtd_graph {
     bool trace = false;
     double timeout_s = 10.0;
     int nest = kNestTile;
-    // FP64 GEMM / SYRK items fed by TMA when the geometry allows; the environment variable
-    // MTD_TMA64=0, read when the graph is finalised, keeps them on the cp.async engine
-    bool use_tma64 = true;
+    // FP64 GEMM / SYRK items fed by TMA (tma64.cuh) when the geometry allows and the
+    // environment variable MTD_TMA64=1 is set when the graph is finalised; by default they run
+    // on the cp.async engine, which measured faster on B200 (the TMA engine's swizzled
+    // fragment addressing costs more issue slots than the copies it saves)
+    bool use_tma64 = false;
     int prec = MTD_PREC_FP64;  // element type of the matrix runs factor
     unsigned short *d_bf16 = nullptr;  // MTD_PREC_BF16: BF16 copy of the panels (bf16_ld x n)
     int64_t bf16_ld = 0;
@@ -374,7 +376,7 @@ int mtd_graph_finalize(mtd_graph *g) {
     if (rc) return rc;
     {
         const char *e = std::getenv("MTD_TMA64");
-        g->use_tma64 = !(e && e[0] == '0');
+        g->use_tma64 = e && e[0] == '1';
     }
     const std::vector<DevTask> &tasks = g->low.tasks;
     const std::vector<int> &succ = g->low.succ;

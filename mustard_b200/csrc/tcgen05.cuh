@@ -497,6 +497,7 @@ struct WsState {
     uint64_t full[kWsStages];   // slice g landed (TMA complete_tx); parity (g / kWsStages) & 1
     uint64_t empty[kWsStages];  // MMAs of slice g done (tcgen05.commit)
     uint64_t accf[2];           // an item's last MMAs into accumulator b done
+    uint64_t quiet;             // thread 32's last MMAs done, before the TMEM is freed
     uint32_t prod;              // slices loaded so far (thread 0)
     uint32_t cons;              // slices whose MMAs were issued (thread 32)
 };
@@ -510,6 +511,7 @@ __device__ __forceinline__ void ws_init(WsState *w) {
         }
         for (int b = 0; b < 2; ++b)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&w->accf[b])), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&w->quiet)), "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         w->prod = 0;
         w->cons = 0;
@@ -606,6 +608,15 @@ __device__ bool ws_mma(WsState *w, uint8_t *ring, int kind, int K, uint32_t acc,
                      : "memory");
     w->cons = g;
     return ok;
+}
+
+// Thread 32, once, before the CTA frees its TMEM: wait (bounded) until every MMA it issued
+// has completed (they normally have: the last item was drained).
+__device__ __forceinline__ void ws_quiesce(WsState *w, unsigned long long deadline) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_addr(&w->quiet))
+                 : "memory");
+    wait_bar(&w->quiet, 0u, deadline);
 }
 
 // The C update of a finished accumulator is shared by warps 2 .. 15.  Warp w covers TMEM lane

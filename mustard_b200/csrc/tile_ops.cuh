@@ -643,22 +643,6 @@ __device__ int op_trsm_llnu(const RunArgs &p, const MatCtx &m, const DevTask &t,
 // Update work items: one kGemmTile x kGemmTile output block each.
 // ---------------------------------------------------------------------------------
 
-// Pull the mm x nn block of C at `C` into L2 (two 128-byte lines per thread for a 128 x 128
-// FP64 block) before the k-loop, so the epilogue's read-modify-write finds it there instead
-// of in HBM.
-#ifndef MTD_C_PREFETCH
-#define MTD_C_PREFETCH 0
-#endif
-template <typename T>
-__device__ __forceinline__ void prefetch_c_l2(const T *C, int64_t ldc, int mm, int nn) {
-    constexpr int kLineElems = 128 / int(sizeof(T));
-    const int lines_per_col = (mm + kLineElems - 1) / kLineElems;
-    for (int e = threadIdx.x; e < lines_per_col * nn; e += kThreads) {
-        const int c = e / lines_per_col, l = e % lines_per_col;
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(C + l * kLineElems + int64_t(c) * ldc));
-    }
-}
-
 // FP64 update items whose operands come by TMA (tma64.cuh): the run carries the tensor maps
 // (single-matrix FP64 runs of suitable geometry), the depth is whole k-slices and both
 // operand blocks start on 16-row atoms.
@@ -681,7 +665,6 @@ __device__ MTD_T64_INLINE int update_tma64(const RunArgs &p, t64::State *s64, vo
                             int mm, int nn, bool lower) {
     t64::Engine<BL> e;
     e.zero();
-    if (MTD_C_PREFETCH) prefetch_c_l2(C, ldc, mm, nn);
     uint8_t *ring = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem) + 1023) & ~uintptr_t(1023));
     // the tensor maps' addresses are taken on the kernel parameter itself
     if (!e.run(s64, ring, p.tmap64_mn, p.tmap64_k, c, p.timeout_ns)) {
@@ -692,10 +675,16 @@ __device__ MTD_T64_INLINE int update_tma64(const RunArgs &p, t64::State *s64, vo
     return 0;
 }
 
+// Called by every thread of an update item between its k-loop and its C update (the
+// scheduler claims its next item there); nothing by default.
+struct NoHook {
+    __device__ __forceinline__ void operator()() const {}
+};
+
 // C -= A B^T   (cublasGemmEx N, T; cholesky_mustard.cu:376)
-template <typename T, int VEC, int SPLIT = 1>
+template <typename T, int VEC, int SPLIT = 1, typename H = NoHook>
 __device__ int op_gemm_nt(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem,
-                          t64::State *s64 = nullptr) {
+                          t64::State *s64 = nullptr, const H &hook = H{}) {
     using Mg = GemmMma<kBNContig, VEC, T, SPLIT>;
     const int nbn = (t.n + kGemmTile - 1) / kGemmTile;
     const int r0 = (item / nbn) * kGemmTile, c0 = (item % nbn) * kGemmTile;
@@ -706,16 +695,16 @@ __device__ int op_gemm_nt(const RunArgs &p, const MatCtx &m, const DevTask &t, i
                                            at<double>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn, false);
     Mg e;
     e.zero();
-    if (MTD_C_PREFETCH) prefetch_c_l2(at<T>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn);
     e.run(smem, at<T>(m, t.ar + r0, t.ac), m.lda, at<T>(m, t.br + c0, t.bc), m.lda, mm, nn, t.k);
+    hook();
     e.sub_from(at<T>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn);
     return 0;
 }
 
 // C -= A B   (cublasGemmEx N, N; lu_mustard.cu:511)
-template <int VEC>
+template <int VEC, typename H = NoHook>
 __device__ int op_gemm_nn(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem,
-                          t64::State *s64 = nullptr) {
+                          t64::State *s64 = nullptr, const H &hook = H{}) {
     using Mg = GemmMma<kBKContig, VEC>;
     const int nbn = (t.n + kGemmTile - 1) / kGemmTile;
     const int r0 = (item / nbn) * kGemmTile, c0 = (item % nbn) * kGemmTile;
@@ -726,16 +715,16 @@ __device__ int op_gemm_nn(const RunArgs &p, const MatCtx &m, const DevTask &t, i
                                            at<double>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn, false);
     Mg e;
     e.zero();
-    if (MTD_C_PREFETCH) prefetch_c_l2(at<double>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn);
     e.run(smem, at<double>(m, t.ar + r0, t.ac), m.lda, at<double>(m, t.br, t.bc + c0), m.lda, mm, nn, t.k);
+    hook();
     e.sub_from(at<double>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn);
     return 0;
 }
 
 // C -= A A^T, lower triangle only   (cublasDsyrk L, N; cholesky_mustard.cu:327)
-template <typename T, int VEC, int SPLIT = 1>
+template <typename T, int VEC, int SPLIT = 1, typename H = NoHook>
 __device__ int op_syrk_ln(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem,
-                          t64::State *s64 = nullptr) {
+                          t64::State *s64 = nullptr, const H &hook = H{}) {
     using Mg = GemmMma<kBNContig, VEC, T, SPLIT>;
     int pb = 0;
     while ((pb + 1) * (pb + 2) / 2 <= item) ++pb;
@@ -748,8 +737,8 @@ __device__ int op_syrk_ln(const RunArgs &p, const MatCtx &m, const DevTask &t, i
                                            at<double>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn, pb == qb);
     Mg e;
     e.zero();
-    if (MTD_C_PREFETCH) prefetch_c_l2(at<T>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn);
     e.run(smem, at<T>(m, t.ar + r0, t.ac), m.lda, at<T>(m, t.ar + c0, t.ac), m.lda, mm, nn, t.k);
+    hook();
     e.sub_from(at<T>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn, pb == qb, 0, 0);
     return 0;
 }

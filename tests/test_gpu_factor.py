@@ -178,10 +178,11 @@ def test_large_lu_against_lapack(mtd):
 
 
 @pytest.mark.parametrize("kind", ["chol", "lu"])
-@pytest.mark.parametrize("n", [1100, 1024])
-def test_cuda_graph_executor_matches_scheduler(mtd, kind, n):
+@pytest.mark.parametrize("n,tma", [(1100, "0"), (1024, "1")])
+def test_cuda_graph_executor_matches_scheduler(mtd, kind, n, tma, monkeypatch):
     # --tiled mode: the same tile kernels as one host-launched CUDA graph (its GEMM items are
-    # always on the cp.async engine; at n = 1024 the scheduler's are TMA-fed).
+    # always on the cp.async engine; at n = 1024 with MTD_TMA64=1 the scheduler's are TMA-fed).
+    monkeypatch.setenv("MTD_TMA64", tma)
     tile = 256
     a = gen.spd_input(n, 6) if kind == "chol" else gen.lu_input(n, 6)
     g = mtd.TaskGraph(mtd.KIND_CHOLESKY if kind == "chol" else mtd.KIND_LU, n, tile).build_tiled().finalize()
@@ -226,9 +227,10 @@ def test_nest_edge_must_be_multiple_of_64(mtd):
 @pytest.mark.parametrize("n,tile,nest", [(1024, 256, 128), (2048, 512, 128), (1040, 384, 128), (1536, 768, 64),
                                          (4096, 1024, 128)])
 def test_tma_fed_updates_match_cp_async_engine(mtd, kind, n, tile, nest, monkeypatch):
-    # FP64 GEMM / SYRK items read their operands by TMA when n, the tile and the nested
-    # sub-tile are multiples of 16; MTD_TMA64=0 keeps the cp.async engine.  Both sum every
-    # element in the same k order, so the factors agree bit for bit (and with the oracle).
+    # With MTD_TMA64=1, FP64 GEMM / SYRK items read their operands by TMA when n, the tile and
+    # the nested sub-tile are multiples of 16; by default they use the cp.async engine.  Both
+    # sum every element in the same k order, so the factors agree bit for bit (and with the
+    # oracle).
     a = gen.spd_input(n, 17) if kind == "chol" else gen.lu_input(n, 17)
     outs = []
     for flag in ("0", "1"):

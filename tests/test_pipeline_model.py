@@ -118,3 +118,130 @@ def test_model_catches_a_parity_bit_not_carried_across_items():
         except AssertionError:
             caught += 1
     assert caught == 6
+
+
+# ---- the warp-specialised pipeline (tcgen05.cuh ws_load / ws_mma / ws_drain) ---------------
+#
+# Three actors share one ring that runs on across items: the loader (thread 0) puts slice g
+# (counted over the CTA's whole run) into stage g % stages once the MMAs of slice g - stages
+# are done (waiting on empty[s] with parity (g / stages - 1) & 1); the MMA thread waits for
+# full[s] with parity (g / stages) & 1, issues the slice's MMAs and commits them to empty[s];
+# after an item's last slice it commits to accf[buf] (buf alternating per item); the drain
+# warps wait on accf[buf] with parity (items drained from buf so far) & 1.  A round ends
+# when the loader has issued the item's slices, the MMA thread its MMAs and the drain warps
+# the previous item's update.  Loads land in any order; commits complete in issue order.
+
+
+def run_ws(items, stages, seed, drop_use_parity=False):
+    rng = random.Random(seed)
+    full = [Barrier() for _ in range(stages)]
+    empty = [Barrier() for _ in range(stages)]
+    accf = [Barrier(), Barrier()]
+    loads, commits = [], []              # in flight
+    holds = [None] * stages              # which slice a stage holds (after its load landed)
+    reading = [None] * stages            # slice whose MMAs are reading the stage
+    st = {"prod": 0, "cons": 0}
+    drained = [0, 0]
+
+    def settle_one():
+        # one asynchronous completion, if any is in flight
+        if loads and (not commits or rng.random() < 0.5):
+            s, label = loads.pop(rng.randrange(len(loads)))
+            assert reading[s] is None, "a load overwrote a stage the MMAs still read"
+            holds[s] = label
+            full[s].completed.append(label)
+            return True
+        if commits:
+            kind, idx, label = commits.pop(0)
+            if kind == "empty":
+                reading[idx] = None
+                empty[idx].completed.append(label)
+            else:
+                accf[idx].completed.append(label)
+            return True
+        return False
+
+    def wait(bar, parity, want):         # a coroutine: yields until the phase completed
+        while not bar.passes(parity):
+            yield
+        assert bar.completed[-1] == want, (bar.completed[-1], want)
+
+    def loader(nk):
+        for _ in range(nk):
+            g, s = st["prod"], st["prod"] % stages
+            if g >= stages:
+                par = 0 if drop_use_parity else ((g // stages) - 1) & 1
+                yield from wait(empty[s], par, ("slice", g - stages))
+            loads.append((s, ("slice", g)))
+            st["prod"] += 1
+            yield
+
+    def mma(nk, buf, it):
+        for _ in range(nk):
+            g, s = st["cons"], st["cons"] % stages
+            yield from wait(full[s], (g // stages) & 1, ("slice", g))
+            assert holds[s] == ("slice", g)
+            reading[s] = ("slice", g)
+            commits.append(("empty", s, ("slice", g)))
+            st["cons"] += 1
+            yield
+        commits.append(("accf", buf, ("item", it)))
+
+    def drain(pending):
+        if pending is None:
+            return
+        pb, pit = pending
+        yield from wait(accf[pb], drained[pb] & 1, ("item", pit))
+        drained[pb] += 1
+
+    def run_round(actors):               # random interleaving of the actors and completions
+        live = list(actors)
+        stalls = 0
+        while live:
+            a = rng.choice(live)
+            try:
+                next(a)
+            except StopIteration:
+                live.remove(a)
+            if rng.random() < 0.5 and settle_one():
+                stalls = 0
+            stalls += 1
+            if stalls > 10_000:
+                while settle_one():
+                    pass
+                assert stalls < 20_000, "deadlock"
+
+    pending = None
+    for it, nk in enumerate(items):
+        buf = it & 1
+        run_round([loader(nk), mma(nk, buf, it), drain(pending)])
+        pending = (buf, it)
+    run_round([drain(pending)])
+    while settle_one():
+        pass
+    assert not loads and not commits
+    return st["prod"], drained
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_ws_pipeline_waits_see_their_own_completions(seed):
+    rng = random.Random(2000 + seed)
+    # slices of 32 (TF32) / 64 (BF16) columns: 48 / 24 at tile 1536, 1 for shallow nested updates
+    items = [rng.choice([1, 2, 3, 5, 6, 7, 12, 24, 48]) for _ in range(30)]
+    prod, drained = run_ws(items, 6, seed)
+    assert prod == sum(items) and sum(drained) == len(items)
+
+
+def test_ws_model_catches_a_wrong_stage_parity():
+    """A mistake planted in the model: the loader waits on empty[s] with parity 0 for every
+    use of the stage.  Some wait then returns on a stale completion, or the load overwrites a
+    stage the MMAs still read."""
+    caught = 0
+    for seed in range(6):
+        rng = random.Random(seed)
+        items = [rng.choice([2, 3, 5, 7, 12]) for _ in range(10)]
+        try:
+            run_ws(items, 6, seed, drop_use_parity=True)
+        except AssertionError:
+            caught += 1
+    assert caught == 6
