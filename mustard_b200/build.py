@@ -22,6 +22,7 @@ CUDA_FLAGS += os.environ.get("MTD_NVCC_EXTRA", "").split()
 
 LIB_SOURCES = ["runtime.cu", "gen.cu", "dag.cpp", "solver.cu", "batch.cu", "adjoint.cu"]
 CLI_PROGRAMS = {"lu_mustard": "lu_mustard.cpp", "cholesky_mustard": "cholesky_mustard.cpp"}
+PROBES = {"dmma_probe": os.path.join(PKG, "probe", "dmma_probe.cu")}  # measurement tools
 
 
 def _newer(target, deps):
@@ -69,6 +70,10 @@ def build(verbose: bool = False, ptxas_verbose: bool = False) -> str:
             _run([NVCC, "-O2", "-std=c++17", "-x", "cu", path, "-o", out,
                   "-I", os.path.join(ROOT, "include"), "-L", LIB_DIR, "-lmustard_b200",
                   "-Xlinker", "-rpath,$ORIGIN/../lib"] + ARCH, verbose)
+    for prog, path in PROBES.items():
+        out = os.path.join(BIN_DIR, prog)
+        if _newer(out, [path]):
+            _run([NVCC, "-O3", "-std=c++17", path, "-o", out] + ARCH, verbose)
     return LIB
 
 

@@ -376,7 +376,10 @@ __device__ __forceinline__ void sync_ws_drain_warps() { asm volatile("bar.sync 2
 // The persistent loop of the tcgen05 kernel on the warp-specialised pipeline (tcgen05.cuh,
 // ws_*).  One item per round, taken from one of two claim slots:
 //   - a TMA item (GEMM_NT / SYRK_LN with TMA operands): thread 0 loads its slices and then
-//     claims the next item into the other slot; thread 32 issues its MMAs into accumulator
+//     tries once to claim the next item into the other slot (never waiting: this item
+//     completes only in the next round, and the work a waiting claim would wait for may be
+//     its successors); if nothing was ready, the next round starts with thread 0 waiting for
+//     an item while warps 2 .. 15 complete this one; thread 32 issues its MMAs into accumulator
 //     `buf`; warps 2 .. 15 first update C from the previous TMA item's accumulator (waiting on
 //     its accf barrier; thread 64 then completes that item) and then prefetch this item's C.
 //     The round ends when all three are done, so the previous item's C update and this
@@ -414,15 +417,24 @@ __device__ __forceinline__ void persistent_loop_ws(const RunArgs &p, double *sme
         }
         pv = false;
     };
-    if (threadIdx.x == 0) {
-        int tk = 0, it = 0;
-        s_cmd[0] = pop_item(p, &tk, &it);
-        s_task[0] = tk;
-        s_item[0] = it;
-    }
+    if (threadIdx.x == 0) s_cmd[0] = kCmdNone;
     __syncthreads();
     for (int r = 0;; ++r) {
-        const int slot = r & 1, cmd = s_cmd[slot], task = s_task[slot], item = s_item[slot];
+        const int slot = r & 1;
+        if (s_cmd[slot] == kCmdNone) {
+            // nothing claimed yet: thread 0 waits for an item while warps 2 .. 15 complete the
+            // pending one, which may be the item that releases the work it waits for
+            if (threadIdx.x == 0) {
+                int tk = 0, it = 0;
+                s_cmd[slot] = pop_item(p, &tk, &it);
+                s_task[slot] = tk;
+                s_item[slot] = it;
+            } else if (warp >= 2) {
+                drain_pending();
+            }
+            __syncthreads();
+        }
+        const int cmd = s_cmd[slot], task = s_task[slot], item = s_item[slot];
         if (cmd != kCmdWork) {
             if (warp >= 2) drain_pending();
             break;
@@ -440,8 +452,10 @@ __device__ __forceinline__ void persistent_loop_ws(const RunArgs &p, double *sme
                 const void *map = path == kTcTmaBf16 ? static_cast<const void *>(p.tmap_bf16) : static_cast<const void *>(p.tmap);
                 if (!tc::ws_load(&ws, ring, map, kind, t.ar + g.r0, g.brow, t.ac, t.k, global_ns() + p.timeout_ns))
                     report_error(p.ctl, MTD_ERR_TIMEOUT, 0);
+                // one attempt, never a wait: this item completes only in the next round, and
+                // what a waiting claim would wait for may be its successors
                 int tk = 0, it = 0;
-                s_cmd[slot ^ 1] = pop_item(p, &tk, &it);
+                s_cmd[slot ^ 1] = claim_item(p, &tk, &it, global_ns());
                 s_task[slot ^ 1] = tk;
                 s_item[slot ^ 1] = it;
             } else if (threadIdx.x == 32) {

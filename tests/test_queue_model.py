@@ -160,6 +160,67 @@ class Model:
                 yield from self.complete(task)
 
 
+    def claim_waiting(self):
+        """pop_item: claim attempts until one succeeds (or the run is over)."""
+        while True:
+            r = yield from self.claim()
+            if r is not None:
+                return r
+            yield
+
+    def cta_ws(self, ws_ops, rng, waiting_claim_in_round=False):
+        """The warp-specialised tcgen05 loop (persistent_loop_ws): an item of a ws kind runs
+        (loads and MMAs) while thread 0 tries once to claim the next item and the drain warps
+        complete the previous ws item, all interleaved; it is itself completed in the next
+        round.  When the attempt found nothing, the next round starts with thread 0 waiting
+        for an item while the drain warps complete the pending one.  Any other item finds
+        nothing pending, runs, completes, then thread 0 waits for the next.  With
+        waiting_claim_in_round (a planted mistake) thread 0 waits for its claim inside the ws
+        round, before the round's own item can complete."""
+        pending, nxt = None, None
+
+        def interleave(gens):
+            results = {}
+            while gens:
+                k = rng.choice(sorted(gens))
+                try:
+                    next(gens[k])
+                except StopIteration as e:
+                    results[k] = e.value
+                    del gens[k]
+                yield
+            return results
+
+        while True:
+            if nxt is None:
+                gens = {"claim": self.claim_waiting()}
+                if pending is not None:
+                    gens["complete"] = self.complete(pending)
+                res = yield from interleave(gens)
+                pending, nxt = None, res["claim"]
+            if nxt == "exit":
+                if pending is not None:
+                    yield from self.complete(pending)
+                return
+            task, item = nxt
+            nxt = None
+            if self.op[task] in ws_ops:
+                gens = {"run": self.run_item(task, item),
+                        "claim": self.claim_waiting() if waiting_claim_in_round else self.claim()}
+                if pending is not None:
+                    gens["complete"] = self.complete(pending)
+                res = yield from interleave(gens)
+                nxt = res["claim"]
+                pending = task
+            else:
+                if pending is not None:
+                    yield from self.complete(pending)
+                    pending = None
+                yield from self.run_item(task, item)
+                yield from self.complete(task)
+                nxt = yield from self.claim_waiting()
+
+
 def cholesky_dag(t):
     """The reference's tiled Cholesky task list (cholesky_mustard.cu:224-395) as tasks with
     items, last-writer predecessors, and the three-queue assignment (0: POTRF/TRSM/SYRK and
@@ -185,15 +246,19 @@ def cholesky_dag(t):
     return tasks, preds, succ
 
 
-def run_model(tasks, preds, succ, n_items, n_ctas, seed, deferred=False, max_steps=2_000_000):
+def run_model(tasks, preds, succ, n_items, n_ctas, seed, deferred=False, max_steps=2_000_000, ws=False,
+              ws_bug=False):
     rng = random.Random(seed)
     m = Model(n_items, succ, [len(p) for p in preds], [q for *_, q in tasks], 3)
     m.op = [op for op, *_ in tasks]
     for r in (i for i, p in enumerate(preds) if not p):  # kernel_populate_queue
         for _ in m.release(r):
             pass
-    ctas = [m.cta_deferred({"GEMM", "SYRK"}, random.Random(seed * 31 + c)) if deferred else m.cta()
-            for c in range(n_ctas)]
+    if ws:
+        ctas = [m.cta_ws({"GEMM", "SYRK"}, random.Random(seed * 37 + c), ws_bug) for c in range(n_ctas)]
+    else:
+        ctas = [m.cta_deferred({"GEMM", "SYRK"}, random.Random(seed * 31 + c)) if deferred else m.cta()
+                for c in range(n_ctas)]
     live = list(range(n_ctas))
     steps = 0
     while live:
@@ -207,14 +272,14 @@ def run_model(tasks, preds, succ, n_items, n_ctas, seed, deferred=False, max_ste
     return m
 
 
-@pytest.mark.parametrize("deferred", [False, True])
-@pytest.mark.parametrize("t,n_ctas,seed", [(3, 2, 1), (4, 4, 2), (5, 8, 3), (6, 3, 4), (6, 16, 5), (2, 1, 6)])
-def test_cholesky_dag_runs_each_item_once_in_dependency_order(t, n_ctas, seed, deferred):
+@pytest.mark.parametrize("mode", ["plain", "deferred", "ws"])
+@pytest.mark.parametrize("t,n_ctas,seed", [(3, 2, 1), (4, 4, 2), (5, 8, 3), (6, 3, 4), (6, 16, 5), (2, 1, 6), (3, 1, 7)])
+def test_cholesky_dag_runs_each_item_once_in_dependency_order(t, n_ctas, seed, mode):
     tasks, preds, succ = cholesky_dag(t)
     rng = random.Random(seed)
     # a few items per task (a join's single no-op item is one of them)
     n_items = [1 if (idx % 7 == 3 and preds[idx]) else rng.randint(1, 3) for idx in range(len(tasks))]
-    m = run_model(tasks, preds, succ, n_items, n_ctas, seed, deferred=deferred)
+    m = run_model(tasks, preds, succ, n_items, n_ctas, seed, deferred=mode == "deferred", ws=mode == "ws")
     want = sorted((tk, i) for tk, n in enumerate(n_items) for i in range(n))
     assert sorted(m.runs) == want                       # every item exactly once
     assert m.tasks_done == len(tasks) and m.done_tasks == set(range(len(tasks)))
@@ -265,3 +330,12 @@ def test_model_detects_a_broken_claim():
             live.remove(i)
     want = sorted((tk, i) for tk, n in enumerate(n_items) for i in range(n))
     assert sorted(m.runs) != want
+
+
+def test_ws_model_catches_a_waiting_claim_inside_the_round():
+    """The mistake the warp-specialised loop first had: thread 0 waited for its next claim
+    inside the round of a TMA item, whose completion comes only in the next round.  On one
+    CTA the last update before a diagonal factorisation then waits for ever."""
+    tasks, preds, succ = cholesky_dag(3)
+    with pytest.raises(AssertionError, match="no termination"):
+        run_model(tasks, preds, succ, [1] * len(tasks), 1, 3, ws=True, ws_bug=True, max_steps=200_000)
