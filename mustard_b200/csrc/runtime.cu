@@ -104,7 +104,9 @@ int smem_setup(int device) {
             cudaFuncSetAttribute(persistent_kernel<VEC, double, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  bytes) != cudaSuccess ||
             cudaFuncSetAttribute(persistent_kernel<VEC, float, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 bytes) != cudaSuccess)
+                                 bytes) != cudaSuccess ||
+            cudaFuncSetAttribute(persistent_kernel<VEC, double, 1, false, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
             return MTD_ERR_CUDA;
         done[device].store(true, std::memory_order_release);
     }
@@ -584,7 +586,8 @@ int launch_run(const RunArgs &a, const int *deps_init, const int *roots, int n_r
         else persistent_kernel<1, float, 3, true><<<grid, kThreads, bytes, s>>>(a);
         return cudaGetLastError() == cudaSuccess ? MTD_OK : MTD_ERR_CUDA;
     }
-    if (fp64 && vec2) persistent_kernel<2, double><<<grid, kThreads, bytes, s>>>(a);
+    if (fp64 && vec2 && a.tma64) persistent_kernel<2, double, 1, false, true><<<grid, kThreads, bytes, s>>>(a);
+    else if (fp64 && vec2) persistent_kernel<2, double><<<grid, kThreads, bytes, s>>>(a);
     else if (fp64) persistent_kernel<1, double><<<grid, kThreads, bytes, s>>>(a);
     else if (x3 && vec2) persistent_kernel<2, float, 3><<<grid, kThreads, bytes, s>>>(a);
     else if (x3) persistent_kernel<1, float, 3><<<grid, kThreads, bytes, s>>>(a);

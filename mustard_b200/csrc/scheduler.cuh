@@ -238,9 +238,9 @@ __device__ __forceinline__ int op_update_tc(const RunArgs &p, const MatCtx &m, c
     return 0;
 }
 
-template <int VEC, typename T, int SPLIT = 1, bool ADJ = false, typename H = NoHook>
+template <int VEC, typename T, int SPLIT = 1, bool ADJ = false>
 __device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int item, void *smem,
-                                        tc::State *tcs = nullptr, t64::State *s64 = nullptr, const H &hook = H{}) {
+                                        tc::State *tcs = nullptr, t64::State *s64 = nullptr) {
     if (t.op == kOpJoin) return 0;  // a join's one item: nothing to compute
     if constexpr (ADJ) return dispatch_adjoint<T, VEC, SPLIT>(p, t, item, smem);
     const MatCtx m = mat_ctx<T>(p, t);
@@ -250,12 +250,12 @@ __device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int 
         switch (t.op) {
         case MTD_OP_POTRF: return op_potrf<T, VEC>(p, m, t, smem);
         case MTD_OP_TRSM_RLT: return op_trsm_rlt<T, VEC>(p, m, t, item, smem);
-        case MTD_OP_SYRK_LN: return op_syrk_ln<T, VEC>(p, m, t, item, smem, s64, hook);
-        case MTD_OP_GEMM_NT: return op_gemm_nt<T, VEC>(p, m, t, item, smem, s64, hook);
+        case MTD_OP_SYRK_LN: return op_syrk_ln<T, VEC>(p, m, t, item, smem, s64);
+        case MTD_OP_GEMM_NT: return op_gemm_nt<T, VEC>(p, m, t, item, smem, s64);
         case MTD_OP_GETRF: return op_getrf<VEC>(p, m, t, smem);
         case MTD_OP_TRSM_LLNU: return op_trsm_llnu<VEC>(p, m, t, item, smem);
         case MTD_OP_TRSM_RUN: return op_trsm_run<VEC>(p, m, t, item, smem);
-        case MTD_OP_GEMM_NN: return op_gemm_nn<VEC>(p, m, t, item, smem, s64, hook);
+        case MTD_OP_GEMM_NN: return op_gemm_nn<VEC>(p, m, t, item, smem, s64);
         default: break;
         }
     } else {
@@ -508,7 +508,9 @@ __device__ __forceinline__ void persistent_loop_ws(const RunArgs &p, double *sme
     }
 }
 
-template <int VEC, typename T, int SPLIT = 1, bool ADJ = false>
+// T64: the instance whose FP64 GEMM / SYRK items may read their operands by TMA (tma64.cuh,
+// runs that carry the tensor maps); the other instances carry none of that code.
+template <int VEC, typename T, int SPLIT = 1, bool ADJ = false, bool T64 = false>
 __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const __grid_constant__ RunArgs p) {
     extern __shared__ __align__(128) double smem[];
     constexpr bool kTc = uses_tcgen05<VEC, T, SPLIT, ADJ>();
@@ -527,56 +529,28 @@ __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const __grid_co
         tc::release(&tcs);
         return;
     } else {
-        // Two claim slots: an update item's thread 0 makes one non-blocking attempt to claim
-        // the CTA's next item between its k-loop and its C update, so the claim's round trip
-        // overlaps the epilogue; without it (nothing ready then, or another kind of item) the
-        // next item is claimed after this one completes, waiting as long as it takes.  The
-        // early attempt never waits: the item it would wait for may be a successor only this
-        // item's completion releases.
-        __shared__ int s_cmd[2], s_task[2], s_item[2], s_early;
+        __shared__ int s_cmd, s_task, s_item;
         // FP64 factorisations: barriers of the TMA-fed GEMM / SYRK items (tma64.cuh), kept
         // for the whole run (the items use them only when the run carries tensor maps)
         __shared__ t64::State s64;
-        constexpr bool kT64 = sizeof(T) == 8 && !ADJ;
+        constexpr bool kT64 = T64 && sizeof(T) == 8 && !ADJ;
         if constexpr (kT64) t64::init(&s64);
-        if (threadIdx.x == 0) {
-            int tk = 0, it = 0;
-            s_cmd[0] = pop_item(p, &tk, &it);
-            s_task[0] = tk;
-            s_item[0] = it;
-            s_early = 0;
-        }
-        __syncthreads();
-        for (int r = 0;; ++r) {
-            const int slot = r & 1, cmd = s_cmd[slot], task = s_task[slot], item = s_item[slot];
+        while (true) {
+            if (threadIdx.x == 0) {
+                int tk = 0, it = 0;
+                s_cmd = pop_item(p, &tk, &it);
+                s_task = tk;
+                s_item = it;
+            }
+            __syncthreads();
+            const int cmd = s_cmd, task = s_task, item = s_item;
             if (cmd != kCmdWork) break;
             const unsigned long long t_start = p.trace ? global_ns() : 0ull;
             DevTask t;
             load_task(p, task, &t);
-            auto early_claim = [&]() {
-                if (threadIdx.x == 0 && !ADJ) {
-                    int tk = 0, it = 0;
-                    if (claim_item(p, &tk, &it, global_ns()) == kCmdWork) {
-                        s_cmd[slot ^ 1] = kCmdWork;
-                        s_task[slot ^ 1] = tk;
-                        s_item[slot ^ 1] = it;
-                        s_early = 1;
-                    }
-                }
-            };
-            const int st = dispatch<VEC, T, SPLIT, ADJ>(p, t, item, smem, nullptr, kT64 ? &s64 : nullptr, early_claim);
+            const int st = dispatch<VEC, T, SPLIT, ADJ>(p, t, item, smem, nullptr, kT64 ? &s64 : nullptr);
             __syncthreads();
-            if (threadIdx.x == 0) {
-                finish_item(p, task, item, t_start, st == 0);
-                if (!s_early) {
-                    int tk = 0, it = 0;
-                    s_cmd[slot ^ 1] = pop_item(p, &tk, &it);
-                    s_task[slot ^ 1] = tk;
-                    s_item[slot ^ 1] = it;
-                }
-                s_early = 0;
-            }
-            __syncthreads();
+            if (threadIdx.x == 0) finish_item(p, task, item, t_start, st == 0);
         }
     }
 }

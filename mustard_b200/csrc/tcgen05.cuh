@@ -300,10 +300,13 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const void *map, int x
 
 // 1: TMA items run on the warp-specialised pipeline (thread 0 loads, thread 32 issues MMAs,
 // warps 2 .. 15 drain accumulators; ws_* below), with 32-deep TF32 / 64-deep BF16 slices of
-// 32 KB in a ring of six stages; 0: the single-thread pipeline (mainloop_tma*) with 64-deep /
-// 128-deep slices of 64 KB in three stages.
+// 32 KB in a ring of six stages; 0 (default): the single-thread pipeline (mainloop_tma*) with
+// 64-deep / 128-deep slices of 64 KB in three stages.  Measured on one B200 (Cholesky,
+// N = 32768, tile 1536): TF32 factor 64.4 ms with the warp-specialised pipeline against
+// 56.3 ms, BF16 59.9 against 49.1 ms -- the items are bound by the operand data rate per SM
+// (~85 GB/s at depth 1536) and by per-item costs the single-thread loop already overlaps.
 #ifndef MTD_TC_WS
-#define MTD_TC_WS 1
+#define MTD_TC_WS 0
 #endif
 
 // TMA pipeline geometry: kTmaBK-deep k-slices (A then B).  An operand slice is 4 MN atoms of

@@ -675,16 +675,10 @@ __device__ MTD_T64_INLINE int update_tma64(const RunArgs &p, t64::State *s64, vo
     return 0;
 }
 
-// Called by every thread of an update item between its k-loop and its C update (the
-// scheduler claims its next item there); nothing by default.
-struct NoHook {
-    __device__ __forceinline__ void operator()() const {}
-};
-
 // C -= A B^T   (cublasGemmEx N, T; cholesky_mustard.cu:376)
-template <typename T, int VEC, int SPLIT = 1, typename H = NoHook>
+template <typename T, int VEC, int SPLIT = 1>
 __device__ int op_gemm_nt(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem,
-                          t64::State *s64 = nullptr, const H &hook = H{}) {
+                          t64::State *s64 = nullptr) {
     using Mg = GemmMma<kBNContig, VEC, T, SPLIT>;
     const int nbn = (t.n + kGemmTile - 1) / kGemmTile;
     const int r0 = (item / nbn) * kGemmTile, c0 = (item % nbn) * kGemmTile;
@@ -696,15 +690,14 @@ __device__ int op_gemm_nt(const RunArgs &p, const MatCtx &m, const DevTask &t, i
     Mg e;
     e.zero();
     e.run(smem, at<T>(m, t.ar + r0, t.ac), m.lda, at<T>(m, t.br + c0, t.bc), m.lda, mm, nn, t.k);
-    hook();
     e.sub_from(at<T>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn);
     return 0;
 }
 
 // C -= A B   (cublasGemmEx N, N; lu_mustard.cu:511)
-template <int VEC, typename H = NoHook>
+template <int VEC>
 __device__ int op_gemm_nn(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem,
-                          t64::State *s64 = nullptr, const H &hook = H{}) {
+                          t64::State *s64 = nullptr) {
     using Mg = GemmMma<kBKContig, VEC>;
     const int nbn = (t.n + kGemmTile - 1) / kGemmTile;
     const int r0 = (item / nbn) * kGemmTile, c0 = (item % nbn) * kGemmTile;
@@ -716,15 +709,14 @@ __device__ int op_gemm_nn(const RunArgs &p, const MatCtx &m, const DevTask &t, i
     Mg e;
     e.zero();
     e.run(smem, at<double>(m, t.ar + r0, t.ac), m.lda, at<double>(m, t.br, t.bc + c0), m.lda, mm, nn, t.k);
-    hook();
     e.sub_from(at<double>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn);
     return 0;
 }
 
 // C -= A A^T, lower triangle only   (cublasDsyrk L, N; cholesky_mustard.cu:327)
-template <typename T, int VEC, int SPLIT = 1, typename H = NoHook>
+template <typename T, int VEC, int SPLIT = 1>
 __device__ int op_syrk_ln(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem,
-                          t64::State *s64 = nullptr, const H &hook = H{}) {
+                          t64::State *s64 = nullptr) {
     using Mg = GemmMma<kBNContig, VEC, T, SPLIT>;
     int pb = 0;
     while ((pb + 1) * (pb + 2) / 2 <= item) ++pb;
@@ -738,7 +730,6 @@ __device__ int op_syrk_ln(const RunArgs &p, const MatCtx &m, const DevTask &t, i
     Mg e;
     e.zero();
     e.run(smem, at<T>(m, t.ar + r0, t.ac), m.lda, at<T>(m, t.ar + c0, t.ac), m.lda, mm, nn, t.k);
-    hook();
     e.sub_from(at<T>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn, pb == qb, 0, 0);
     return 0;
 }
