@@ -134,6 +134,15 @@ struct RunArgs {
     int tma64;
     alignas(64) unsigned char tmap64_mn[128];
     alignas(64) unsigned char tmap64_k[128];
+    // FP32-accurate runs (MTD_PREC_FP32): the low parts of the panels that TRSM items write
+    // (x minus x truncated to TF32, rounded to nearest TF32; column-major, leading dimension
+    // lo_ld), read with the panels themselves by the three-pass tcgen05 updates; its TMA
+    // tensor map (3D like `tmap`, box 32 x 32 x 4) when tma_lo != 0, `tmap` then holding the
+    // matrix's map with the same box.
+    void *lo;
+    int64_t lo_ld;
+    int tma_lo;
+    alignas(64) unsigned char tmap_lo[128];
 };
 
 }  // namespace mtd

@@ -423,6 +423,16 @@ struct BlockMmaT {
         for_each(M, N, [&](int r, int c, T v) { C[r + int64_t(c) * ldc] = __float2bfloat16_rn(float(v)); });
     }
 
+    // C(r, c) = the low part of acc(r, c) for three-pass TF32 products: v minus v truncated to
+    // TF32 (the part a tensor core reading v's bits uses), rounded to nearest TF32.
+    __device__ __forceinline__ void store_lo_to(float *C, int64_t ldc, int M, int N) const {
+        for_each(M, N, [&](int r, int c, T v) {
+            const float x = float(v);
+            const float lo = x - __uint_as_float(__float_as_uint(x) & 0xffffe000u);
+            C[r + int64_t(c) * ldc] = __uint_as_float(to_tf32(lo));
+        });
+    }
+
     // C(r, c) = acc(r, c) as the tensor cores of this mode read it: rounded to nearest TF32
     // for single TF32 products (so later products that truncate their operands see the
     // rounded value), unchanged for FP64 and split-TF32.

@@ -45,6 +45,8 @@ struct mtd_graph {
     int prec = MTD_PREC_FP64;  // element type of the matrix runs factor
     unsigned short *d_bf16 = nullptr;  // MTD_PREC_BF16: BF16 copy of the panels (bf16_ld x n)
     int64_t bf16_ld = 0;
+    float *d_lo = nullptr;  // MTD_PREC_FP32: low parts of the panels (lo_ld x n)
+    int64_t lo_ld = 0;
     Lowered low;   // device form, kept for the CUDA-graph executor and item queries
     int n_dev = 0;
 
@@ -249,6 +251,8 @@ void release_device(mtd_graph *g) {
     cudaFree(g->d_ws_lower);
     cudaFree(g->d_bf16);
     g->d_bf16 = nullptr;
+    cudaFree(g->d_lo);
+    g->d_lo = nullptr;
     cudaFree(g->d_ws_upper);
     cudaFree(g->d_trace);
 }
@@ -425,6 +429,13 @@ int mtd_graph_finalize(mtd_graph *g) {
         g->bf16_ld = (g->dag.n() + 63) & ~int64_t(63);
         rc = rc ? rc : dev_alloc(&g->d_bf16, size_t(g->bf16_ld) * size_t(g->dag.n()));
     }
+    // FP32-accurate runs whose updates can take the three-pass tcgen05 path: the panels' low
+    // parts (the TMA boxes start on 32-row atoms, so n, the tile and the nested sub-tile are
+    // multiples of 32)
+    if (g->prec == MTD_PREC_FP32 && g->dag.n() % 32 == 0 && g->dag.tile() % 32 == 0 && g->nest % 32 == 0) {
+        g->lo_ld = (g->dag.n() + 63) & ~int64_t(63);
+        rc = rc ? rc : dev_alloc(&g->d_lo, size_t(g->lo_ld) * size_t(g->dag.n()));
+    }
     if (g->trace) rc = rc ? rc : dev_alloc(&g->d_trace, size_t(4 * g->trace_cap));
     if (!rc && cudaMallocHost(reinterpret_cast<void **>(&g->h_ctl), sizeof(RunCtl)) != cudaSuccess) {
         g->h_ctl = nullptr;
@@ -442,6 +453,8 @@ int mtd_graph_finalize(mtd_graph *g) {
         // epilogue never stores; keep them finite
         if (g->d_bf16)
             ok = ok && cudaMemset(g->d_bf16, 0, size_t(g->bf16_ld) * size_t(g->dag.n()) * 2) == cudaSuccess;
+        if (g->d_lo)  // rows past n of the last atom are read by TMA; keep them finite
+            ok = ok && cudaMemset(g->d_lo, 0, size_t(g->lo_ld) * size_t(g->dag.n()) * sizeof(float)) == cudaSuccess;
         ok = ok && cudaMemset(g->d_ctl, 0, sizeof(RunCtl)) == cudaSuccess;
         if (!ok) rc = MTD_ERR_CUDA;
     }
@@ -532,6 +545,25 @@ void encode_tmap_bf16(RunArgs &a, void *d16, int64_t n, int64_t ld) {
     a.tma_bf16 = 1;
 }
 
+// 3D TMA map of an FP32 n x n column-major matrix (ld elements; n a multiple of 32): 32 rows of
+// an atom, columns, atoms 128 bytes apart; box 32 x bk x 4 (a 128-row operand slice per load);
+// 128-byte swizzle with 32-byte atoms, zero fill past the matrix.  False without the encoder or
+// on an encoding error.
+bool encode_f32_3d(unsigned char *storage, void *ptr, int64_t n, int64_t ld, int bk) {
+    const PFN_cuTensorMapEncodeTiled_v12000 encode = tmap_encoder();
+    if (!encode || n % 32 != 0 || ld % 4 != 0) return false;
+    CUtensorMap map;
+    const cuuint64_t dims[3] = {32, cuuint64_t(n), cuuint64_t(n / 32)};
+    const cuuint64_t strides[2] = {cuuint64_t(ld) * sizeof(float), 32 * sizeof(float)};
+    const cuuint32_t box[3] = {32, cuuint32_t(bk), 4}, elem[3] = {1, 1, 1};
+    if (encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, ptr, dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    std::memcpy(storage, &map, sizeof(map));
+    return true;
+}
+
 // TMA tensor maps of an FP64 n x n column-major matrix (ld elements) for the FP64 GEMM /
 // SYRK items (tma64.cuh): 3D {16 rows of an atom, columns, atoms} with box {16, 16, 8} for
 // m- / n-contiguous operands, 2D {rows, columns} with box {16, 128} for the k-contiguous
@@ -617,6 +649,16 @@ static int run_persistent(mtd_graph *g, void *dA, int64_t lda, void *stream, int
     // the others keep the TF32 path on the FP32 matrix
     if (g->prec == MTD_PREC_BF16 && vec2 && g->dag.tile() % 64 == 0 && g->nest % 64 == 0)
         mtd::encode_tmap_bf16(a, g->d_bf16, g->dag.n(), g->bf16_ld);
+    // FP32-accurate runs: the three-pass tcgen05 updates read the matrix and its low parts by
+    // TMA (boxes of 32-deep slices); the TRSM items write the low parts only then
+    if (g->prec == MTD_PREC_FP32 && g->d_lo && vec2 && g->dag.n() % 32 == 0 &&
+        mtd::encode_f32_3d(a.tmap, dA, g->dag.n(), lda, tc::kX3BK) &&
+        mtd::encode_f32_3d(a.tmap_lo, g->d_lo, g->dag.n(), g->lo_ld, tc::kX3BK)) {
+        a.tma = tc::kTmaMap3D;
+        a.lo = g->d_lo;
+        a.lo_ld = g->lo_ld;
+        a.tma_lo = 1;
+    }
     // FP64 GEMM / SYRK items read their operands by TMA when every operand block starts on a
     // 16-row atom (tile and nested sub-tile edges multiples of 16)
     if (g->prec == MTD_PREC_FP64 && vec2 && g->dag.tile() % 16 == 0 && g->nest % 16 == 0 && g->use_tma64)

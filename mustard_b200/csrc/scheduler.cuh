@@ -166,7 +166,7 @@ __device__ __forceinline__ void finish_item(const RunArgs &p, int task, int item
 // fifth-generation tensor cores (tcgen05, accumulator in TMEM); everything else on mma.sync.
 template <int VEC, typename T, int SPLIT, bool ADJ>
 constexpr bool uses_tcgen05() {
-    return VEC == 2 && sizeof(T) == 4 && SPLIT == 1 && !ADJ;
+    return VEC == 2 && sizeof(T) == 4 && (SPLIT == 1 || SPLIT == 3) && !ADJ;
 }
 
 // One 128 x 128 output tile of C -= A B^T (GEMM_NT) or of the lower part of C -= A A^T
@@ -203,7 +203,7 @@ __device__ __forceinline__ UpdateGeom update_geom(const DevTask &t, int item) {
     return g;
 }
 
-enum { kTcStaged = 0, kTcTmaTf32 = 1, kTcTmaBf16 = 2 };
+enum { kTcStaged = 0, kTcTmaTf32 = 1, kTcTmaBf16 = 2, kTcTmaX3 = 3 };
 
 // How a GEMM_NT / SYRK_LN item runs on tcgen05: BF16 operands from the BF16 copy of the
 // panels when the depth is whole 128-column stages and both operand slices start on 64-row
@@ -211,6 +211,9 @@ enum { kTcStaged = 0, kTcTmaTf32 = 1, kTcTmaBf16 = 2 };
 // stages; otherwise staged by cp.async.
 __device__ __forceinline__ int tc_path(const RunArgs &p, const DevTask &t, const UpdateGeom &g, bool tmap) {
     if (t.op != MTD_OP_GEMM_NT && t.op != MTD_OP_SYRK_LN) return kTcStaged;
+    if (p.tma_lo)  // FP32-accurate runs: three passes, both operand slices on 32-row atoms
+        return (t.k % tc::kX3BK == 0 && t.ac == g.bcol && (t.ar + g.r0) % 32 == 0 && g.brow % 32 == 0) ? kTcTmaX3
+                                                                                                     : kTcStaged;
     if (p.tma_bf16 && t.k % tc::kBfBK == 0 && t.ac == g.bcol && (t.ar + g.r0) % 64 == 0 && g.brow % 64 == 0)
         return kTcTmaBf16;
     if (tmap && t.k % tc::kTmaBK == 0 && t.ac == g.bcol) return kTcTmaTf32;
@@ -244,7 +247,9 @@ __device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int 
     if (t.op == kOpJoin) return 0;  // a join's one item: nothing to compute
     if constexpr (ADJ) return dispatch_adjoint<T, VEC, SPLIT>(p, t, item, smem);
     const MatCtx m = mat_ctx<T>(p, t);
-    if constexpr (uses_tcgen05<VEC, T, SPLIT, ADJ>())
+    // single-pass TF32 runs stage their other updates for tcgen05 too; FP32-accurate runs keep
+    // them on the three-product mma.sync path
+    if constexpr (uses_tcgen05<VEC, T, SPLIT, ADJ>() && SPLIT == 1)
         if (t.op == MTD_OP_GEMM_NT || t.op == MTD_OP_SYRK_LN) return op_update_tc(p, m, t, item, smem, tcs);
     if constexpr (sizeof(T) == 8) {
         switch (t.op) {
@@ -332,11 +337,15 @@ __device__ __forceinline__ void persistent_loop_tc(const RunArgs &p, double *sme
             if (threadIdx.x == 0) {
                 const uint32_t acc = tcs.taddr + tc::kAccCols * s_buf;
                 // the tensor maps' addresses are taken on the kernel parameter itself
-                const bool ok = path == kTcTmaBf16
-                                    ? tc::mainloop_tma_bf16(&tcs, tc_stages(smem), p.tmap_bf16, t.ar + g.r0, g.brow,
-                                                            t.ac, t.k, acc, p.timeout_ns)
-                                    : tc::mainloop_tma(&tcs, tc_stages(smem), p.tmap, p.tma, t.ar + g.r0, g.brow,
-                                                       t.ac, t.k, acc, p.timeout_ns);
+                const bool ok =
+                    path == kTcTmaBf16
+                        ? tc::mainloop_tma_bf16(&tcs, tc_stages(smem), p.tmap_bf16, t.ar + g.r0, g.brow, t.ac, t.k, acc,
+                                                p.timeout_ns)
+                    : path == kTcTmaX3
+                        ? tc::mainloop_tma_x3(&tcs, tc_stages(smem), p.tmap, p.tmap_lo, t.ar + g.r0, g.brow, t.ac, t.k,
+                                              acc, p.timeout_ns)
+                        : tc::mainloop_tma(&tcs, tc_stages(smem), p.tmap, p.tma, t.ar + g.r0, g.brow, t.ac, t.k, acc,
+                                           p.timeout_ns);
                 if (ok) {
                     pend.C = C;
                     pend.ldc = m.lda;
@@ -443,7 +452,8 @@ __device__ __forceinline__ void persistent_loop_ws(const RunArgs &p, double *sme
         DevTask t;
         load_task(p, task, &t);
         const UpdateGeom g = update_geom(t, item);
-        const int path = tc_path(p, t, g, p.tma != 0);
+        int path = tc_path(p, t, g, p.tma != 0);
+        if (path == kTcTmaX3) path = kTcStaged;  // three-pass items run on the single-thread pipeline only
         if (path != kTcStaged) {
             const MatCtx m = mat_ctx<T>(p, t);
             float *C = at<float>(m, t.cr + g.r0, t.cc + g.c0);

@@ -689,6 +689,90 @@ __device__ __forceinline__ void ws_drain(uint32_t acc, float *C, int64_t ldc, in
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 }
 
+// FP32-accurate updates: C -= A B^T as A_h B_h^T + A_h B_l^T + A_l B_h^T, three TF32 passes
+// (tcgen05.mma kind::tf32, FP32 accumulation in TMEM).  A_h, B_h are the panels as stored
+// (full FP32 values: the tensor core reads their TF32 part, i.e. truncates them); A_l, B_l
+// come from the low-part copy the TRSM items write (x - trunc(x), rounded to nearest TF32, so
+// the tensor core reads it exactly).  A stage holds 32-deep slices of the four operands (16 KB
+// each, the TF32 layout of mainloop_tma with 4 KB atoms): 64 KB, three stages; 4 x 3 MMAs.
+// `map` / `map_lo`: 3D maps of the matrix and of the low copy, box 32 x 32 x 4.  a_row, b_row
+// multiples of 32, K a multiple of 32; otherwise as mainloop_tma (thread 0 alone, into `acc`).
+constexpr int kX3BK = 32;
+constexpr int kX3Stages = 3;
+constexpr int kX3AtomBytes = 32 * kX3BK * 4;              // 4 KB
+constexpr int kX3OperandBytes = 4 * kX3AtomBytes;         // 16 KB
+constexpr int kX3StageBytes = 4 * kX3OperandBytes;        // 64 KB
+static_assert(kX3Stages * kX3StageBytes <= kSmemBytes, "three-pass stages fit the engine's shared memory");
+static_assert(kX3Stages <= kStages, "three-pass stages use the engine's barriers");
+
+__device__ bool mainloop_tma_x3(State *st, uint8_t *smem, const void *map, const void *map_lo, int a_row, int b_row,
+                                int k0, int K, uint32_t acc, unsigned long long timeout_ns) {
+    bool ok = true;
+    {
+        const unsigned long long deadline = now_ns() + timeout_ns;
+        const int nk = K / kX3BK;
+        uint32_t ph = st->phases, fph = st->fphases;
+        asm volatile("fence.proxy.async.global;" ::: "memory");  // see mainloop_tma
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        auto issue = [&](int s, int kt) {
+            const uint32_t bar = smem_addr(&st->full[s]), base = smem_addr(smem + s * kX3StageBytes);
+            const int k = k0 + kt * kX3BK;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kX3StageBytes)
+                         : "memory");
+            tma_load_3d(base, map, 0, k, a_row >> 5, bar);
+            tma_load_3d(base + kX3OperandBytes, map, 0, k, b_row >> 5, bar);
+            tma_load_3d(base + 2 * kX3OperandBytes, map_lo, 0, k, a_row >> 5, bar);
+            tma_load_3d(base + 3 * kX3OperandBytes, map_lo, 0, k, b_row >> 5, bar);
+        };
+        for (int s = 0; s < kX3Stages && s < nk; ++s) issue(s, s);
+        for (int kt = 0; kt < nk && ok; ++kt) {
+            const int s = kt % kX3Stages;
+            ok = wait_bar(&st->full[s], (fph >> s) & 1u, deadline);
+            fph ^= 1u << s;
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t ah0 = smem_addr(smem + s * kX3StageBytes), bh0 = ah0 + kX3OperandBytes,
+                           al0 = ah0 + 2 * kX3OperandBytes, bl0 = ah0 + 3 * kX3OperandBytes;
+            const uint64_t lead = uint64_t(kX3AtomBytes >> 4) << 16, stride = uint64_t(512 >> 4) << 32;
+            auto desc = [&](uint32_t a) {
+                return uint64_t((a >> 4) & 0x3fff) | lead | stride | (1ull << 46) | (1ull << 61);
+            };
+#pragma unroll
+            for (int q = 0; q < kX3BK / 8; ++q) {
+                const uint64_t ah = desc(ah0 + q * 1024), bh = desc(bh0 + q * 1024), al = desc(al0 + q * 1024),
+                               bl = desc(bl0 + q * 1024);
+                const uint32_t first = (kt > 0 || q > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p, q;\n\t"
+                    "setp.ne.b32 p, %6, 0;\n\t"
+                    "setp.eq.b32 q, %6, %6;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %5, p;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %3, %5, q;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %4, %2, %5, q;\n\t}" ::"r"(acc),
+                    "l"(ah), "l"(bh), "l"(bl), "l"(al), "r"(kIdescTf32), "r"(first)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_addr(&st->mbar[s]))
+                         : "memory");
+            if (kt > 0 && kt - 1 + kX3Stages < nk) {
+                const int sp = (kt - 1) % kX3Stages;
+                ok = wait_bar(&st->mbar[sp], (ph >> sp) & 1u, deadline);
+                ph ^= 1u << sp;
+                if (ok) issue(sp, kt - 1 + kX3Stages);
+            }
+        }
+        for (int kt = nk > kX3Stages ? nk - kX3Stages : 0; kt < nk && ok; ++kt) {
+            const int s = kt % kX3Stages;
+            ok = wait_bar(&st->mbar[s], (ph >> s) & 1u, deadline);
+            ph ^= 1u << s;
+        }
+        st->phases = ph;
+        st->fphases = fph;
+    }
+    return ok;
+}
+
 // A TMA item whose accumulator is final but whose update of C is still to be done.
 struct Pending {
     float *C;

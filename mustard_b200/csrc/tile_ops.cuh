@@ -576,6 +576,9 @@ __device__ int op_trsm_rlt(const RunArgs &p, const MatCtx &m, const DevTask &t, 
             if (p.bf16)  // BF16-update runs: the updates read the panel from its BF16 copy
                 e.store_bf16_to(static_cast<__nv_bfloat16 *>(p.bf16) + (t.cr + r0) + int64_t(t.cc + jb) * p.bf16_ld,
                                 p.bf16_ld, mm, jn);
+        if constexpr (sizeof(T) == 4 && SPLIT == 3)
+            if (p.lo)  // FP32-accurate runs: the three-pass updates read the panel's low part
+                e.store_lo_to(static_cast<float *>(p.lo) + (t.cr + r0) + int64_t(t.cc + jb) * p.lo_ld, p.lo_ld, mm, jn);
         block_fence_sync();
     }
     return 0;

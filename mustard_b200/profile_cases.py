@@ -9,7 +9,8 @@
         a whole tiled factorisation
     python -m mustard_b200.profile_cases gemm --n 8192 --tile 1024 --prec tf32
         the same cases on a float32 matrix with TF32 tensor-core products (tcgen05 GEMM /
-        SYRK items fed by TMA; Cholesky and the GEMM-only step only)
+        SYRK items fed by TMA; Cholesky and the GEMM-only step only); --prec bf16 (BF16
+        updates) and --prec fp32 (FP32-accurate: three TF32 passes) likewise
 
 Each case runs `--runs` launches (default 2: the first is the one to capture with
 `-c 1`), checks the run status, and prints the device time of the last launch.  With
@@ -58,7 +59,7 @@ def main():
     ap.add_argument("--n", type=int, default=6144)
     ap.add_argument("--tile", type=int, default=768)
     ap.add_argument("--runs", type=int, default=2)
-    ap.add_argument("--prec", choices=["fp64", "tf32", "bf16"], default="fp64")
+    ap.add_argument("--prec", choices=["fp64", "tf32", "bf16", "fp32"], default="fp64")
     ap.add_argument("--trace", action="store_true", help="per-operation item-time breakdown")
     ap.add_argument("--trace-out", default=None,
                     help="also write the records, task spans and critical path to this JSON file")
@@ -86,7 +87,7 @@ def main():
                 g.add_task(mtd.OP_GEMM_NT, (j, i), [(j, i), (j, 0), (i, 0)])
                 flops += 2.0 * ext[j] * ext[i] * ext[0]
     if args.prec != "fp64":
-        g.set_precision(mtd.PREC_TF32 if args.prec == "tf32" else mtd.PREC_BF16)
+        g.set_precision({"tf32": mtd.PREC_TF32, "bf16": mtd.PREC_BF16, "fp32": mtd.PREC_FP32}[args.prec])
         a = a.t().contiguous().float().t()
     if args.trace_out:
         args.trace = True

@@ -193,3 +193,48 @@ def test_bf16_factor_refines_to_fp64_accuracy(mtd, method):
     assert mixed.backward_error(a, x, b) <= 2e-13
     assert mixed.forward_error(x, mixed.solve_fp64(a, b)) <= 1e2 * 1e-12
     s.close()
+
+
+@pytest.mark.parametrize("n,tile,nest", [(1536, 512, 128), (2048, 384, 64), (1024, 256, 128)])
+def test_fp32_three_pass_factor_accuracy(mtd, n, tile, nest):
+    """MTD_PREC_FP32 with n, the tile and the nested sub-tile multiples of 32: the GEMM / SYRK
+    items run three TF32 passes on tcgen05 (panel x panel + panel x low part + low part x
+    panel, the low parts written by the TRSM items); the factor is FP32-accurate, two orders
+    of magnitude closer to LAPACK's FP64 factor than the single-pass TF32 one."""
+    import torch
+    a = gen.spd_input(n, 3)
+    ref = np.tril(tiled.cholesky_lapack(a))
+    errs = {}
+    for prec in (mtd.PREC_TF32, mtd.PREC_FP32):
+        g = mtd.TaskGraph(mtd.KIND_CHOLESKY, n, tile).build_tiled().set_precision(prec)
+        g.set_nest(nest).finalize()
+        d = torch.from_numpy(np.ascontiguousarray(a.T).astype(np.float32)).cuda().t()
+        assert g.run_f32(d) == 0
+        l32 = np.tril(np.asfortranarray(d.t().contiguous().cpu().numpy().T).astype(np.float64))
+        errs[prec] = rel_diff(l32, ref)
+        # a second run on the same graph (barrier parities and the low copy reused)
+        d = torch.from_numpy(np.ascontiguousarray(a.T).astype(np.float32)).cuda().t()
+        assert g.run_f32(d) == 0
+        assert rel_diff(np.tril(np.asfortranarray(d.t().contiguous().cpu().numpy().T).astype(np.float64)), ref) \
+            == errs[prec]
+        g.close()
+    assert errs[mtd.PREC_FP32] < 3e-6, errs
+    assert errs[mtd.PREC_FP32] * 100 < errs[mtd.PREC_TF32], errs
+
+
+def test_fp32_three_pass_ir_kappa_1e5(mtd):
+    """kappa = 1e5 (kappa u_TF32 ~ 50: a single-pass TF32 factor is at the edge of breaking
+    down): the FP32-accurate factor refines by plain IR to FP64 backward error."""
+    n, tile = 2048, 512
+    a = mixed.spd_kappa(n, 1e5, 10)
+    b = mixed.rhs(n, 1, 11)
+    s = mtd.SpdSolver(n, tile, mtd.PREC_FP32)
+    assert s.factor(to_dev(a)) == 0
+    xd = _dev_rect(np.zeros((n, 1)))
+    st = s.solve(_dev_rect(b), xd, method=mtd.REFINE_IR, tol=1e-13, max_iter=30)
+    x = _host_rect(xd)
+    assert st["converged"] and st["backward_error"] <= 1e-13, st
+    assert st["iterations"] <= 20, st
+    assert mixed.backward_error(a, x, b) <= 2e-13
+    assert mixed.forward_error(x, mixed.solve_fp64(a, b)) <= 1e5 * 1e-12
+    s.close()
