@@ -21,9 +21,10 @@ cpu_baseline= host LAPACK dgetrf + dpotrf (scipy's OpenBLAS, all host cores) on 
 parity      = the factors of one more LU and Cholesky (after the timed steps) checked on the
               device (probe residual ||(A - LU) X|| / ||A X|| over 8 random columns) and
               against LAPACK's factors of the same inputs (max |diff| / max |LAPACK|).
-reference_gpu (opt-in, --reference-gpu) = the reference's own 1-rank build (oracle/_ref/,
-              built from its sources by oracle/ref/Makefile) timed on the same GPU in its
-              --subgraph and single-cuSOLVER-call modes, at N = 24000.
+reference_gpu = the reference's own 1-rank build (oracle/_ref/, built from its sources by
+              oracle/ref/Makefile) timed on the same GPU in its --subgraph (T = 6) and
+              single-cuSOLVER-call modes at N = 24000, with our rate over its per kind
+              (skip with --no-reference-gpu).
 mixed_ir    = time-to-solution of an FP64-accurate SPD solve at the same N (rank 0, after
               the timed steps): plain FP64 Cholesky + solve against a TF32 tensor-core
               factor + FP64 iterative refinement to normwise backward error 1e-13; the
@@ -223,16 +224,16 @@ def to_host(t):
 
 def reference_gpu_baseline(n, timeout):
     """The reference's own 1-rank build on this GPU (oracle/_ref/lu_mustard, cholesky_mustard):
-    its device-side scheduler (--subgraph) at T = 6 (and T = 8 for Cholesky: 120 tasks, the
-    most its scheduler's device graph launches allow) with its default and the published SM
-    limit, and its single cuSOLVER call; 4 runs each, run 0 dropped as its own scripts do."""
+    its device-side scheduler (--subgraph) at T = 6 with its default SM limit, and its single
+    cuSOLVER call -- the fastest settings of each in the full sweep -- on its own input
+    (include/gen.h); 4 runs each, run 0 dropped as its own scripts do."""
     from oracle import reference_gpu as rg
     if not rg.available():
         return {"unavailable": "the reference's drivers are not built (oracle/ref/Makefile)"}
     out = {"runs": []}
-    plan = [("lu", 6, "subgraph", 20), ("lu", 6, "subgraph", 100), ("lu", 1, "single", 20),
-            ("chol", 6, "subgraph", 20), ("chol", 8, "subgraph", 20), ("chol", 6, "subgraph", 100),
-            ("chol", 1, "single", 20)]
+    # the best of each mode in the full sweep on a B200 (profiles/reference_gpu_n24000.md):
+    # --subgraph at T = 6 with the default SM limit, and the single cuSOLVER call
+    plan = [("lu", 6, "subgraph", 20), ("lu", 1, "single", 20), ("chol", 6, "subgraph", 20), ("chol", 1, "single", 20)]
     for kind, t, mode, sm in plan:
         if n % t:
             continue
@@ -338,8 +339,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=60.0,
                     help="stop the LAPACK runs once this many seconds are spent (at least one run)")
     ap.add_argument("--no-parity", action="store_true", help="skip the parity checks after the timed steps")
-    ap.add_argument("--reference-gpu", action="store_true",
-                    help="also time the reference's own 1-rank build on this GPU (oracle/_ref)")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own 1-rank build on this GPU (oracle/_ref)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer measurement")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision + IR comparison")
     ap.add_argument("--mixed-kappa", type=float, default=1e2)
@@ -603,10 +604,20 @@ def main():
             mixed["bf16_ir"] = {"error": f"{type(e).__name__}: {e}"}
 
     ref_gpu = None
-    if rank == 0 and args.reference_gpu:
+    if rank == 0 and not args.no_reference_gpu and args.only is None:
         torch.cuda.synchronize()
         torch.cuda.empty_cache()  # the reference's process needs its own device memory
         ref_gpu = reference_gpu_baseline(n, timeout=300)
+        ours = {"lu": roofline["lu_tflops"], "chol": roofline["chol_tflops"]}
+        ratios = {}
+        for kind in ("lu", "chol"):
+            for key in (f"{kind}_best", f"{kind}_subgraph_best"):
+                if key in ref_gpu:
+                    ratios[key] = ours[kind] / ref_gpu[key]["tflops_mean"]
+        if "lu_best" in ref_gpu and "chol_best" in ref_gpu:  # one step = one LU + one Cholesky
+            ref_step_s = ref_gpu["lu_best"]["mean_s"] + ref_gpu["chol_best"]["mean_s"]
+            ratios["step_vs_best"] = ref_step_s / (dev_ms * 1e-3)
+        ref_gpu["ours_over_reference"] = ratios
 
     if rank == 0:
         line = {
