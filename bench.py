@@ -28,7 +28,8 @@ reference_gpu = the reference's own 1-rank build (oracle/_ref/, built from its s
 mixed_ir    = time-to-solution of an FP64-accurate SPD solve at the same N (rank 0, after
               the timed steps): plain FP64 Cholesky + solve against a TF32 tensor-core
               factor + FP64 iterative refinement to normwise backward error 1e-13; the
-              same with BF16 updates beside it (`bf16_ir`).
+              same with BF16 updates beside it (`bf16_ir`), and at condition number 1e5 the
+              FP32-accurate factor (three TF32 passes) + IR (`kappa_1e5`).
 
 `--impl reference` times the oracle's restatement of the reference's tiled algorithm (scipy /
 OpenBLAS tile calls, all host cores) alone, on a bounded sample N = --cpu-n that its config
@@ -602,6 +603,22 @@ def main():
                                 "ratio_vs_fp64": bf.get("ratio_vs_fp64")}
         except Exception as e:  # a side report: the line above stands without it
             mixed["bf16_ir"] = {"error": f"{type(e).__name__}: {e}"}
+        # kappa = 1e5 (config 2's middle case): single-pass TF32 / BF16 factors are at or past
+        # breakdown there; the FP32-accurate factor (three TF32 passes on tcgen05) + FP64 IR
+        try:
+            recs5 = mixed_bench.run_case(n, args.tile_chol, 1e5, 1, args.seed, [(mtd.PREC_FP32, mtd.REFINE_IR, 0.0)],
+                                         1e-13, 30, 2)
+            f64, f32 = recs5[0], recs5[1]
+            mixed["kappa_1e5"] = {
+                "workload": f"as above with kappa 1e5, N={n}",
+                "fp64_time_to_solution_ms": f64["time_to_solution_ms"],
+                "fp32_3pass_ir": {"time_to_solution_ms": f32.get("time_to_solution_ms"),
+                                  "iterations": f32.get("iterations"), "backward_error": f32.get("backward_error"),
+                                  "converged": f32.get("converged"), "factor_ms": f32.get("factor_ms"),
+                                  "forward_error_vs_fp64": f32.get("forward_error_vs_fp64")},
+                "ratio_vs_fp64": f32.get("ratio_vs_fp64")}
+        except Exception as e:
+            mixed["kappa_1e5"] = {"error": f"{type(e).__name__}: {e}"}
 
     ref_gpu = None
     if rank == 0 and not args.no_reference_gpu and args.only is None:
