@@ -35,6 +35,12 @@
 
 namespace mtd {
 
+// 1: BlockMmaT::run refills a stage right after the slice barrier, before that slice's
+// compute; 0: after it.
+#ifndef MTD_EARLY_ISSUE
+#define MTD_EARLY_ISSUE 0
+#endif
+
 enum { kBNContig = 0, kBKContig = 1 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -344,6 +350,21 @@ struct BlockMmaT {
             cp_async_wait<STAGES - 2>();
             __syncthreads();
             const int st = kt % STAGES;
+#if MTD_EARLY_ISSUE
+            // the stage slice kt + STAGES - 1 goes into was read in iteration kt - 1, which every
+            // thread has finished (the barrier above): refill it before this slice's compute, so
+            // the copies have STAGES - 1 compute phases to land
+            {
+                const int nk = kt + STAGES - 1;
+                if (nk < ktiles) {
+                    const int ns = nk % STAGES;
+                    load_a(As + ns * A_STAGE, A, lda, M, K, nk * BK);
+                    load_b(Bs + ns * B_STAGE, B, ldb, N, K, nk * BK);
+                }
+                cp_async_commit();
+            }
+            compute_stage(As + st * A_STAGE, Bs + st * B_STAGE);
+#else
             compute_stage(As + st * A_STAGE, Bs + st * B_STAGE);
             const int nk = kt + STAGES - 1;
             if (nk < ktiles) {
@@ -352,6 +373,7 @@ struct BlockMmaT {
                 load_b(Bs + ns * B_STAGE, B, ldb, N, K, nk * BK);
             }
             cp_async_commit();
+#endif
         }
         cp_async_wait<0>();
         __syncthreads();
