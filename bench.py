@@ -259,6 +259,7 @@ def reference_gpu_baseline(n, timeout):
 # FP64 kernel sources whose DRAM traffic `roofline.traffic` reports; the figure comes from
 # one ncu capture and is reported only while these files still hash to the captured state.
 TRAFFIC_SOURCES = ["mustard_b200/csrc/scheduler.cuh", "mustard_b200/csrc/mma.cuh", "mustard_b200/csrc/tile_ops.cuh",
+                   "mustard_b200/csrc/tma64.cuh", "mustard_b200/csrc/tcgen05.cuh", "mustard_b200/csrc/adjoint_ops.cuh",
                    "mustard_b200/csrc/device_types.hpp", "mustard_b200/csrc/dag.cpp"]
 
 
@@ -317,7 +318,7 @@ def run_reference(args, rank, world):
 # The ncu capture behind roofline.traffic (profiles/dram_traffic_bench_n24000_t1536.md):
 # DRAM read + write bytes of one step's two launches, and the hash of the FP64 kernel
 # sources it measured.
-TRAFFIC_CAPTURE = {"sources_sha16": "", "bytes": 76424422400 + 35419470336 + 39205473280 + 17637506560}
+TRAFFIC_CAPTURE = {"sources_sha16": "b86497b519d2a1c0", "bytes": 75478524672 + 33292412928 + 36982104576 + 16762892544}
 
 METRIC = "FP64-accurate LU/Cholesky TFLOP/s, N=24000, 1 B200: mixed+IR vs plain FP64"
 
