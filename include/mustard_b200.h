@@ -288,7 +288,7 @@ int mtd_solver_destroy(mtd_solver *s);
 typedef struct mtd_batch mtd_batch;
 
 typedef struct mtd_batch_solve_stats {
-    int iterations;            /* refinement steps (1 = the direct FP64 solve only)     */
+    int iterations;            /* solves applied: FP64 1 + corrections; low: corrections */
     int converged_count;       /* matrices whose backward error reached tol             */
     double max_backward_error; /* max over matrices and columns (FP64), -1 if not known */
     double solve_ms;           /* host wall time of the solve call                      */
@@ -312,6 +312,50 @@ int mtd_batch_convert(mtd_batch *b, const double *const *dA, const int64_t *lda,
 int mtd_batch_solve(mtd_batch *b, const double *const *dA, const int64_t *lda, void *const *dF, const int64_t *ldf,
                     const double *const *dB, const int64_t *ldb, double *const *dX, const int64_t *ldx,
                     const int *nrhs, int method, double tol, int max_iter, void *stream, mtd_batch_solve_stats *stats);
+/* Factor AND solve in ONE persistent launch (stream-ordered, no host synchronisation: it
+ * can be captured into a CUDA graph).  The launch's task graph is the merged factorisation
+ * DAG plus, per matrix, a solve task after its last factor task (one CTA: the whole solve
+ * with its refinement steps, as mtd_batch_solve's launches do them) and, for low-precision
+ * batches, a conversion task before its first (dF[m] = lower(dA[m]) + shift I, rounded to
+ * float: dF needs no initialisation).  So one matrix's solve overlaps the other matrices'
+ * factorisations.  FP64 batches factor dF[m] in place; dA (the FP64 matrices, for the
+ * residuals) may then be NULL with MTD_REFINE_NONE.  Low-precision batches need dA and
+ * MTD_REFINE_IR.  Results: mtd_batch_solve_status. */
+int mtd_batch_factor_solve(mtd_batch *b, void *const *dF, const int64_t *ldf, const double *const *dA,
+                           const int64_t *lda, const double *const *dB, const int64_t *ldb, double *const *dX,
+                           const int64_t *ldx, const int *nrhs, int method, double tol, int max_iter, double shift,
+                           void *stream);
+/* Wait for the last mtd_batch_factor_solve.  Per matrix (each array nullable): info as
+ * mtd_batch_status, latency_ms up to the end of its solve, berr = its normwise backward error
+ * (max over its columns; -1 without dA; NaN if its factorisation failed), iterations = the
+ * solves applied.  stats: max iterations, matrices with berr <= tol, the max berr, and
+ * solve_ms = the launch's device time (first work to last matrix done). */
+int mtd_batch_solve_status(mtd_batch *b, int *info, double *latency_ms, double *berr, int *iterations,
+                           mtd_batch_solve_stats *stats);
+/* CTA-to-task schedule of the batch's launches: the order in which the matrices' first
+ * tasks enter the ready queues (MTD_BATCH_ORDER_*; the queues are FIFO, so it is the order
+ * in which the 148 CTAs start the matrices), ORed with MTD_BATCH_SOLVE_LATE to queue the
+ * solve tasks of mtd_batch_factor_solve behind all factor work instead of ahead of it. */
+enum {
+    MTD_BATCH_ORDER_INPUT = 0,
+    MTD_BATCH_ORDER_LARGEST_FIRST = 1,
+    MTD_BATCH_ORDER_SMALLEST_FIRST = 2,
+    MTD_BATCH_SOLVE_LATE = 4,
+    MTD_BATCH_NUM_SCHEDULES = 6 /* candidates the schedule tuner times: 3 orders x 2 */
+};
+int mtd_batch_set_schedule(mtd_batch *b, int schedule);
+int mtd_batch_get_schedule(const mtd_batch *b);
+/* Schedule tuner: times mtd_batch_factor_solve (arguments as there) under each of the
+ * MTD_BATCH_NUM_SCHEDULES schedules (candidate c = (c / 2) | (c % 2 ? MTD_BATCH_SOLVE_LATE :
+ * 0)), `reps` timed launches each after one untimed, and keeps the fastest (set on the
+ * batch and returned in *best).  FP64 batches factor in place, so before every launch the
+ * tuner restores dF[m] from dSrc[m] (device copies, outside the timed region); dSrc may be
+ * NULL for low-precision batches, whose conversion tasks rewrite dF.  ms (nullable, 6
+ * entries): each candidate's best device time. */
+int mtd_batch_tune_schedule(mtd_batch *b, void *const *dF, const int64_t *ldf, const void *const *dSrc,
+                            const int64_t *ldsrc, const double *const *dA, const int64_t *lda, const double *const *dB,
+                            const int64_t *ldb, double *const *dX, const int64_t *ldx, const int *nrhs, int method,
+                            double tol, int max_iter, double shift, int reps, int *best, double *ms, void *stream);
 int mtd_batch_destroy(mtd_batch *b);
 /* Autotuner: picks tile[m] and nest[m] for a batch of sizes n[m] by timing, for each
  * distinct size, trial factorisations of that size's share of the batch (seeded SPD

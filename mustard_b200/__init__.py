@@ -19,7 +19,8 @@ import os
 
 from . import _capi
 from ._capi import (  # noqa: F401  (re-exported constants)
-    GEN_SPD, GEN_UNIFORM_DIAG, KIND_CHOLESKY, KIND_CUSTOM, KIND_LU, OP_GEMM_NN, OP_GEMM_NT,
+    BATCH_NUM_SCHEDULES, BATCH_ORDER_INPUT, BATCH_ORDER_LARGEST_FIRST, BATCH_ORDER_SMALLEST_FIRST,
+    BATCH_SOLVE_LATE, GEN_SPD, GEN_UNIFORM_DIAG, KIND_CHOLESKY, KIND_CUSTOM, KIND_LU, OP_GEMM_NN, OP_GEMM_NT,
     OP_GETRF, OP_NAMES, OP_POTRF, OP_SYRK_LN, OP_TRSM_LLNU, OP_TRSM_RLT, OP_TRSM_RUN,
     PREC_BF16, PREC_FP32, PREC_FP64, PREC_TF32, REFINE_GMRES_IR, REFINE_IR, REFINE_NONE, STATUS_NAMES, MtdError,
     lib, lib_path)
@@ -415,6 +416,60 @@ class Batch:
                                               int(max_iter), _stream_handle(stream), ctypes.byref(st)))
         return {"iterations": st.iterations, "converged_count": st.converged_count,
                 "max_backward_error": st.max_backward_error, "solve_ms": st.solve_ms}
+
+    def _solve_args(self, factors, bs, xs, a64):
+        pf, lf = self._ptrs(factors)
+        pb, lb = self._ptrs(bs)
+        px, lx = self._ptrs(xs)
+        nr = (ctypes.c_int * self.count)(*[(b.shape[1] if b.dim() == 2 else 1) for b in bs])
+        pa, la = self._ptrs(a64) if a64 is not None else (None, None)
+        return pf, lf, pa, la, pb, lb, px, lx, nr
+
+    def factor_solve(self, factors, bs, xs, a64=None, method=_capi.REFINE_NONE, tol=1e-13, max_iter=20,
+                     shift=0.0, stream=None):
+        """Factor and solve in ONE persistent launch (mtd_batch_factor_solve; stream-ordered,
+        CUDA-graph capturable).  FP64 batches factor ``factors`` in place; low-precision
+        batches write them from ``a64`` (+ shift I) inside the launch.  Results:
+        solve_status()."""
+        args = self._solve_args(factors, bs, xs, a64)
+        self._keep = (factors, bs, xs, a64)
+        _capi.check(self._lib.mtd_batch_factor_solve(self._h, *args, method, float(tol), int(max_iter),
+                                                     float(shift), _stream_handle(stream)))
+
+    def solve_status(self):
+        """Wait for the last factor_solve: (rc, info, latency_ms, berr, iterations, stats)."""
+        c = self.count
+        info, lat = (ctypes.c_int * c)(), (ctypes.c_double * c)()
+        berr, its = (ctypes.c_double * c)(), (ctypes.c_int * c)()
+        st = _capi.BatchSolveStats()
+        rc = self._lib.mtd_batch_solve_status(self._h, info, lat, berr, its, ctypes.byref(st))
+        stats = {"iterations": st.iterations, "converged_count": st.converged_count,
+                 "max_backward_error": st.max_backward_error, "device_ms": st.solve_ms}
+        return rc, list(info), list(lat), list(berr), list(its), stats
+
+    @property
+    def schedule(self):
+        return self._lib.mtd_batch_get_schedule(self._h)
+
+    @schedule.setter
+    def schedule(self, value):
+        _capi.check(self._lib.mtd_batch_set_schedule(self._h, int(value)))
+
+    def tune_schedule(self, factors, bs, xs, a64=None, source=None, method=_capi.REFINE_NONE, tol=1e-13,
+                      max_iter=20, shift=0.0, reps=2, stream=None):
+        """Time factor_solve under each CTA-to-task schedule and keep the fastest
+        (mtd_batch_tune_schedule).  FP64 batches need ``source``: the inputs ``factors`` is
+        restored from before every trial.  Returns (schedule, {schedule: ms})."""
+        pf, lf, pa, la, pb, lb, px, lx, nr = self._solve_args(factors, bs, xs, a64)
+        ps, ls = self._ptrs(source) if source is not None else (None, None)
+        best = ctypes.c_int(0)
+        ms = (ctypes.c_double * _capi.BATCH_NUM_SCHEDULES)()
+        self._keep = (factors, bs, xs, a64, source)
+        _capi.check(self._lib.mtd_batch_tune_schedule(self._h, pf, lf, ps, ls, pa, la, pb, lb, px, lx, nr, method,
+                                                      float(tol), int(max_iter), float(shift), int(reps),
+                                                      ctypes.byref(best), ms, _stream_handle(stream)))
+        sched = [(c // 2) | (_capi.BATCH_SOLVE_LATE if c % 2 else 0) for c in range(_capi.BATCH_NUM_SCHEDULES)]
+        return best.value, {s: ms[c] for c, s in enumerate(sched)}
 
     def close(self):
         if getattr(self, "_h", None):

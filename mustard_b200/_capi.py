@@ -34,6 +34,8 @@ class RunStats(ctypes.Structure):
 
 PREC_FP64, PREC_TF32, PREC_FP32, PREC_BF16 = 0, 1, 2, 3
 REFINE_NONE, REFINE_IR, REFINE_GMRES_IR = 0, 1, 2
+BATCH_ORDER_INPUT, BATCH_ORDER_LARGEST_FIRST, BATCH_ORDER_SMALLEST_FIRST = 0, 1, 2
+BATCH_SOLVE_LATE, BATCH_NUM_SCHEDULES = 4, 6
 
 
 class SolveStats(ctypes.Structure):
@@ -56,6 +58,15 @@ SIGNATURES = {
     "mtd_batch_convert": (_i, [_vp, _pp, _pi64, _pp, _pi64, _d, _vp]),
     "mtd_batch_solve": (_i, [_vp, _pp, _pi64, _pp, _pi64, _pp, _pi64, _pp, _pi64, ctypes.POINTER(_i), _i, _d, _i, _vp,
                              ctypes.POINTER(BatchSolveStats)]),
+    "mtd_batch_factor_solve": (_i, [_vp, _pp, _pi64, _pp, _pi64, _pp, _pi64, _pp, _pi64, ctypes.POINTER(_i), _i, _d,
+                                    _i, _d, _vp]),
+    "mtd_batch_solve_status": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_d), ctypes.POINTER(_d),
+                                    ctypes.POINTER(_i), ctypes.POINTER(BatchSolveStats)]),
+    "mtd_batch_set_schedule": (_i, [_vp, _i]),
+    "mtd_batch_get_schedule": (_i, [_vp]),
+    "mtd_batch_tune_schedule": (_i, [_vp, _pp, _pi64, _pp, _pi64, _pp, _pi64, _pp, _pi64, _pp, _pi64,
+                                     ctypes.POINTER(_i), _i, _d, _i, _d, _i, ctypes.POINTER(_i), ctypes.POINTER(_d),
+                                     _vp]),
     "mtd_batch_destroy": (_i, [_vp]),
     "mtd_batch_autotune": (_i, [_i, _pi64, _i, _pi64, ctypes.POINTER(_i), ctypes.POINTER(_d), _vp]),
     "mtd_adjoint_create": (_i, [ctypes.POINTER(_vp), _i, _pi64, _i64, _i]),

@@ -14,6 +14,10 @@ normwise backward error 1e-13):
              latency (completion of the matrix's last task after the launch's first work,
              on the device clock);
   solve      factor replay + per-matrix solves, time-to-solution and max backward error;
+  one launch factor AND solve (+ refinement; + conversion from FP64 for fp32) as ONE
+             persistent launch (mtd_batch_factor_solve), captured in a CUDA graph and
+             replayed: device time, wall time-to-solution, latencies, backward errors; first
+             the schedule tuner times the six CTA-to-task schedules and keeps the fastest;
   defaults   the same factor launch with the library's default tiles (what tuning buys);
   torch      torch.linalg.cholesky + cholesky_solve per size group, for reference.
 One JSON line per measurement.
@@ -53,6 +57,58 @@ def views(groups, count, dtype=None):
         for j, i in enumerate(idx):
             out[i] = src[j].t()
     return out
+
+
+def one_launch(b, pname, prec, work, restore, rhs, a64, groups, base, flops_s, reps):
+    """Factor + solve (+ IR) as ONE persistent launch: tune the CTA-to-task schedule, capture
+    the launch in a CUDA graph and time its replays."""
+    fp64 = prec == mtd.PREC_FP64
+    kw = dict(a64=a64, method=mtd.REFINE_NONE) if fp64 else \
+        dict(a64=a64, method=mtd.REFINE_IR, tol=1e-13, max_iter=30)
+    xs = [torch.zeros_like(r) for r in rhs]
+    src = views({n: (idx, a) for n, (idx, a) in groups.items()}, len(rhs)) if fp64 else None
+    t0 = time.perf_counter()
+    sched, trial = b.tune_schedule(work, rhs, xs, source=src, reps=2, **kw)
+    tune_s = time.perf_counter() - t0
+    names = {0: "input order", 1: "largest first", 2: "smallest first"}
+    label = {s_: names[s_ & 3] + (", solves late" if s_ & mtd.BATCH_SOLVE_LATE else ", solves early")
+             for s_ in trial}
+    print(json.dumps(dict(base, prec=pname, step="schedule tuner", wall_s=tune_s, chosen=label[sched],
+                          device_ms={label[k]: v for k, v in trial.items()})), flush=True)
+    restore()
+    torch.cuda.synchronize()
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            b.factor_solve(work, rhs, xs, stream=s, **kw)
+    best = None
+    for _ in range(reps):
+        restore()
+        for x in xs:
+            x.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record()
+        g.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        wall = (time.perf_counter() - t0) * 1e3
+        ms = e0.elapsed_time(e1)
+        rc, info, lat, berr, its, st = b.solve_status()
+        assert rc == 0 and not any(info), rc
+        if best is None or ms < best[0]:
+            best = (ms, wall, lat, st)
+    ms, wall, lat, st = best
+    lat = np.asarray(lat)
+    print(json.dumps(dict(base, prec=pname, step="factor+solve", launches="ONE graph-captured persistent launch",
+                          schedule=label[sched], device_ms=ms, time_to_solution_ms=wall,
+                          tflops=flops_s / (wall * 1e-3) / 1e12, iterations=st["iterations"],
+                          converged=st["converged_count"], max_backward_error=st["max_backward_error"],
+                          latency_p50_ms=float(np.percentile(lat, 50)), latency_p99_ms=float(np.percentile(lat, 99)))),
+          flush=True)
+    del g
 
 
 def main():
@@ -137,10 +193,12 @@ def main():
                     t = (time.perf_counter() - t0) * 1e3
                     if best_t is None or t < best_t:
                         best_t, st = t, s_
-                print(json.dumps(dict(base, prec=pname, step="factor+solve", time_to_solution_ms=best_t,
+                print(json.dumps(dict(base, prec=pname, step="factor+solve", launches="factor graph + solve launches",
+                                      time_to_solution_ms=best_t,
                                       tflops=flops_s / (best_t * 1e-3) / 1e12, iterations=st["iterations"],
                                       converged=st["converged_count"], max_backward_error=st["max_backward_error"])),
                       flush=True)
+                one_launch(b, pname, prec, work, restore, rhs, a64, groups, base, flops_s, args.reps)
             del g
             b.close()
         del work_groups, pristine, work

@@ -20,7 +20,7 @@ CUDA_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr
 # engine-shape overrides for tuning builds, e.g. MTD_NVCC_EXTRA="-DMTD_PANEL_STAGES=4"
 CUDA_FLAGS += os.environ.get("MTD_NVCC_EXTRA", "").split()
 
-LIB_SOURCES = ["runtime.cu", "gen.cu", "dag.cpp", "solver.cu", "batch.cu", "adjoint.cu"]
+LIB_SOURCES = ["runtime.cu", "batch_run.cu", "gen.cu", "dag.cpp", "solver.cu", "batch.cu", "adjoint.cu"]
 CLI_PROGRAMS = {"lu_mustard": "lu_mustard.cpp", "cholesky_mustard": "cholesky_mustard.cpp"}
 PROBES = {"dmma_probe": os.path.join(PKG, "probe", "dmma_probe.cu")}  # measurement tools
 
@@ -52,13 +52,19 @@ def build(verbose: bool = False, ptxas_verbose: bool = False) -> str:
     os.makedirs(BUILD_DIR, exist_ok=True)
     os.makedirs(BIN_DIR, exist_ok=True)
     deps = _deps()
-    objs = []
+    objs, jobs = [], []
     for src in LIB_SOURCES:
         obj = os.path.join(BUILD_DIR, src + ".o")
         objs.append(obj)
         if _newer(obj, deps) or ptxas_verbose:
             extra = ["-Xptxas", "-v"] if ptxas_verbose else []
-            _run([NVCC] + CUDA_FLAGS + extra + ["-c", os.path.join(CSRC, src), "-o", obj], verbose)
+            jobs.append([NVCC] + CUDA_FLAGS + extra + ["-c", os.path.join(CSRC, src), "-o", obj])
+    # the translation units compile independently (the two persistent-kernel units take most
+    # of the time), so in parallel
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(_run, cmd, verbose) for cmd in jobs]:
+            f.result()
     if _newer(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-lpthread", "-ldl"], verbose)
     for prog, src in CLI_PROGRAMS.items():

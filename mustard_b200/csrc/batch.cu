@@ -19,354 +19,85 @@
 #include <vector>
 
 #include "../../include/mustard_b200.h"
+#include "batch_ops.cuh"
 #include "dag.hpp"
 #include "device_types.hpp"
 
 namespace mtd {
 int launch_run(const RunArgs &a, const int *deps_init, const int *roots, int n_roots, long long total_items,
                int prec, bool vec2, int grid, cudaStream_t s, bool adjoint);
+int launch_run_solve(const RunArgs &a, const int *deps_init, const int *roots, int n_roots, long long total_items,
+                     int prec, bool vec2, int grid, cudaStream_t s);
 }
 using namespace mtd;
 
 namespace {
 
-constexpr int kSB = 64;        // solve block (= inverse block edge)
-constexpr int kMaxRhs = 16;
-constexpr int kBT = 256;       // threads of the batched solve kernels
+constexpr int kSB = bsolve::kSB;
+constexpr int kMaxRhs = bsolve::kMaxRhs;
+constexpr int kBT = 256;       // threads of the standalone batched solve kernels
 constexpr int kInfoOk = 0x7f7f7f7f;  // per-matrix info sentinel (bytes 0x7f): no bad pivot
+using bsolve::kOnD;
+using bsolve::kOnR;
+using bsolve::kOnX;
 
-// Per-matrix arguments of the solve kernels.
-struct SolveMat {
-    const double *a;  // FP64 matrix (lower triangle read), for residuals
-    int64_t lda;
-    const void *f;    // factor (element type of the batch)
-    int64_t ldf;
-    int64_t ws_off, ws_ld;
-    const double *b;
-    int64_t ldb;
-    double *x;
-    int64_t ldx;
-    double *r;        // residual scratch, n x nrhs (ld n)
-    void *d;          // low-precision correction scratch, n x nrhs (ld n)
-    double *rowsum;   // n scratch for ||A||_inf
-    int n, nrhs;
+// The standalone solve kernels, one CTA per matrix (batch_ops.cuh holds their bodies, which
+// the solve tasks of the factor-and-solve launch share).  A refinement step skips the
+// matrices that have converged (`done`: berr[m] <= tol), as a solve task stops refining its
+// own matrix, so both paths apply the same steps to every matrix.
+struct Skip {
+    const double *berr;  // nullptr: skip nothing
+    double tol;
+    __device__ bool operator()() const { return berr && berr[blockIdx.x] <= tol; }
 };
 
-// One element copied global -> shared with cp.async (4 or 8 bytes, through L1: the solves
-// read back blocks this CTA wrote); an invalid element is zero-filled (0 source bytes, the
-// source address then only has to be a valid one).
+// (2 CTAs per SM: the FP64 blocks fill the shared memory; more float CTAs would spill)
 template <typename T>
-__device__ __forceinline__ void cp_elem(T *dst, const T *src, bool valid) {
-    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
-    if constexpr (sizeof(T) == 8)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// Shared memory of the batched solve kernels: two 64 x 65 blocks, two nrhs x 64 vector
-// blocks and (triangular solve) one nrhs x 64 accumulator.
-template <typename T>
-constexpr size_t trsv_smem() {
-    return (2 * kSB * (kSB + 1) + 3 * kMaxRhs * kSB) * sizeof(T);
-}
-constexpr size_t residual_smem() { return (2 * kSB * (kSB + 1) + 2 * kMaxRhs * kSB) * sizeof(double); }
-
-// Forward then backward substitution with L and the inverses of its 64 x 64 diagonal
-// blocks, on the n x nrhs block Y (ld ldy), one CTA per matrix.  Block row j subtracts
-// L(j, k) Y(k) for the rows k solved before it and applies the inverse of its diagonal
-// block; the blocks it needs (L(j, k) with Y(k), then the inverse) stream through a
-// two-deep cp.async ring, the next one in flight while the current product runs.  (The
-// first version loaded every block element by element in dependent load / store loops:
-// ~5 ms per launch for a batch of 4096 matrices of up to 1024.)
-enum { kOnX = 0, kOnD = 1, kOnR = 2 };  // which block of SolveMat the solve overwrites
-
-template <typename T>
-__global__ void __launch_bounds__(kBT) batch_trsv_kernel(const SolveMat *mats, const T *ws, int target) {
+__global__ void __launch_bounds__(kBT, 2) batch_trsv_kernel(const SolveMat *mats, const T *ws, int target, Skip done) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *Lb = reinterpret_cast<T *>(smem_raw);  // 2 x [kSB][kSB + 1]
-    T *Yb = Lb + 2 * kSB * (kSB + 1);         // 2 x [kMaxRhs][kSB]
-    T *Acc = Yb + 2 * kMaxRhs * kSB;          // [kMaxRhs][kSB]
-    const SolveMat &sm = mats[blockIdx.x];
-    const int n = sm.n, nrhs = sm.nrhs, tid = threadIdx.x;
-    const T *L = static_cast<const T *>(sm.f);
-    const int64_t ldl = sm.ldf;
-    const T *W = ws + sm.ws_off;
-    const int64_t ldw = sm.ws_ld;
-    T *Y = target == kOnX ? reinterpret_cast<T *>(sm.x)
-                          : (target == kOnR ? reinterpret_cast<T *>(sm.r) : static_cast<T *>(sm.d));
-    const int64_t ldy = target == kOnX ? sm.ldx : n;
-    const int nb = (n + kSB - 1) / kSB;
-    for (int pass = 0; pass < 2; ++pass) {
-        const bool back = pass == 1;
-        for (int s = 0; s < nb; ++s) {
-            const int j = back ? nb - 1 - s : s;
-            const int rj = min(kSB, n - j * kSB);
-            // step t < s: L(j, k_t) (transposed in the backward pass) and Y(k_t); t = s: W_j
-            auto issue = [&](int t) {
-                T *Ld = Lb + (t & 1) * kSB * (kSB + 1);
-                if (t < s) {
-                    const int k = back ? nb - 1 - t : t;
-                    const int rk = min(kSB, n - k * kSB);
-                    for (int e = tid; e < kSB * kSB; e += kBT) {
-                        const int a = e % kSB, c = e / kSB;
-                        if (!back) {
-                            const bool v = a < rj && c < rk;
-                            cp_elem(Ld + a * (kSB + 1) + c, v ? L + (int64_t(j) * kSB + a) + (int64_t(k) * kSB + c) * ldl : L, v);
-                        } else {
-                            const bool v = a < rk && c < rj;
-                            cp_elem(Ld + c * (kSB + 1) + a, v ? L + (int64_t(k) * kSB + a) + (int64_t(j) * kSB + c) * ldl : L, v);
-                        }
-                    }
-                    T *Yd = Yb + (t & 1) * kMaxRhs * kSB;
-                    for (int e = tid; e < kSB * nrhs; e += kBT) {
-                        const int r = e % kSB, c = e / kSB;
-                        cp_elem(Yd + c * kSB + r, r < rk ? Y + (int64_t(k) * kSB + r) + c * ldy : Y, r < rk);
-                    }
-                } else {
-                    for (int e = tid; e < kSB * kSB; e += kBT) {
-                        const int a = e % kSB, c = e / kSB;
-                        const bool v = a < rj && c < rj;
-                        cp_elem(back ? Ld + c * (kSB + 1) + a : Ld + a * (kSB + 1) + c,
-                                v ? W + (int64_t(j) * kSB + a) + int64_t(c) * ldw : W, v);
-                    }
-                }
-                cp_commit();
-            };
-            issue(0);
-            for (int e = tid; e < kSB * nrhs; e += kBT) {
-                const int r = e % kSB, c = e / kSB;
-                Acc[c * kSB + r] = r < rj ? Y[(int64_t(j) * kSB + r) + c * ldy] : T(0);
-            }
-            for (int t = 0; t <= s; ++t) {
-                cp_wait_all();
-                __syncthreads();  // block t landed; every thread is done with the other buffer
-                if (t + 1 <= s) issue(t + 1);
-                const T *Lc = Lb + (t & 1) * kSB * (kSB + 1);
-                if (t < s) {
-                    const T *Yc = Yb + (t & 1) * kMaxRhs * kSB;
-                    for (int o = tid; o < kSB * nrhs; o += kBT) {
-                        const int r = o % kSB, c = o / kSB;
-                        T acc = T(0);
-#pragma unroll 8
-                        for (int q = 0; q < kSB; ++q) acc += Lc[r * (kSB + 1) + q] * Yc[c * kSB + q];
-                        Acc[c * kSB + r] -= acc;
-                    }
-                } else {
-                    for (int o = tid; o < kSB * nrhs; o += kBT) {
-                        const int r = o % kSB, c = o / kSB;
-                        T acc = T(0);
-#pragma unroll 8
-                        for (int q = 0; q < kSB; ++q) acc += Lc[r * (kSB + 1) + q] * Acc[c * kSB + q];
-                        if (r < rj) Y[(int64_t(j) * kSB + r) + c * ldy] = acc;
-                    }
-                }
-            }
-            __syncthreads();  // Y(j) stored before later rows read it; Acc and the ring are free
-        }
-    }
+    if (done()) return;
+    bsolve::trsv<T, kBT>(mats[blockIdx.x], ws, target, bsolve::Smem{smem_raw});
 }
 
-// r = b - A_sym x, then the matrix's normwise backward error (max over its columns) into
-// berr[m]; one CTA per matrix.  A's infinity norm comes from anorm[m] (computed by
-// batch_anorm_kernel).  Block row I of r is formed in registers over the whole symmetric
-// block row (A(I, J) read from the lower triangle, transposed for J > I), the blocks of A
-// and of x streaming through a two-deep cp.async ring; r(I) is written once.  (The first
-// version read x from global memory inside its inner loop and accumulated the transposed
-// contributions in global r: ~11 ms per launch for a batch of 4096 matrices of up to 1024.)
-__global__ void __launch_bounds__(kBT) batch_residual_kernel(const SolveMat *mats, const double *anorm, double *berr) {
+// r = b - A_sym x and the matrix's backward error into berr[m]; the first call of a solve
+// (want_anorm) also computes ||A_sym||_inf into anorm[m], which later calls read.
+__global__ void __launch_bounds__(kBT, 2) batch_residual_kernel(const SolveMat *mats, double *anorm, double *berr,
+                                                                int want_anorm, Skip done) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *Ab = reinterpret_cast<double *>(smem_raw);  // 2 x [kSB][kSB + 1]
-    double *Xb = Ab + 2 * kSB * (kSB + 1);              // 2 x [kMaxRhs][kSB]
-    __shared__ double red[3][kMaxRhs][kBT / 32];
-    const SolveMat &sm = mats[blockIdx.x];
-    const int n = sm.n, nrhs = sm.nrhs, tid = threadIdx.x;
-    const double *A = sm.a;
-    const int64_t lda = sm.lda;
-    const int nb = (n + kSB - 1) / kSB;
-    constexpr int kOut = kMaxRhs * kSB / kBT;  // outputs per thread: o = tid + kBT q
-    static_assert(kMaxRhs * kSB % kBT == 0, "whole outputs per thread");
-    for (int I = 0; I < nb; ++I) {
-        const int ri = min(kSB, n - I * kSB);
-        auto issue = [&](int J) {
-            double *Ad = Ab + (J & 1) * kSB * (kSB + 1);
-            const int cj = min(kSB, n - J * kSB);
-            if (J < I) {  // A(I, J) straight from the lower triangle
-                for (int e = tid; e < kSB * kSB; e += kBT) {
-                    const int r = e % kSB, c = e / kSB;
-                    const bool v = r < ri && c < cj;
-                    cp_elem(Ad + r * (kSB + 1) + c, v ? A + (int64_t(I) * kSB + r) + (int64_t(J) * kSB + c) * lda : A, v);
-                }
-            } else if (J > I) {  // A(I, J) = A(J, I)^T
-                for (int e = tid; e < kSB * kSB; e += kBT) {
-                    const int c = e % kSB, r = e / kSB;
-                    const bool v = r < ri && c < cj;
-                    cp_elem(Ad + r * (kSB + 1) + c, v ? A + (int64_t(J) * kSB + c) + (int64_t(I) * kSB + r) * lda : A, v);
-                }
-            } else {  // diagonal block: the strict upper part mirrored from the lower one
-                for (int e = tid; e < kSB * kSB; e += kBT) {
-                    const int r = e % kSB, c = e / kSB;
-                    const bool v = r < ri && c < cj;
-                    const int64_t off = r >= c ? (int64_t(I) * kSB + r) + (int64_t(I) * kSB + c) * lda
-                                               : (int64_t(I) * kSB + c) + (int64_t(I) * kSB + r) * lda;
-                    cp_elem(Ad + r * (kSB + 1) + c, v ? A + off : A, v);
-                }
-            }
-            double *Xd = Xb + (J & 1) * kMaxRhs * kSB;
-            for (int e = tid; e < kSB * nrhs; e += kBT) {
-                const int k = e % kSB, c = e / kSB;
-                cp_elem(Xd + c * kSB + k, k < cj ? sm.x + (int64_t(J) * kSB + k) + c * sm.ldx : sm.x, k < cj);
-            }
-            cp_commit();
-        };
-        double acc[kOut];
-#pragma unroll
-        for (int q = 0; q < kOut; ++q) acc[q] = 0.0;
-        issue(0);
-        for (int J = 0; J < nb; ++J) {
-            cp_wait_all();
-            __syncthreads();  // block J landed; the other buffer is free
-            if (J + 1 < nb) issue(J + 1);
-            const double *Ac = Ab + (J & 1) * kSB * (kSB + 1);
-            const double *Xc = Xb + (J & 1) * kMaxRhs * kSB;
-#pragma unroll
-            for (int q = 0; q < kOut; ++q) {
-                const int o = tid + kBT * q, r = o % kSB, c = o / kSB;
-                if (c < nrhs) {
-                    double s = 0.0;
-#pragma unroll 8
-                    for (int k = 0; k < kSB; ++k) s += Ac[r * (kSB + 1) + k] * Xc[c * kSB + k];
-                    acc[q] += s;
-                }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < kOut; ++q) {
-            const int o = tid + kBT * q, r = o % kSB, c = o / kSB;
-            if (c < nrhs && r < ri)
-                sm.r[(int64_t(I) * kSB + r) + int64_t(c) * n] = sm.b[(int64_t(I) * kSB + r) + c * sm.ldb] - acc[q];
-        }
-        __syncthreads();  // the ring is free for the next block row
-    }
-    __syncthreads();
-    // column maxima of |r|, |x|, |b|
-    for (int c = 0; c < nrhs; ++c) {
-        double mr = 0.0, mx = 0.0, mb = 0.0;
-        for (int i = tid; i < n; i += kBT) {
-            mr = fmax(mr, fabs(sm.r[i + int64_t(c) * n]));
-            mx = fmax(mx, fabs(sm.x[i + int64_t(c) * sm.ldx]));
-            mb = fmax(mb, fabs(sm.b[i + int64_t(c) * sm.ldb]));
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
-            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-            mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, o));
-        }
-        if ((tid & 31) == 0) {
-            red[0][c][tid >> 5] = mr;
-            red[1][c][tid >> 5] = mx;
-            red[2][c][tid >> 5] = mb;
-        }
-    }
-    __syncthreads();
-    if (tid == 0) {
-        double worst = 0.0;
-        for (int c = 0; c < nrhs; ++c) {
-            double mr = 0.0, mx = 0.0, mb = 0.0;
-            for (int w = 0; w < kBT / 32; ++w) {
-                mr = fmax(mr, red[0][c][w]);
-                mx = fmax(mx, red[1][c][w]);
-                mb = fmax(mb, red[2][c][w]);
-            }
-            const double den = anorm[blockIdx.x] * mx + mb;
-            worst = fmax(worst, den > 0 ? mr / den : mr);
-        }
-        berr[blockIdx.x] = worst;
-    }
+    if (done()) return;  // converged before the last step: x and berr[m] stand
+    const double be = bsolve::residual<kBT>(mats[blockIdx.x], anorm + blockIdx.x, want_anorm != 0,
+                                            bsolve::Smem{smem_raw});
+    if (threadIdx.x == 0) berr[blockIdx.x] = be;
 }
 
-// ||A_sym||_inf per matrix (max row sum of |A| over the full symmetric matrix).
-__global__ void __launch_bounds__(kBT) batch_anorm_kernel(const SolveMat *mats, double *anorm) {
-    __shared__ double red[kBT / 32];
-    const SolveMat &sm = mats[blockIdx.x];
-    const int n = sm.n, tid = threadIdx.x;
-    double best = 0.0;
-    for (int i = tid; i < n; i += kBT) {
-        double s = 0.0;
-        for (int j = 0; j <= i; ++j) s += fabs(sm.a[i + int64_t(j) * sm.lda]);  // row i, lower part
-        for (int j = i + 1; j < n; ++j) s += fabs(sm.a[j + int64_t(i) * sm.lda]);  // column i below
-        best = fmax(best, s);
-    }
-    for (int o = 16; o > 0; o >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, o));
-    if ((tid & 31) == 0) red[tid >> 5] = best;
-    __syncthreads();
-    if (tid == 0) {
-        double m = 0.0;
-        for (int w = 0; w < kBT / 32; ++w) m = fmax(m, red[w]);
-        anorm[blockIdx.x] = m;
-    }
-}
-
-// d = r / max|r| per column (rounded to T), or x += max|r| * d; one CTA per matrix.
+// d = r / max|r| per column (rounded to T), or x += max|r| * d.
 template <typename T>
-__global__ void __launch_bounds__(kBT) batch_scale_kernel(const SolveMat *mats, double *colscale, bool to_low) {
+__global__ void __launch_bounds__(kBT) batch_scale_kernel(const SolveMat *mats, double *colscale, bool to_low, Skip done) {
     __shared__ double red[kBT / 32];
-    const SolveMat &sm = mats[blockIdx.x];
-    const int n = sm.n, tid = threadIdx.x;
+    if (done()) return;
     double *scale = colscale + int64_t(blockIdx.x) * kMaxRhs;
-    T *d = static_cast<T *>(sm.d);
-    for (int c = 0; c < sm.nrhs; ++c) {
-        if (to_low) {
-            double m = 0.0;
-            for (int i = tid; i < n; i += kBT) m = fmax(m, fabs(sm.r[i + int64_t(c) * n]));
-            for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-            __syncthreads();
-            if ((tid & 31) == 0) red[tid >> 5] = m;
-            __syncthreads();
-            double s = 0.0;
-            for (int w = 0; w < kBT / 32; ++w) s = fmax(s, red[w]);
-            if (s == 0.0) s = 1.0;
-            if (tid == 0) scale[c] = s;
-            for (int i = tid; i < n; i += kBT) d[i + int64_t(c) * n] = static_cast<T>(sm.r[i + int64_t(c) * n] / s);
-        } else {
-            const double s = scale[c];
-            for (int i = tid; i < n; i += kBT) sm.x[i + int64_t(c) * sm.ldx] += s * static_cast<double>(d[i + int64_t(c) * n]);
-        }
-    }
+    if (to_low)
+        bsolve::scale_to_low<T, kBT>(mats[blockIdx.x], scale, red);
+    else
+        bsolve::add_scaled<T, kBT>(mats[blockIdx.x], scale);
 }
 
-// x += r (FP64 correction), one CTA per matrix.
-__global__ void batch_add_kernel(const SolveMat *mats) {
-    const SolveMat &sm = mats[blockIdx.x];
-    for (int64_t e = threadIdx.x; e < int64_t(sm.n) * sm.nrhs; e += blockDim.x) {
-        const int64_t i = e % sm.n, c = e / sm.n;
-        sm.x[i + c * sm.ldx] += sm.r[i + c * sm.n];
-    }
+// x += r (FP64 correction).
+__global__ void __launch_bounds__(kBT) batch_add_kernel(const SolveMat *mats, Skip done) {
+    if (!done()) bsolve::add_r<kBT>(mats[blockIdx.x]);
 }
 
-// X = B (columns), one CTA per matrix.
-__global__ void batch_copy_rhs_kernel(const SolveMat *mats, bool zero) {
-    const SolveMat &sm = mats[blockIdx.x];
-    for (int64_t e = threadIdx.x; e < int64_t(sm.n) * sm.nrhs; e += blockDim.x) {
-        const int64_t i = e % sm.n, c = e / sm.n;
-        sm.x[i + c * sm.ldx] = zero ? 0.0 : sm.b[i + c * sm.ldb];
-    }
+// X = B (columns), or X = 0.
+__global__ void __launch_bounds__(kBT) batch_copy_rhs_kernel(const SolveMat *mats, bool zero) {
+    bsolve::copy_rhs<kBT>(mats[blockIdx.x], zero);
 }
 
-// dst = lower triangle of src (+ shift on the diagonal), as float; grid (chunks, count).
-__global__ void batch_convert_kernel(const SolveMat *mats, double shift) {
+// F = lower triangle of A (+ shift on the diagonal), as float; grid (column strips, count).
+__global__ void __launch_bounds__(kBT) batch_convert_kernel(const SolveMat *mats, double shift) {
     const SolveMat &sm = mats[blockIdx.y];
-    const int64_t n = sm.n, total = n * n;
-    float *f = static_cast<float *>(const_cast<void *>(sm.f));
-    for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t i = e % n, j = e / n;
-        if (i < j) continue;
-        double v = sm.a[i + j * sm.lda];
-        if (i == j) v += shift;
-        f[i + j * sm.ldf] = static_cast<float>(v);
-    }
+    for (int c0 = blockIdx.x * kConvertCols; c0 < sm.n; c0 += gridDim.x * kConvertCols)
+        bsolve::convert<float, kBT>(sm.a, sm.lda, static_cast<float *>(const_cast<void *>(sm.f)), sm.ldf, sm.n, shift,
+                                    c0, min(sm.n, c0 + kConvertCols));
 }
 
 template <typename T>
@@ -405,10 +136,30 @@ struct mtd_batch {
     bool pending = false;
     // solve state
     SolveMat *d_solve = nullptr, *h_solve = nullptr;  // pinned staging
-    double *d_r = nullptr, *d_rowsum = nullptr, *d_anorm = nullptr, *d_berr = nullptr, *d_scale = nullptr;
+    double *d_r = nullptr, *d_anorm = nullptr, *d_berr = nullptr, *d_scale = nullptr;
     double *h_berr = nullptr;      // pinned
     void *d_low = nullptr;
     int64_t rhs_total = 0;
+    // the merged factor DAG on the host (the factor-and-solve tables extend it), each matrix's
+    // roots and task range, and the CTA-to-task schedule (MTD_BATCH_ORDER_* | SOLVE_LATE)
+    std::vector<DevTask> h_tasks;
+    std::vector<int> h_succ, h_deps_init, first_task;
+    std::vector<std::vector<int>> roots_of;
+    int schedule = MTD_BATCH_ORDER_INPUT;
+    int last_tasks = 0;            // tasks of the last launch (factor or factor-and-solve)
+    // factor-and-solve launch: its tables (built at first use for the current schedule) and
+    // its per-matrix outcomes
+    int fs_convert = -1;           // the tables hold conversion tasks (1) or not (0); -1: not built
+    int fs_tasks = 0, fs_roots = 0;
+    long long fs_qcap[kNumQueues] = {0, 0, 0};
+    DevTask *d_fs_tasks = nullptr;
+    int *d_fs_succ = nullptr, *d_fs_deps_init = nullptr, *d_fs_deps = nullptr, *d_fs_items_left = nullptr,
+        *d_fs_roots = nullptr;
+    unsigned long long *d_fs_queue[kNumQueues] = {nullptr, nullptr, nullptr};
+    double *d_fs_berr = nullptr;
+    int *d_fs_iters = nullptr;
+    double fs_tol = 0.0;
+    bool fs_pending = false;
 };
 
 namespace {
@@ -434,12 +185,206 @@ void release(mtd_batch *b) {
     cudaFree(b->d_solve);
     if (b->h_solve) cudaFreeHost(b->h_solve);
     cudaFree(b->d_r);
-    cudaFree(b->d_rowsum);
     cudaFree(b->d_anorm);
     cudaFree(b->d_berr);
     cudaFree(b->d_scale);
     if (b->h_berr) cudaFreeHost(b->h_berr);
     cudaFree(b->d_low);
+    cudaFree(b->d_fs_berr);
+    cudaFree(b->d_fs_iters);
+}
+
+// The factor-and-solve tables (rebuilt when the schedule changes).
+void release_fs(mtd_batch *b) {
+    cudaFree(b->d_fs_tasks);
+    cudaFree(b->d_fs_succ);
+    cudaFree(b->d_fs_deps_init);
+    cudaFree(b->d_fs_deps);
+    cudaFree(b->d_fs_items_left);
+    cudaFree(b->d_fs_roots);
+    for (int q = 0; q < kNumQueues; ++q) cudaFree(b->d_fs_queue[q]);
+    b->d_fs_tasks = nullptr;
+    b->d_fs_succ = b->d_fs_deps_init = b->d_fs_deps = b->d_fs_items_left = b->d_fs_roots = nullptr;
+    for (int q = 0; q < kNumQueues; ++q) b->d_fs_queue[q] = nullptr;
+    b->fs_convert = -1;
+}
+
+// The matrices in the order their first tasks enter the queues under the batch's schedule.
+std::vector<int> schedule_order(const mtd_batch *b) {
+    std::vector<int> order(b->count);
+    for (int m = 0; m < b->count; ++m) order[m] = m;
+    const int o = b->schedule & 3;
+    if (o == MTD_BATCH_ORDER_LARGEST_FIRST)
+        std::stable_sort(order.begin(), order.end(), [b](int x, int y) { return b->n[x] > b->n[y]; });
+    else if (o == MTD_BATCH_ORDER_SMALLEST_FIRST)
+        std::stable_sort(order.begin(), order.end(), [b](int x, int y) { return b->n[x] < b->n[y]; });
+    return order;
+}
+
+// The factor launch's root list in schedule order.
+std::vector<int> scheduled_roots(const mtd_batch *b) {
+    std::vector<int> roots;
+    for (int m : schedule_order(b))
+        for (int r : b->roots_of[m]) roots.push_back(r);
+    return roots;
+}
+
+// The factor-and-solve task graph: the merged factor DAG, a solve task per matrix after its
+// sinks (queue 0, or queue 2 with MTD_BATCH_SOLVE_LATE) and, with `convert`, a conversion
+// task per matrix (queue 0) before its roots, which become the launch's roots in schedule
+// order.  Uploaded into the batch's fs tables.
+int build_fs(mtd_batch *b, bool convert) {
+    release_fs(b);
+    const int count = b->count, n0 = b->n_dev;
+    std::vector<DevTask> t = b->h_tasks;
+    std::vector<int> succ = b->h_succ, deps = b->h_deps_init, roots;
+    const int solve_queue = (b->schedule & MTD_BATCH_SOLVE_LATE) ? kNumQueues - 1 : 0;
+    const int total = n0 + count * (convert ? 2 : 1);
+    t.resize(total);
+    deps.resize(total, 0);
+    for (int m = 0; m < count; ++m) {
+        DevTask s{};
+        s.op = kOpBatchSolve;
+        s.queue = solve_queue;
+        s.n_items = 1;
+        s.m = s.n = static_cast<int32_t>(b->n[m]);
+        s.mat = m;
+        s.succ_begin = 0;
+        s.succ_count = 0;
+        t[n0 + m] = s;
+        for (int i = b->first_task[m]; i < b->first_task[m + 1]; ++i)
+            if (t[i].succ_count == 0) {  // a sink of matrix m: the solve follows it
+                t[i].succ_begin = static_cast<int32_t>(succ.size());
+                t[i].succ_count = 1;
+                succ.push_back(n0 + m);
+                ++deps[n0 + m];
+            }
+    }
+    for (int m : schedule_order(b)) {
+        if (!convert) {
+            for (int r : b->roots_of[m]) roots.push_back(r);
+            continue;
+        }
+        const int c = n0 + count + m;
+        DevTask d{};
+        d.op = kOpBatchConvert;
+        d.queue = 0;
+        d.n_items = static_cast<int32_t>((b->n[m] + kConvertCols - 1) / kConvertCols);
+        d.m = d.n = static_cast<int32_t>(b->n[m]);
+        d.mat = m;
+        d.succ_begin = static_cast<int32_t>(succ.size());
+        d.succ_count = static_cast<int32_t>(b->roots_of[m].size());
+        for (int r : b->roots_of[m]) {
+            succ.push_back(r);
+            deps[r] = 1;
+        }
+        t[c] = d;
+        roots.push_back(c);
+    }
+    long long qcap[kNumQueues] = {0, 0, 0};
+    for (const DevTask &d : t) qcap[d.queue] += d.n_items;
+    int rc = dalloc(&b->d_fs_tasks, t.size());
+    if (!rc) rc = dalloc(&b->d_fs_succ, succ.size());
+    if (!rc) rc = dalloc(&b->d_fs_deps_init, t.size());
+    if (!rc) rc = dalloc(&b->d_fs_deps, t.size());
+    if (!rc) rc = dalloc(&b->d_fs_items_left, t.size());
+    if (!rc) rc = dalloc(&b->d_fs_roots, roots.size());
+    for (int q = 0; q < kNumQueues && !rc; ++q) rc = dalloc(&b->d_fs_queue[q], size_t(qcap[q]));
+    if (!rc && (cudaMemcpy(b->d_fs_tasks, t.data(), t.size() * sizeof(DevTask), cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(b->d_fs_succ, succ.data(), succ.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(b->d_fs_deps_init, deps.data(), deps.size() * sizeof(int), cudaMemcpyHostToDevice) !=
+                    cudaSuccess ||
+                cudaMemcpy(b->d_fs_roots, roots.data(), roots.size() * sizeof(int), cudaMemcpyHostToDevice) !=
+                    cudaSuccess))
+        rc = MTD_ERR_CUDA;
+    if (rc) {
+        release_fs(b);
+        return rc;
+    }
+    b->fs_tasks = total;
+    b->fs_roots = static_cast<int>(roots.size());
+    for (int q = 0; q < kNumQueues; ++q) b->fs_qcap[q] = qcap[q];
+    b->fs_convert = convert ? 1 : 0;
+    return MTD_OK;
+}
+
+// Pinned staging, device table and scratch of the batched solves (allocated at first use).
+int ensure_solve_buffers(mtd_batch *b) {
+    const int count = b->count;
+    if (!b->h_solve && cudaMallocHost(reinterpret_cast<void **>(&b->h_solve), count * sizeof(SolveMat)) != cudaSuccess)
+        return MTD_ERR_OUT_OF_MEMORY;
+    if (!b->h_berr && cudaMallocHost(reinterpret_cast<void **>(&b->h_berr), count * sizeof(double)) != cudaSuccess)
+        return MTD_ERR_OUT_OF_MEMORY;
+    int rc = MTD_OK;
+    if (!b->d_solve) rc = dalloc(&b->d_solve, count);
+    if (!rc && !b->d_r) rc = dalloc(&b->d_r, size_t(b->rhs_total));
+    if (!rc && !b->d_anorm) rc = dalloc(&b->d_anorm, count);
+    if (!rc && !b->d_berr) rc = dalloc(&b->d_berr, count);
+    if (!rc && !b->d_scale) rc = dalloc(&b->d_scale, size_t(count) * kMaxRhs);
+    if (!rc && !b->d_low && cudaMalloc(&b->d_low, size_t(b->rhs_total) * sizeof(float)) != cudaSuccess)
+        rc = MTD_ERR_OUT_OF_MEMORY;
+    if (!rc && !b->d_fs_berr) rc = dalloc(&b->d_fs_berr, count);
+    if (!rc && !b->d_fs_iters) rc = dalloc(&b->d_fs_iters, count);
+    return rc;
+}
+
+// Validate a solve's arguments and stage its per-matrix table (SolveMat) in pinned memory.
+int stage_solve(mtd_batch *b, const double *const *dA, const int64_t *lda, void *const *dF, const int64_t *ldf,
+                const double *const *dB, const int64_t *ldb, double *const *dX, const int64_t *ldx, const int *nrhs) {
+    for (int m = 0; m < b->count; ++m) {
+        if (!dF[m] || !dB[m] || !dX[m] || nrhs[m] < 1 || nrhs[m] > kMaxRhs || ldb[m] < b->n[m] ||
+            ldx[m] < b->n[m] || ldf[m] < b->n[m])
+            return MTD_ERR_INVALID_ARG;
+        if (dA && (!dA[m] || lda[m] < b->n[m])) return MTD_ERR_INVALID_ARG;
+        SolveMat &sm = b->h_solve[m];
+        sm.a = dA ? dA[m] : nullptr;
+        sm.lda = dA ? lda[m] : 0;
+        sm.f = dF[m];
+        sm.ldf = ldf[m];
+        sm.ws_off = b->ws_off[m];
+        sm.ws_ld = b->ws_ld[m];
+        sm.b = dB[m];
+        sm.ldb = ldb[m];
+        sm.x = dX[m];
+        sm.ldx = ldx[m];
+        sm.r = b->d_r + b->rhs_off[m];
+        sm.d = static_cast<float *>(b->d_low) + b->rhs_off[m];
+        sm.n = static_cast<int>(b->n[m]);
+        sm.nrhs = nrhs[m];
+    }
+    return MTD_OK;
+}
+
+// Stage the per-run matrix table (dA[m] factored in place) and reset the per-matrix info
+// and completion stamps, on stream s; *vec2: every matrix allows 16-byte operand loads.
+int stage_factor(mtd_batch *b, void *const *dA, const int64_t *lda, cudaStream_t s, bool *vec2) {
+    const int64_t epc = 16 / static_cast<int64_t>(batch_elem(b));
+    *vec2 = true;
+    for (int m = 0; m < b->count; ++m) {
+        if (!dA[m] || lda[m] < b->n[m]) return MTD_ERR_INVALID_ARG;
+        b->h_mats[m] = BatchMat{dA[m], lda[m], b->ws_off[m], b->ws_ld[m]};
+        *vec2 = *vec2 && reinterpret_cast<uintptr_t>(dA[m]) % 16 == 0 && lda[m] % epc == 0 && b->n[m] % epc == 0 &&
+                b->tile[m] % epc == 0;
+    }
+    if (cudaMemcpyAsync(b->d_mats, b->h_mats, b->count * sizeof(BatchMat), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemsetAsync(b->d_info, 0x7f, b->count * sizeof(int), s) != cudaSuccess ||
+        cudaMemsetAsync(b->d_done, 0, b->count * sizeof(unsigned long long), s) != cudaSuccess)
+        return MTD_ERR_CUDA;
+    return MTD_OK;
+}
+
+// The run arguments every batched launch shares (the task tables are the caller's).
+RunArgs batch_args(const mtd_batch *b) {
+    RunArgs a{};
+    a.qctl = b->d_qctl;
+    a.ctl = b->d_ctl;
+    a.ws_lower = b->d_ws;
+    a.ws_upper = nullptr;
+    a.timeout_ns = 10ull * 1000000000ull;
+    a.mats = b->d_mats;
+    a.mat_info = b->d_info;
+    a.mat_done_ns = b->d_done;
+    return a;
 }
 
 // Default tile for a size when the caller gives none: one tile up to 512 (its diagonal
@@ -492,13 +437,18 @@ int mtd_batch_create(mtd_batch **out, int count, const int64_t *n, const int64_t
         if (rc) break;
         const int base = static_cast<int>(tasks.size());
         const int sbase = static_cast<int>(succ.size());
+        b->first_task.push_back(base);
+        b->roots_of.emplace_back();
         for (size_t t = 0; t < low.tasks.size(); ++t) {
             DevTask d = low.tasks[t];
             d.mat = m;
             d.succ_begin += sbase;
             tasks.push_back(d);
             deps_init.push_back(static_cast<int>(low.preds[t].size()));
-            if (low.preds[t].empty()) roots.push_back(base + static_cast<int>(t));
+            if (low.preds[t].empty()) {
+                roots.push_back(base + static_cast<int>(t));
+                b->roots_of.back().push_back(base + static_cast<int>(t));
+            }
         }
         for (int s : low.succ) succ.push_back(s + base);
         for (int q = 0; q < kNumQueues; ++q) b->qcap[q] += low.queue_cap[q];
@@ -512,7 +462,8 @@ int mtd_batch_create(mtd_batch **out, int count, const int64_t *n, const int64_t
     if (!rc && roots.empty()) rc = MTD_ERR_BAD_DAG;
     b->n_dev = static_cast<int>(tasks.size());
     b->n_roots = static_cast<int>(roots.size());
-    b->total_items = b->qcap[0] + b->qcap[1];
+    b->total_items = 0;
+    for (int q = 0; q < kNumQueues; ++q) b->total_items += b->qcap[q];
     b->rhs_total = rhs_total;
     const int nt = b->n_dev;
     if (!rc) rc = dalloc(&b->d_tasks, nt);
@@ -546,28 +497,40 @@ int mtd_batch_create(mtd_batch **out, int count, const int64_t *n, const int64_t
         return rc;
     }
     std::memset(b->h_ctl, 0, sizeof(RunCtl));
+    b->first_task.push_back(b->n_dev);
+    b->h_tasks = std::move(tasks);
+    b->h_succ = std::move(succ);
+    b->h_deps_init = std::move(deps_init);
     *out = b;
     return MTD_OK;
 }
 
 int mtd_batch_num_tasks(const mtd_batch *b) { return b ? b->n_dev : -MTD_ERR_INVALID_ARG; }
 
+int mtd_batch_set_schedule(mtd_batch *b, int schedule) {
+    if (!b || schedule < 0 || (schedule & ~(3 | MTD_BATCH_SOLVE_LATE)) || (schedule & 3) > MTD_BATCH_ORDER_SMALLEST_FIRST)
+        return MTD_ERR_INVALID_ARG;
+    if (schedule == b->schedule) return MTD_OK;
+    if ((b->pending || b->fs_pending) && b->last_stream && cudaStreamSynchronize(b->last_stream) != cudaSuccess)
+        return MTD_ERR_CUDA;
+    b->schedule = schedule;
+    const std::vector<int> roots = scheduled_roots(b);
+    if (cudaMemcpy(b->d_roots, roots.data(), roots.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+        return MTD_ERR_CUDA;
+    // factor-and-solve tables already built are rebuilt now, so the next launch allocates
+    // nothing (it may be under CUDA-graph capture)
+    return b->fs_convert >= 0 ? build_fs(b, b->fs_convert == 1) : MTD_OK;
+}
+
+int mtd_batch_get_schedule(const mtd_batch *b) { return b ? b->schedule : -MTD_ERR_INVALID_ARG; }
+
 int mtd_batch_factor(mtd_batch *b, void *const *dA, const int64_t *lda, void *stream) {
     if (!b || !dA || !lda) return MTD_ERR_INVALID_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const int64_t epc = 16 / static_cast<int64_t>(batch_elem(b));
     bool vec2 = true;
-    for (int m = 0; m < b->count; ++m) {
-        if (!dA[m] || lda[m] < b->n[m]) return MTD_ERR_INVALID_ARG;
-        b->h_mats[m] = BatchMat{dA[m], lda[m], b->ws_off[m], b->ws_ld[m]};
-        vec2 = vec2 && reinterpret_cast<uintptr_t>(dA[m]) % 16 == 0 && lda[m] % epc == 0 && b->n[m] % epc == 0 &&
-               b->tile[m] % epc == 0;
-    }
-    if (cudaMemcpyAsync(b->d_mats, b->h_mats, b->count * sizeof(BatchMat), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-        cudaMemsetAsync(b->d_info, 0x7f, b->count * sizeof(int), s) != cudaSuccess ||
-        cudaMemsetAsync(b->d_done, 0, b->count * sizeof(unsigned long long), s) != cudaSuccess)
-        return MTD_ERR_CUDA;
-    RunArgs a{};
+    int rc = stage_factor(b, dA, lda, s, &vec2);
+    if (rc) return rc;
+    RunArgs a = batch_args(b);
     a.n_tasks = b->n_dev;
     a.tasks = b->d_tasks;
     a.succ = b->d_succ;
@@ -577,19 +540,13 @@ int mtd_batch_factor(mtd_batch *b, void *const *dA, const int64_t *lda, void *st
         a.queue[q] = b->d_queue[q];
         a.queue_cap[q] = b->qcap[q];
     }
-    a.qctl = b->d_qctl;
-    a.ctl = b->d_ctl;
-    a.ws_lower = b->d_ws;
-    a.ws_upper = nullptr;
-    a.timeout_ns = 10ull * 1000000000ull;
-    a.mats = b->d_mats;
-    a.mat_info = b->d_info;
-    a.mat_done_ns = b->d_done;
-    int rc = launch_run(a, b->d_deps_init, b->d_roots, b->n_roots, b->total_items, b->prec, vec2, b->sms, s, false);
+    rc = launch_run(a, b->d_deps_init, b->d_roots, b->n_roots, b->total_items, b->prec, vec2, b->sms, s, false);
     if (rc) return rc;
     if (cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, s) != cudaSuccess) return MTD_ERR_CUDA;
     b->last_stream = s;
+    b->last_tasks = b->n_dev;
     b->pending = true;
+    b->fs_pending = false;
     return MTD_OK;
 }
 
@@ -611,7 +568,7 @@ int mtd_batch_status(mtd_batch *b, int *info, double *latency_ms) {
             latency_ms[m] = done[m] > b->h_ctl->start_ns ? double(done[m] - b->h_ctl->start_ns) * 1e-6 : -1.0;
     }
     if (b->h_ctl->error) return b->h_ctl->error;
-    if (b->h_ctl->tasks_done != b->n_dev) return MTD_ERR_TIMEOUT;
+    if (b->h_ctl->tasks_done != b->last_tasks) return MTD_ERR_TIMEOUT;
     return MTD_OK;
 }
 
@@ -625,50 +582,19 @@ int mtd_batch_solve(mtd_batch *b, const double *const *dA, const int64_t *lda, v
     if (low && method == MTD_REFINE_NONE) return MTD_ERR_INVALID_ARG;  // a low-precision factor needs refinement
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int count = b->count;
-    int rc = MTD_OK;
-    if (!b->h_berr) {
-        if (!b->h_solve && cudaMallocHost(reinterpret_cast<void **>(&b->h_solve), count * sizeof(SolveMat)) != cudaSuccess)
-            return MTD_ERR_OUT_OF_MEMORY;
-        if (cudaMallocHost(reinterpret_cast<void **>(&b->h_berr), count * sizeof(double)) != cudaSuccess)
-            return MTD_ERR_OUT_OF_MEMORY;
-        if (!b->d_solve) rc = dalloc(&b->d_solve, count);
-        if (!rc) rc = dalloc(&b->d_r, size_t(b->rhs_total));
-        if (!rc) rc = dalloc(&b->d_anorm, count);
-        if (!rc) rc = dalloc(&b->d_berr, count);
-        if (!rc) rc = dalloc(&b->d_scale, size_t(count) * kMaxRhs);
-        if (!rc && cudaMalloc(&b->d_low, size_t(b->rhs_total) * sizeof(float)) != cudaSuccess) rc = MTD_ERR_OUT_OF_MEMORY;
-        if (rc) return rc;
-    }
-    for (int m = 0; m < count; ++m) {
-        if (nrhs[m] < 1 || nrhs[m] > kMaxRhs || ldb[m] < b->n[m] || ldx[m] < b->n[m] || ldf[m] < b->n[m])
-            return MTD_ERR_INVALID_ARG;
-        if (dA && lda[m] < b->n[m]) return MTD_ERR_INVALID_ARG;
-        SolveMat &sm = b->h_solve[m];
-        sm.a = dA ? dA[m] : nullptr;
-        sm.lda = dA ? lda[m] : 0;
-        sm.f = dF[m];
-        sm.ldf = ldf[m];
-        sm.ws_off = b->ws_off[m];
-        sm.ws_ld = b->ws_ld[m];
-        sm.b = dB[m];
-        sm.ldb = ldb[m];
-        sm.x = dX[m];
-        sm.ldx = ldx[m];
-        sm.r = b->d_r + b->rhs_off[m];
-        sm.d = static_cast<float *>(b->d_low) + b->rhs_off[m];
-        sm.rowsum = nullptr;
-        sm.n = static_cast<int>(b->n[m]);
-        sm.nrhs = nrhs[m];
-    }
+    int rc = ensure_solve_buffers(b);
+    if (!rc) rc = stage_solve(b, dA, lda, dF, ldf, dB, ldb, dX, ldx, nrhs);
+    if (rc) return rc;
     const auto t0 = std::chrono::steady_clock::now();
     if (cudaMemcpyAsync(b->d_solve, b->h_solve, count * sizeof(SolveMat), cudaMemcpyHostToDevice, s) != cudaSuccess)
         return MTD_ERR_CUDA;
-    const size_t smem64 = trsv_smem<double>(), smem32 = trsv_smem<float>(), smem_res = residual_smem();
+    const size_t smem = bsolve::smem_bytes<kBT>(), smem64 = bsolve::trsv_bytes<double>(),
+                 smem32 = bsolve::trsv_bytes<float>();
     if (cudaFuncSetAttribute(batch_trsv_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem64)) !=
             cudaSuccess ||
         cudaFuncSetAttribute(batch_trsv_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem32)) !=
             cudaSuccess ||
-        cudaFuncSetAttribute(batch_residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_res)) !=
+        cudaFuncSetAttribute(batch_residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) !=
             cudaSuccess)
         return MTD_ERR_CUDA;
     const double *ws64 = reinterpret_cast<const double *>(b->d_ws);
@@ -677,15 +603,15 @@ int mtd_batch_solve(mtd_batch *b, const double *const *dA, const int64_t *lda, v
     double worst = -1.0;
     if (!low) {  // one FP64 solve: x = (L L^T)^-1 b
         batch_copy_rhs_kernel<<<count, kBT, 0, s>>>(b->d_solve, false);
-        batch_trsv_kernel<double><<<count, kBT, smem64, s>>>(b->d_solve, ws64, kOnX);
+        batch_trsv_kernel<double><<<count, kBT, smem64, s>>>(b->d_solve, ws64, kOnX, Skip{nullptr, 0.0});
         st.iterations = 1;
     } else {
         batch_copy_rhs_kernel<<<count, kBT, 0, s>>>(b->d_solve, true);  // x = 0
     }
     if (dA) {
-        batch_anorm_kernel<<<count, kBT, 0, s>>>(b->d_solve, b->d_anorm);
         for (int it = 0;; ++it) {
-            batch_residual_kernel<<<count, kBT, smem_res, s>>>(b->d_solve, b->d_anorm, b->d_berr);
+            batch_residual_kernel<<<count, kBT, smem, s>>>(b->d_solve, b->d_anorm, b->d_berr, it == 0,
+                                                           Skip{(it > 1 || (it > 0 && !low)) ? b->d_berr : nullptr, tol});
             if (cudaMemcpyAsync(b->h_berr, b->d_berr, count * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
                 cudaStreamSynchronize(s) != cudaSuccess)
                 return MTD_ERR_CUDA;
@@ -699,21 +625,153 @@ int mtd_batch_solve(mtd_batch *b, const double *const *dA, const int64_t *lda, v
             if (method == MTD_REFINE_NONE) break;
             if ((it > 0 || !low) && done == count) break;
             if (it >= max_iter) break;
+            // matrices already at tol keep their x (from the second residual on for a
+            // low-precision factor, whose first residual is of x = 0)
+            const Skip at_tol{(it > 0 || !low) ? b->d_berr : nullptr, tol};
             if (low) {  // x += M^-1 r through the low-precision factor
-                batch_scale_kernel<float><<<count, kBT, 0, s>>>(b->d_solve, b->d_scale, true);
-                batch_trsv_kernel<float><<<count, kBT, smem32, s>>>(b->d_solve, ws32, kOnD);
-                batch_scale_kernel<float><<<count, kBT, 0, s>>>(b->d_solve, b->d_scale, false);
+                batch_scale_kernel<float><<<count, kBT, 0, s>>>(b->d_solve, b->d_scale, true, at_tol);
+                batch_trsv_kernel<float><<<count, kBT, smem32, s>>>(b->d_solve, ws32, kOnD, at_tol);
+                batch_scale_kernel<float><<<count, kBT, 0, s>>>(b->d_solve, b->d_scale, false, at_tol);
             } else {    // x += (L L^T)^-1 r in FP64
-                batch_trsv_kernel<double><<<count, kBT, smem64, s>>>(b->d_solve, ws64, kOnR);
-                batch_add_kernel<<<count, kBT, 0, s>>>(b->d_solve);
+                batch_trsv_kernel<double><<<count, kBT, smem64, s>>>(b->d_solve, ws64, kOnR, at_tol);
+                batch_add_kernel<<<count, kBT, 0, s>>>(b->d_solve, at_tol);
             }
-            st.iterations = it + 1;
+            st.iterations = it + 1 + (low ? 0 : 1);  // + the first FP64 solve
         }
     }
     if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) return MTD_ERR_CUDA;
     st.max_backward_error = worst;
     st.solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     if (stats) *stats = st;
+    return rc;
+}
+
+int mtd_batch_factor_solve(mtd_batch *b, void *const *dF, const int64_t *ldf, const double *const *dA,
+                           const int64_t *lda, const double *const *dB, const int64_t *ldb, double *const *dX,
+                           const int64_t *ldx, const int *nrhs, int method, double tol, int max_iter, double shift,
+                           void *stream) {
+    if (!b || !dF || !ldf || !dB || !ldb || !dX || !ldx || !nrhs || max_iter < 0) return MTD_ERR_INVALID_ARG;
+    if (method != MTD_REFINE_NONE && method != MTD_REFINE_IR) return MTD_ERR_INVALID_ARG;
+    const bool low = b->prec != MTD_PREC_FP64;
+    if ((method == MTD_REFINE_IR || low) && (!dA || !lda)) return MTD_ERR_INVALID_ARG;
+    if (low && method == MTD_REFINE_NONE) return MTD_ERR_INVALID_ARG;  // a low-precision factor needs refinement
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc = ensure_solve_buffers(b);
+    if (!rc) rc = stage_solve(b, dA, lda, dF, ldf, dB, ldb, dX, ldx, nrhs);
+    if (!rc && b->fs_convert != (low ? 1 : 0)) rc = build_fs(b, low);
+    bool vec2 = true;
+    if (!rc) rc = stage_factor(b, dF, ldf, s, &vec2);
+    if (rc) return rc;
+    if (cudaMemcpyAsync(b->d_solve, b->h_solve, b->count * sizeof(SolveMat), cudaMemcpyHostToDevice, s) !=
+            cudaSuccess ||
+        cudaMemsetAsync(b->d_fs_berr, 0xff, b->count * sizeof(double), s) != cudaSuccess ||  // NaN: not solved
+        cudaMemsetAsync(b->d_fs_iters, 0, b->count * sizeof(int), s) != cudaSuccess)
+        return MTD_ERR_CUDA;
+    RunArgs a = batch_args(b);
+    a.n_tasks = b->fs_tasks;
+    a.tasks = b->d_fs_tasks;
+    a.succ = b->d_fs_succ;
+    a.deps = b->d_fs_deps;
+    a.items_left = b->d_fs_items_left;
+    long long items = 0;
+    for (int q = 0; q < kNumQueues; ++q) {
+        a.queue[q] = b->d_fs_queue[q];
+        a.queue_cap[q] = b->fs_qcap[q];
+        items += b->fs_qcap[q];
+    }
+    a.solve = b->d_solve;
+    a.solve_berr = b->d_fs_berr;
+    a.solve_iters = b->d_fs_iters;
+    a.solve_tol = tol;
+    a.solve_shift = shift;
+    a.solve_method = method;
+    a.solve_max_iter = max_iter;
+    rc = launch_run_solve(a, b->d_fs_deps_init, b->d_fs_roots, b->fs_roots, items, b->prec, vec2, b->sms, s);
+    if (rc) return rc;
+    if (cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, s) != cudaSuccess) return MTD_ERR_CUDA;
+    b->last_stream = s;
+    b->last_tasks = b->fs_tasks;
+    b->fs_tol = tol;
+    b->pending = true;
+    b->fs_pending = true;
+    return MTD_OK;
+}
+
+int mtd_batch_solve_status(mtd_batch *b, int *info, double *latency_ms, double *berr, int *iterations,
+                           mtd_batch_solve_stats *stats) {
+    if (!b) return MTD_ERR_INVALID_ARG;
+    if (!b->fs_pending) return MTD_ERR_STATE;
+    const int count = b->count;
+    std::vector<double> lat(count), be(count);
+    std::vector<int> it(count);
+    const int rc = mtd_batch_status(b, info, lat.data());
+    if (rc == MTD_ERR_CUDA) return rc;
+    if (cudaMemcpy(be.data(), b->d_fs_berr, count * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(it.data(), b->d_fs_iters, count * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return MTD_ERR_CUDA;
+    if (latency_ms) std::copy(lat.begin(), lat.end(), latency_ms);
+    if (berr) std::copy(be.begin(), be.end(), berr);
+    if (iterations) std::copy(it.begin(), it.end(), iterations);
+    if (stats) {
+        mtd_batch_solve_stats st{};
+        st.max_backward_error = -1.0;
+        double span = 0.0;
+        for (int m = 0; m < count; ++m) {
+            st.iterations = std::max(st.iterations, it[m]);
+            if (be[m] == be[m]) {  // not NaN: solved
+                st.max_backward_error = std::max(st.max_backward_error, be[m]);
+                st.converged_count += be[m] >= 0.0 && be[m] <= b->fs_tol;
+            }
+            span = std::max(span, lat[m]);
+        }
+        st.solve_ms = span;
+        *stats = st;
+    }
+    return rc;
+}
+
+int mtd_batch_tune_schedule(mtd_batch *b, void *const *dF, const int64_t *ldf, const void *const *dSrc,
+                            const int64_t *ldsrc, const double *const *dA, const int64_t *lda, const double *const *dB,
+                            const int64_t *ldb, double *const *dX, const int64_t *ldx, const int *nrhs, int method,
+                            double tol, int max_iter, double shift, int reps, int *best, double *ms, void *stream) {
+    if (!b || !dF || !ldf || reps < 1) return MTD_ERR_INVALID_ARG;
+    const bool low = b->prec != MTD_PREC_FP64;
+    if (!low && (!dSrc || !ldsrc)) return MTD_ERR_INVALID_ARG;  // FP64 factors overwrite their inputs
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t es = batch_elem(b);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return MTD_ERR_CUDA;
+    int rc = MTD_OK, winner = b->schedule;
+    double best_ms = 1e300;
+    for (int c = 0; c < MTD_BATCH_NUM_SCHEDULES && !rc; ++c) {
+        const int sched = (c / 2) | (c % 2 ? MTD_BATCH_SOLVE_LATE : 0);
+        rc = mtd_batch_set_schedule(b, sched);
+        double cand = 1e300;
+        for (int rep = 0; rep <= reps && !rc; ++rep) {  // rep 0 is untimed
+            if (dSrc)
+                for (int m = 0; m < b->count && !rc; ++m)
+                    if (cudaMemcpy2DAsync(dF[m], ldf[m] * es, dSrc[m], ldsrc[m] * es, b->n[m] * es, b->n[m],
+                                          cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+                        rc = MTD_ERR_CUDA;
+            if (!rc && cudaEventRecord(e0, s) != cudaSuccess) rc = MTD_ERR_CUDA;
+            if (!rc) rc = mtd_batch_factor_solve(b, dF, ldf, dA, lda, dB, ldb, dX, ldx, nrhs, method, tol, max_iter, shift, s);
+            if (!rc && cudaEventRecord(e1, s) != cudaSuccess) rc = MTD_ERR_CUDA;
+            if (!rc) rc = mtd_batch_solve_status(b, nullptr, nullptr, nullptr, nullptr, nullptr);
+            float t = 0.f;
+            if (!rc && cudaEventElapsedTime(&t, e0, e1) != cudaSuccess) rc = MTD_ERR_CUDA;
+            if (!rc && rep > 0) cand = std::min(cand, double(t));
+        }
+        if (ms) ms[c] = rc ? -1.0 : cand;
+        if (!rc && cand < best_ms) {
+            best_ms = cand;
+            winner = sched;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    rc = mtd_batch_set_schedule(b, winner);
+    if (best) *best = winner;
     return rc;
 }
 
@@ -738,7 +796,7 @@ int mtd_batch_convert(mtd_batch *b, const double *const *dA, const int64_t *lda,
     }
     if (cudaMemcpyAsync(b->d_solve, b->h_solve, b->count * sizeof(SolveMat), cudaMemcpyHostToDevice, s) != cudaSuccess)
         return MTD_ERR_CUDA;
-    batch_convert_kernel<<<dim3(16, b->count), 256, 0, s>>>(b->d_solve, shift);
+    batch_convert_kernel<<<dim3(8, b->count), kBT, 0, s>>>(b->d_solve, shift);
     // the staging buffer is reused by the next call: wait until the copy has been consumed
     if (cudaStreamSynchronize(s) != cudaSuccess) return MTD_ERR_CUDA;
     return cudaGetLastError() == cudaSuccess ? MTD_OK : MTD_ERR_CUDA;
@@ -748,6 +806,7 @@ int mtd_batch_destroy(mtd_batch *b) {
     if (!b) return MTD_ERR_INVALID_ARG;
     if (b->pending && b->last_stream) cudaStreamSynchronize(b->last_stream);
     cudaDeviceSynchronize();
+    release_fs(b);
     release(b);
     delete b;
     return MTD_OK;

@@ -19,7 +19,14 @@ constexpr int kNB = 64;         // diagonal block edge inside POTRF / GETRF (and
 constexpr int kNestTile = 128;  // default sub-tile edge of a nested diagonal factorisation
 
 // Device-side operation codes: the public mtd_op values plus a join (one no-op work item).
+// Codes from kOpJoin up are the scheduler's own tasks; the batched factor-and-solve launch
+// adds two (mtd_batch_factor_solve): a matrix's conversion to the factor's precision (its
+// root) and its solve with refinement (its sink).
 constexpr int kOpJoin = 100;
+constexpr int kOpBatchSolve = 101;    // one item: solve (+ refine) one matrix of the batch
+constexpr int kOpBatchConvert = 102;  // items = 128-column strips: F = lower(A) + shift I, as T
+constexpr int kConvertCols = 128;
+constexpr int kBatchInfoOk = 0x7f7f7f7f;  // per-matrix info of a batched run before any bad pivot
 
 // Cholesky adjoint operations (device tasks of the reverse sweep; see adjoint_ops.cuh).
 constexpr int kOpAdjTrsm = 20;    // C(m x n) := C * L^-1, L = n x n lower at (ar, ac) of the factor
@@ -58,6 +65,23 @@ struct alignas(16) DevTask {
     int32_t pad;
 };
 static_assert(sizeof(DevTask) == 64, "DevTask is read as four 16-byte words");
+
+// Per-matrix arguments of the batched solves (standalone kernels and the solve tasks of
+// the factor-and-solve launch).
+struct SolveMat {
+    const double *a;  // FP64 matrix (lower triangle read), for residuals
+    int64_t lda;
+    const void *f;    // factor (element type of the batch)
+    int64_t ldf;
+    int64_t ws_off, ws_ld;
+    const double *b;
+    int64_t ldb;
+    double *x;
+    int64_t ldx;
+    double *r;        // residual scratch, n x nrhs (ld n)
+    void *d;          // low-precision correction scratch, n x nrhs (ld n)
+    int n, nrhs;
+};
 
 // One matrix of a batched run.
 struct BatchMat {
@@ -143,6 +167,17 @@ struct RunArgs {
     int64_t lo_ld;
     int tma_lo;
     alignas(64) unsigned char tmap_lo[128];
+    // Batched factor-and-solve launches only (solve == nullptr otherwise): per-matrix solve
+    // arguments, the refinement method (MTD_REFINE_*), its tolerance and step limit, the
+    // diagonal shift of the conversion tasks, and per-matrix outcomes (backward error, -1 when
+    // no FP64 matrix was given; solves applied).
+    const SolveMat *solve;
+    double *solve_berr;
+    int *solve_iters;
+    double solve_tol;
+    double solve_shift;
+    int solve_method;
+    int solve_max_iter;
 };
 
 }  // namespace mtd

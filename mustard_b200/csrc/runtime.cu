@@ -607,7 +607,7 @@ int launch_run(const RunArgs &a, const int *deps_init, const int *roots, int n_r
     const int reset_blocks = static_cast<int>(std::min<long long>(
         1024, std::max<long long>(1, (std::max<long long>(total_items, a.n_tasks) + kThreads - 1) / kThreads)));
     reset_kernel<<<reset_blocks, kThreads, 0, s>>>(a, deps_init);
-    seed_kernel<<<1, 32, 0, s>>>(a, roots, n_roots);
+    seed_kernel<<<1, kSeedThreads, 0, s>>>(a, roots, n_roots);
     const int bytes = kOpSmemBytes();
     const bool fp64 = prec == MTD_PREC_FP64;
     const bool x3 = prec == MTD_PREC_FP32;
@@ -936,7 +936,7 @@ extern "C" int mtd_factor_noalloc(int kind, double *dA, int64_t n, int64_t lda, 
     const int reset_blocks =
         static_cast<int>(std::min<long long>(1024, (std::max<long long>(items, nt) + kThreads - 1) / kThreads));
     reset_kernel<<<std::max(reset_blocks, 1), kThreads, 0, s>>>(a, d_deps_init);
-    seed_kernel<<<1, 32, 0, s>>>(a, d_roots, static_cast<int>(roots.size()));
+    seed_kernel<<<1, kSeedThreads, 0, s>>>(a, d_roots, static_cast<int>(roots.size()));
     if (vec2) persistent_kernel<2, double><<<sms, kThreads, kOpSmemBytes(), s>>>(a);
     else persistent_kernel<1, double><<<sms, kThreads, kOpSmemBytes(), s>>>(a);
     if (cudaGetLastError() != cudaSuccess) return MTD_ERR_CUDA;

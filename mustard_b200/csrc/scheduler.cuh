@@ -25,6 +25,7 @@
 
 #include "device_types.hpp"
 #include "adjoint_ops.cuh"
+#include "batch_ops.cuh"
 #include "tcgen05.cuh"
 #include "tile_ops.cuh"
 
@@ -241,9 +242,47 @@ __device__ __forceinline__ int op_update_tc(const RunArgs &p, const MatCtx &m, c
     return 0;
 }
 
-template <int VEC, typename T, int SPLIT = 1, bool ADJ = false>
+// The solve task of one matrix of a batched factor-and-solve launch (the sink of its DAG):
+// the matrix's whole solve with refinement on this CTA (batch_ops.cuh).  A matrix whose
+// factorisation met a bad pivot is not solved: its backward error and step count keep the
+// values the launch reset them to.
+template <typename T>
+__device__ __noinline__ int op_batch_solve(const RunArgs &p, const DevTask &t, void *smem) {
+    static_assert(bsolve::smem_bytes<kThreads>() <= size_t(kOpSmemBytes()), "solve scratch fits the kernel's");
+    if (ld_volatile(p.mat_info + t.mat) != kBatchInfoOk) return 0;
+    double berr = -1.0;
+    int iters = 0;
+    bsolve::solve_refine<T, kThreads>(p.solve[t.mat], static_cast<const T *>(p.ws_lower), p.solve_method,
+                                      p.solve_tol, p.solve_max_iter, bsolve::Smem{static_cast<unsigned char *>(smem)},
+                                      &berr, &iters);
+    if (threadIdx.x == 0) {
+        p.solve_berr[t.mat] = berr;
+        p.solve_iters[t.mat] = iters;
+    }
+    return 0;
+}
+
+// One 128-column strip of a batched matrix's conversion to the factor's precision (the root
+// of its DAG in a low-precision factor-and-solve launch): F = lower(A) + shift I.
+template <typename T>
+__device__ __noinline__ int op_batch_convert(const RunArgs &p, const DevTask &t, int item) {
+    const SolveMat &sm = p.solve[t.mat];
+    const BatchMat bm = p.mats[t.mat];
+    const int c0 = item * kConvertCols;
+    bsolve::convert<T, kThreads>(sm.a, sm.lda, static_cast<T *>(bm.a), bm.lda, sm.n, p.solve_shift, c0,
+                                 min(sm.n, c0 + kConvertCols));
+    return 0;
+}
+
+// SOLVE: the instances of the batched factor-and-solve launch, which also run the solve and
+// conversion tasks; the other instances carry none of that code.
+template <int VEC, typename T, int SPLIT = 1, bool ADJ = false, bool SOLVE = false>
 __device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int item, void *smem,
                                         tc::State *tcs = nullptr, t64::State *s64 = nullptr) {
+    if constexpr (SOLVE) {
+        if (t.op == kOpBatchSolve) return op_batch_solve<T>(p, t, smem);
+        if (t.op == kOpBatchConvert) return op_batch_convert<T>(p, t, item);
+    }
     if (t.op == kOpJoin) return 0;  // a join's one item: nothing to compute
     if constexpr (ADJ) return dispatch_adjoint<T, VEC, SPLIT>(p, t, item, smem);
     const MatCtx m = mat_ctx<T>(p, t);
@@ -300,7 +339,7 @@ __device__ __forceinline__ void sync_drain_warps() {
 // the C update further, into the next item's MMAs, or starting those MMAs before the C
 // update ends, streams GEMM items faster but completes them later, and the factorisation,
 // which waits on its dependency chain, comes out slower.)
-template <int VEC, typename T, int SPLIT>
+template <int VEC, typename T, int SPLIT, bool SOLVE = false>
 __device__ __forceinline__ void persistent_loop_tc(const RunArgs &p, double *smem, tc::State &tcs) {
     __shared__ int s_cmd, s_task, s_item;
     __shared__ tc::Pending pend;
@@ -367,7 +406,7 @@ __device__ __forceinline__ void persistent_loop_tc(const RunArgs &p, double *sme
             __syncthreads();
             continue;
         }
-        const int st = dispatch<VEC, T, SPLIT, false>(p, t, item, smem, &tcs);
+        const int st = dispatch<VEC, T, SPLIT, false, SOLVE>(p, t, item, smem, &tcs);
         // nothing is pending here (drained above): redefining cv after the tile operation
         // frees its registers during it
 #pragma unroll
@@ -520,21 +559,22 @@ __device__ __forceinline__ void persistent_loop_ws(const RunArgs &p, double *sme
 
 // T64: the instance whose FP64 GEMM / SYRK items may read their operands by TMA (tma64.cuh,
 // runs that carry the tensor maps); the other instances carry none of that code.
-template <int VEC, typename T, int SPLIT = 1, bool ADJ = false, bool T64 = false>
+// SOLVE: the batched factor-and-solve launch's instances (see dispatch).
+template <int VEC, typename T, int SPLIT = 1, bool ADJ = false, bool T64 = false, bool SOLVE = false>
 __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const __grid_constant__ RunArgs p) {
     extern __shared__ __align__(128) double smem[];
     constexpr bool kTc = uses_tcgen05<VEC, T, SPLIT, ADJ>();
     if (threadIdx.x == 0) atomicMin(&p.ctl->start_ns, global_ns());
     if constexpr (kTc) {
         __shared__ tc::State tcs;
-        if (MTD_TC_WS) {
+        if (MTD_TC_WS && !SOLVE) {
             __shared__ tc::WsState ws;
             tc::ws_init(&ws);
             tc::init(&tcs);  // TMEM accumulators and the staged items' barriers; its barrier publishes ws
             persistent_loop_ws<VEC, T, SPLIT>(p, smem, tcs, ws);
         } else {
             tc::init(&tcs);  // TMEM accumulators and barriers, held for the whole run
-            persistent_loop_tc<VEC, T, SPLIT>(p, smem, tcs);
+            persistent_loop_tc<VEC, T, SPLIT, SOLVE>(p, smem, tcs);
         }
         tc::release(&tcs);
         return;
@@ -558,7 +598,7 @@ __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const __grid_co
             const unsigned long long t_start = p.trace ? global_ns() : 0ull;
             DevTask t;
             load_task(p, task, &t);
-            const int st = dispatch<VEC, T, SPLIT, ADJ>(p, t, item, smem, nullptr, kT64 ? &s64 : nullptr);
+            const int st = dispatch<VEC, T, SPLIT, ADJ, SOLVE>(p, t, item, smem, nullptr, kT64 ? &s64 : nullptr);
             __syncthreads();
             if (threadIdx.x == 0) finish_item(p, task, item, t_start, st == 0);
         }
@@ -576,7 +616,7 @@ __global__ void __launch_bounds__(kThreads, 1) task_kernel(const RunArgs p, int 
     if (t.n_items > 0) dispatch<VEC, T>(p, t, static_cast<int>(blockIdx.x), smem);
 }
 
-__global__ void reset_ctl_kernel(const RunArgs p) {
+static __global__ void reset_ctl_kernel(const RunArgs p) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         p.ctl->tasks_done = 0;
         p.ctl->error = 0;
@@ -588,7 +628,7 @@ __global__ void reset_ctl_kernel(const RunArgs p) {
 }
 
 // Per-run reset: counters from their initial values, queues empty.
-__global__ void reset_kernel(const RunArgs p, const int *deps_init) {
+static __global__ void reset_kernel(const RunArgs p, const int *deps_init) {
     const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
     const long long tid = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     for (long long i = tid; i < p.n_tasks; i += stride) {
@@ -613,10 +653,57 @@ __global__ void reset_kernel(const RunArgs p, const int *deps_init) {
 }
 
 // Seed the queues with the tasks that have no predecessor (kernel_populate_queue,
-// mustard/mustard.h:87-95).
-__global__ void seed_kernel(const RunArgs p, const int *roots, int n_roots) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        for (int r = 0; r < n_roots; ++r) release_task(p, roots[r]);
+// mustard/mustard.h:87-95), in root order within each queue.  One block: each thread takes a
+// contiguous run of roots, a scan of the per-thread item counts gives every run its slots,
+// and each queue's counters are published once at the end.  (A batched run seeds thousands
+// of roots; pushing them one at a time, each behind a memory fence, took ~6 ms for 4096.)
+constexpr int kSeedThreads = 1024;
+static __global__ void __launch_bounds__(kSeedThreads) seed_kernel(const RunArgs p, const int *roots, int n_roots) {
+    __shared__ long long cnt[kNumQueues][kSeedThreads];
+    __shared__ long long total[kNumQueues];
+    const int tid = threadIdx.x;
+    const int per = (n_roots + kSeedThreads - 1) / kSeedThreads;
+    const int r0 = min(n_roots, tid * per), r1 = min(n_roots, r0 + per);
+    long long c[kNumQueues] = {};
+    for (int r = r0; r < r1; ++r) {
+        const int task = roots[r];
+        c[p.tasks[task].queue] += p.tasks[task].n_items;
+    }
+#pragma unroll
+    for (int q = 0; q < kNumQueues; ++q) cnt[q][tid] = c[q];
+    __syncthreads();
+    if (tid < kNumQueues) {  // exclusive scan of queue tid's counts
+        long long run = 0;
+        for (int i = 0; i < kSeedThreads; ++i) {
+            const long long v = cnt[tid][i];
+            cnt[tid][i] = run;
+            run += v;
+        }
+        total[tid] = run;
+    }
+    __syncthreads();
+    long long off[kNumQueues];
+#pragma unroll
+    for (int q = 0; q < kNumQueues; ++q) off[q] = cnt[q][tid];
+    for (int r = r0; r < r1; ++r) {
+        const int task = roots[r];
+        const int q = p.tasks[task].queue, n = p.tasks[task].n_items;
+        if (off[q] + n > p.queue_cap[q]) break;  // reported below
+        for (int i = 0; i < n; ++i)
+            p.queue[q][off[q] + i] = (static_cast<unsigned long long>(task) << 32) | static_cast<unsigned int>(i);
+        off[q] += n;
+    }
+    __threadfence();  // the slots before the counts that let consumers claim them
+    __syncthreads();
+    if (tid == 0) {
+        for (int q = 0; q < kNumQueues; ++q) {
+            if (total[q] > p.queue_cap[q]) {
+                report_error(p.ctl, MTD_ERR_QUEUE, 0);
+                continue;
+            }
+            p.qctl[q].tail = static_cast<unsigned long long>(total[q]);
+            add_avail(&p.qctl[q].avail, total[q]);
+        }
         __threadfence();
     }
 }

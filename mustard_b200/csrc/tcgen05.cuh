@@ -333,7 +333,7 @@ enum { kTmaNone = 0, kTmaMap2D = 1, kTmaMap3D = 2 };
 // stage is reloaded after its MMAs are done.  On a true return every MMA has completed (the
 // accumulator is final and every stage free); false if a wait timed out.  Operands must
 // already be TF32 values (the tensor core truncates what it reads).
-__device__ bool mainloop_tma(State *st, uint8_t *smem, const void *map, int map_kind, int a_row, int b_row, int k0,
+static __device__ bool mainloop_tma(State *st, uint8_t *smem, const void *map, int map_kind, int a_row, int b_row, int k0,
                              int K, uint32_t acc, unsigned long long timeout_ns) {
     bool ok = true;
     {
@@ -421,7 +421,7 @@ static_assert(kBfStages <= kStages, "BF16 stages use the engine's barriers");
 constexpr uint32_t kIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
                                 (uint32_t(kN >> 3) << 17) | (uint32_t(kM >> 4) << 24);
 
-__device__ bool mainloop_tma_bf16(State *st, uint8_t *smem, const void *map, int a_row, int b_row, int k0, int K,
+static __device__ bool mainloop_tma_bf16(State *st, uint8_t *smem, const void *map, int a_row, int b_row, int k0, int K,
                                   uint32_t acc, unsigned long long timeout_ns) {
     bool ok = true;
     {
@@ -525,7 +525,7 @@ __device__ __forceinline__ int ws_bk(int kind) { return kind == kWsBf16 ? kBfBK 
 
 // Thread 0: load the item's K / bk slices (A rows a_row .., B rows b_row .., columns k0 ..).
 // False if a wait for a free stage ran past the deadline.
-__device__ bool ws_load(WsState *w, uint8_t *ring, const void *map, int kind, int a_row, int b_row, int k0, int K,
+static __device__ bool ws_load(WsState *w, uint8_t *ring, const void *map, int kind, int a_row, int b_row, int k0, int K,
                         unsigned long long deadline) {
     asm volatile("fence.proxy.async.global;" ::: "memory");       // operands other CTAs wrote
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the ring's earlier generic use
@@ -561,7 +561,7 @@ __device__ bool ws_load(WsState *w, uint8_t *ring, const void *map, int kind, in
 
 // Thread 32: acc(128 x 128) = A B^T over the item's slices as they land; commits each slice to
 // its stage's `empty` barrier and the whole item to accf[buf].  False on a timed-out wait.
-__device__ bool ws_mma(WsState *w, uint8_t *ring, int kind, int K, uint32_t acc, int buf,
+static __device__ bool ws_mma(WsState *w, uint8_t *ring, int kind, int K, uint32_t acc, int buf,
                        unsigned long long deadline) {
     const int bk = ws_bk(kind), nk = K / bk;
     uint32_t g = w->cons;
@@ -705,7 +705,7 @@ constexpr int kX3StageBytes = 4 * kX3OperandBytes;        // 64 KB
 static_assert(kX3Stages * kX3StageBytes <= kSmemBytes, "three-pass stages fit the engine's shared memory");
 static_assert(kX3Stages <= kStages, "three-pass stages use the engine's barriers");
 
-__device__ bool mainloop_tma_x3(State *st, uint8_t *smem, const void *map, const void *map_lo, int a_row, int b_row,
+static __device__ bool mainloop_tma_x3(State *st, uint8_t *smem, const void *map, const void *map_lo, int a_row, int b_row,
                                 int k0, int K, uint32_t acc, unsigned long long timeout_ns) {
     bool ok = true;
     {
