@@ -260,6 +260,7 @@ def reference_gpu_baseline(n, timeout):
 # one ncu capture and is reported only while these files still hash to the captured state.
 TRAFFIC_SOURCES = ["mustard_b200/csrc/scheduler.cuh", "mustard_b200/csrc/mma.cuh", "mustard_b200/csrc/tile_ops.cuh",
                    "mustard_b200/csrc/tma64.cuh", "mustard_b200/csrc/tcgen05.cuh", "mustard_b200/csrc/adjoint_ops.cuh",
+                   "mustard_b200/csrc/batch_ops.cuh", "mustard_b200/csrc/lupiv_ops.cuh", "mustard_b200/csrc/sync_util.cuh",
                    "mustard_b200/csrc/device_types.hpp", "mustard_b200/csrc/dag.cpp"]
 
 

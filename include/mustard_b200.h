@@ -364,6 +364,27 @@ int mtd_batch_destroy(mtd_batch *b);
 int mtd_batch_autotune(int count, const int64_t *n, int prec, int64_t *tile_out, int *nest_out, double *trial_ms,
                        void *stream);
 
+/* ---- LU with partial pivoting (no counterpart in the reference) ----
+ *
+ * LAPACK dgetrf's factorisation (P A = L U, row interchanges chosen by the largest |a| of
+ * each column, the first such row on ties) as a device-side task graph of one persistent
+ * launch: per block column of `tile` elements a panel task whose items (at most one per SM)
+ * factor the panel together, the panel's row interchanges on the other block columns, a
+ * unit-lower TRSM and a GEMM update.  tile: 64 or 128 (each item keeps its panel rows in
+ * shared memory, ~213 rows of 128 at most, and one item per SM: n up to ~31,000 at tile 128;
+ * MTD_ERR_INVALID_ARG beyond).  d_ipiv: n device
+ * ints, LAPACK's 1-based ipiv on return.  A zero pivot does not stop the factorisation; the
+ * status call reports the first one as info (1-based column), as dgetrf does. */
+typedef struct mtd_lupiv mtd_lupiv;
+int mtd_lupiv_create(mtd_lupiv **out, int64_t n, int64_t tile);
+int mtd_lupiv_num_tasks(const mtd_lupiv *h);
+/* Stream-ordered; wait with mtd_lupiv_status. */
+int mtd_lupiv_run(mtd_lupiv *h, double *dA, int64_t lda, int *d_ipiv, void *stream);
+int mtd_lupiv_status(mtd_lupiv *h, int *info);
+int mtd_lupiv_destroy(mtd_lupiv *h);
+/* One call: create, run, wait, destroy. */
+int mtd_lu_pivot(double *dA, int64_t n, int64_t lda, int64_t tile, int *d_ipiv, void *stream, int *info);
+
 /* ---- Cholesky adjoint (no counterpart in the reference) ----
  *
  * Reverse-mode derivative of A = L L^T: given the factor L and Lbar = dLoss/dL (lower

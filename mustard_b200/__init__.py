@@ -26,7 +26,7 @@ from ._capi import (  # noqa: F401  (re-exported constants)
     lib, lib_path)
 
 __all__ = [
-    "TaskGraph", "TiledGraphCreator", "tiled_cholesky", "tiled_lu", "generate", "colmajor",
+    "TaskGraph", "TiledGraphCreator", "tiled_cholesky", "tiled_lu", "lu_pivot", "PivotedLU", "generate", "colmajor",
     "probe_fp64_peak", "MtdError", "lib", "lib_path",
 ]
 
@@ -579,6 +579,61 @@ def tiled_lu(a, tile, stream=None):
     """In-place no-pivot LU of the column-major CUDA matrix ``a`` (tiledLU,
     mustard/lu_mustard.cu:256)."""
     return _one_call(KIND_LU, a, tile, stream)
+
+
+class PivotedLU:
+    """LU with partial pivoting (mtd_lupiv): P A = L U with LAPACK dgetrf's interchanges, as
+    one persistent launch over a task graph built once for (n, tile).  No counterpart in
+    the reference, which factors without pivoting."""
+
+    def __init__(self, n, tile=128):
+        self._lib = lib()
+        h = ctypes.c_void_p()
+        _capi.check(self._lib.mtd_lupiv_create(ctypes.byref(h), n, tile))
+        self._h, self.n, self.tile = h, n, tile
+
+    @property
+    def num_tasks(self):
+        return self._lib.mtd_lupiv_num_tasks(self._h)
+
+    def run(self, a, ipiv, stream=None):
+        """Factor the column-major float64 CUDA matrix ``a`` in place; ``ipiv``: an int32
+        CUDA tensor of n entries (LAPACK's 1-based pivots on completion).  Stream-ordered."""
+        ptr, n, ld = _matrix_ptr(a)
+        if n != self.n or ipiv.numel() < n or not ipiv.is_cuda or ipiv.element_size() != 4:
+            raise ValueError("matrix size or pivot vector does not match")
+        self._keep = (a, ipiv)
+        _capi.check(self._lib.mtd_lupiv_run(self._h, ctypes.c_void_p(ptr), ld, ctypes.c_void_p(ipiv.data_ptr()),
+                                            _stream_handle(stream)))
+
+    def status(self):
+        """Wait for the last run; returns LAPACK's info (0, or the first zero pivot's column)."""
+        info = ctypes.c_int(0)
+        _capi.check(self._lib.mtd_lupiv_status(self._h, ctypes.byref(info)))
+        return info.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.mtd_lupiv_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def lu_pivot(a, tile=128, stream=None):
+    """In-place LU with partial pivoting of the column-major float64 CUDA matrix ``a``
+    (dgetrf's result); returns (info, ipiv) with ipiv an int32 CUDA tensor, 1-based."""
+    import torch
+    ptr, n, ld = _matrix_ptr(a)
+    ipiv = torch.empty(n, dtype=torch.int32, device=a.device)
+    info = ctypes.c_int(0)
+    _capi.check(lib().mtd_lu_pivot(ctypes.c_void_p(ptr), n, ld, tile, ctypes.c_void_p(ipiv.data_ptr()),
+                                   _stream_handle(stream), ctypes.byref(info)))
+    return info.value, ipiv
 
 
 def generate(a, which, seed=0, alpha=1.0, stream=None):

@@ -69,6 +69,12 @@ SIGNATURES = {
                                      _vp]),
     "mtd_batch_destroy": (_i, [_vp]),
     "mtd_batch_autotune": (_i, [_i, _pi64, _i, _pi64, ctypes.POINTER(_i), ctypes.POINTER(_d), _vp]),
+    "mtd_lupiv_create": (_i, [ctypes.POINTER(_vp), _i64, _i64]),
+    "mtd_lupiv_num_tasks": (_i, [_vp]),
+    "mtd_lupiv_run": (_i, [_vp, _vp, _i64, _vp, _vp]),
+    "mtd_lupiv_status": (_i, [_vp, ctypes.POINTER(_i)]),
+    "mtd_lupiv_destroy": (_i, [_vp]),
+    "mtd_lu_pivot": (_i, [_vp, _i64, _i64, _i64, _vp, _vp, ctypes.POINTER(_i)]),
     "mtd_adjoint_create": (_i, [ctypes.POINTER(_vp), _i, _pi64, _i64, _i]),
     "mtd_adjoint_num_tasks": (_i, [_vp]),
     "mtd_adjoint_run": (_i, [_vp, _pp, _pi64, _pp, _pi64, _vp]),

@@ -20,7 +20,7 @@ CUDA_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr
 # engine-shape overrides for tuning builds, e.g. MTD_NVCC_EXTRA="-DMTD_PANEL_STAGES=4"
 CUDA_FLAGS += os.environ.get("MTD_NVCC_EXTRA", "").split()
 
-LIB_SOURCES = ["runtime.cu", "batch_run.cu", "gen.cu", "dag.cpp", "solver.cu", "batch.cu", "adjoint.cu"]
+LIB_SOURCES = ["runtime.cu", "batch_run.cu", "gen.cu", "dag.cpp", "solver.cu", "batch.cu", "adjoint.cu", "lupiv.cu"]
 CLI_PROGRAMS = {"lu_mustard": "lu_mustard.cpp", "cholesky_mustard": "cholesky_mustard.cpp"}
 PROBES = {"dmma_probe": os.path.join(PKG, "probe", "dmma_probe.cu")}  # measurement tools
 

@@ -1,7 +1,7 @@
-// The batched factor-and-solve launch (mtd_batch_factor_solve): the persistent kernel's
-// instances that also run the per-matrix conversion and solve tasks (scheduler.cuh,
-// SOLVE = true), in their own translation unit so the factorisation-only instances in
-// runtime.cu stay as they are.
+// The launches of the batched factor-and-solve (mtd_batch_factor_solve) and of the pivoted
+// LU (mtd_lupiv): the persistent kernel's instances that also run their own tasks
+// (scheduler.cuh, SOLVE = true), in their own translation unit so the factorisation-only
+// instances in runtime.cu stay as they are.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -40,6 +40,9 @@ int solve_smem_setup(int device) {
 }
 
 }  // namespace
+
+// Dynamic shared memory of the persistent kernel (what a pivoted panel item may use).
+int ext_op_smem_bytes() { return kOpSmemBytes(); }
 
 // Reset the run's counters and queues, seed the roots, and launch the SOLVE instance for the
 // batch's precision (prec) and operand alignment (vec2) on `grid` CTAs.

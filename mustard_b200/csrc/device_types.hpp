@@ -27,6 +27,10 @@ constexpr int kOpBatchSolve = 101;    // one item: solve (+ refine) one matrix o
 constexpr int kOpBatchConvert = 102;  // items = 128-column strips: F = lower(A) + shift I, as T
 constexpr int kConvertCols = 128;
 constexpr int kBatchInfoOk = 0x7f7f7f7f;  // per-matrix info of a batched run before any bad pivot
+// Pivoted LU (mtd_lupiv): a panel factorisation with partial pivoting (P cooperating items)
+// and the row interchanges of one block column.
+constexpr int kOpPanelPiv = 103;
+constexpr int kOpLaswp = 104;
 
 // Cholesky adjoint operations (device tasks of the reverse sweep; see adjoint_ops.cuh).
 constexpr int kOpAdjTrsm = 20;    // C(m x n) := C * L^-1, L = n x n lower at (ar, ac) of the factor
@@ -178,6 +182,12 @@ struct RunArgs {
     double solve_shift;
     int solve_method;
     int solve_max_iter;
+    // Pivoted LU runs only: the pivot vector (ipiv, 1-based rows as LAPACK's), one arrival
+    // counter per panel (zeroed by the per-run reset) and the panel items' exchange slots.
+    int *ipiv;
+    unsigned int *panel_bar;
+    int n_panel_bar;
+    double *panel_slots;
 };
 
 }  // namespace mtd

@@ -26,6 +26,8 @@
 #include "device_types.hpp"
 #include "adjoint_ops.cuh"
 #include "batch_ops.cuh"
+#include "lupiv_ops.cuh"
+#include "sync_util.cuh"
 #include "tcgen05.cuh"
 #include "tile_ops.cuh"
 
@@ -33,17 +35,6 @@ namespace mtd {
 
 constexpr unsigned long long kEmptySlot = ~0ull;
 enum { kCmdWork = 0, kCmdExit = 1, kCmdNone = 2 };
-
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ unsigned long long ld_volatile(const unsigned long long *p) {
-    return *reinterpret_cast<const volatile unsigned long long *>(p);
-}
-__device__ __forceinline__ int ld_volatile(const int *p) { return *reinterpret_cast<const volatile int *>(p); }
 
 // Signed fetch-and-add on a queue's `avail` count (two's complement in 64 bits).
 __device__ __forceinline__ long long add_avail(long long *c, long long v) {
@@ -274,14 +265,19 @@ __device__ __noinline__ int op_batch_convert(const RunArgs &p, const DevTask &t,
     return 0;
 }
 
-// SOLVE: the instances of the batched factor-and-solve launch, which also run the solve and
-// conversion tasks; the other instances carry none of that code.
+// SOLVE: the instances of the batched factor-and-solve launch and of the pivoted LU, which
+// also run their own tasks (solve, conversion; pivoted panel, row interchanges); the other
+// instances carry none of that code.
 template <int VEC, typename T, int SPLIT = 1, bool ADJ = false, bool SOLVE = false>
 __device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int item, void *smem,
                                         tc::State *tcs = nullptr, t64::State *s64 = nullptr) {
     if constexpr (SOLVE) {
         if (t.op == kOpBatchSolve) return op_batch_solve<T>(p, t, smem);
         if (t.op == kOpBatchConvert) return op_batch_convert<T>(p, t, item);
+        if constexpr (sizeof(T) == 8) {
+            if (t.op == kOpPanelPiv) return op_panel_piv(p, mat_ctx<T>(p, t), t, item, smem);
+            if (t.op == kOpLaswp) return op_laswp(p, mat_ctx<T>(p, t), t, item, smem);
+        }
     }
     if (t.op == kOpJoin) return 0;  // a join's one item: nothing to compute
     if constexpr (ADJ) return dispatch_adjoint<T, VEC, SPLIT>(p, t, item, smem);
@@ -635,6 +631,7 @@ static __global__ void reset_kernel(const RunArgs p, const int *deps_init) {
         p.deps[i] = deps_init[i];
         p.items_left[i] = p.tasks[i].n_items;
     }
+    for (long long i = tid; i < p.n_panel_bar; i += stride) p.panel_bar[i] = 0u;
     for (int q = 0; q < kNumQueues; ++q)
         for (long long i = tid; i < p.queue_cap[q]; i += stride) p.queue[q][i] = kEmptySlot;
     if (tid == 0) {

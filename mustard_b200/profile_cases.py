@@ -7,6 +7,9 @@
     python -m mustard_b200.profile_cases chol --n 6144 --tile 512
     python -m mustard_b200.profile_cases lu   --n 6144 --tile 512
         a whole tiled factorisation
+    python -m mustard_b200.profile_cases lupiv --n 8192 --tile 128
+        LU with partial pivoting (mtd_lupiv) of a U[-1, 1) matrix (no diagonal boost, so most
+        rows are interchanged)
     python -m mustard_b200.profile_cases gemm --n 8192 --tile 1024 --prec tf32
         the same cases on a float32 matrix with TF32 tensor-core products (tcgen05 GEMM /
         SYRK items fed by TMA; Cholesky and the GEMM-only step only); --prec bf16 (BF16
@@ -55,7 +58,7 @@ def op_breakdown(g):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["gemm", "chol", "lu"])
+    ap.add_argument("case", choices=["gemm", "chol", "lu", "lupiv"])
     ap.add_argument("--n", type=int, default=6144)
     ap.add_argument("--tile", type=int, default=768)
     ap.add_argument("--runs", type=int, default=2)
@@ -68,6 +71,8 @@ def main():
         ap.error("the low-precision paths factor SPD matrices only (chol, gemm)")
     n, b = args.n, args.tile
     t = (n + b - 1) // b
+    if args.case == "lupiv":
+        return run_pivoted(n, b, args.runs)
     a = torch.empty((n, n), dtype=torch.float64, device="cuda").t()
     if args.case == "lu":
         mtd.generate(a, mtd.GEN_UNIFORM_DIAG, seed=3)
@@ -121,6 +126,28 @@ def main():
                                 else trace_analysis.summary(g, recs))["critical_path"]
     print(json.dumps(rec))
     g.close()
+
+
+def run_pivoted(n, b, runs):
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    src = (torch.rand((n, n), generator=gen, dtype=torch.float64, device="cuda") * 2.0 - 1.0).t()
+    a = torch.empty_like(src)
+    ipiv = torch.empty(n, dtype=torch.int32, device="cuda")
+    h = mtd.PivotedLU(n, b)
+    s = torch.cuda.current_stream()
+    ms = 0.0
+    for _ in range(runs):
+        a.copy_(src)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        h.run(a, ipiv, stream=s)
+        e1.record(s)
+        info = h.status()
+        ms = e0.elapsed_time(e1)
+    swapped = int((ipiv.cpu() != torch.arange(1, n + 1, dtype=torch.int32)).sum())
+    print(json.dumps({"case": "lupiv", "prec": "fp64", "n": n, "tile": b, "tasks": h.num_tasks, "ms": ms,
+                      "tflops": 2.0 * n ** 3 / 3 / (ms * 1e-3) / 1e12, "info": info, "rows_interchanged": swapped}))
+    h.close()
 
 
 if __name__ == "__main__":
