@@ -33,6 +33,11 @@
 
 namespace mtd {
 
+// 1: the FP64 persistent loop completes an item on thread 32 while thread 0 claims the next.
+#ifndef MTD_OVERLAP_FINISH
+#define MTD_OVERLAP_FINISH 0
+#endif
+
 constexpr unsigned long long kEmptySlot = ~0ull;
 enum { kCmdWork = 0, kCmdExit = 1, kCmdNone = 2 };
 
@@ -581,6 +586,37 @@ __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const __grid_co
         __shared__ t64::State s64;
         constexpr bool kT64 = T64 && sizeof(T) == 8 && !ADJ;
         if constexpr (kT64) t64::init(&s64);
+#if MTD_OVERLAP_FINISH
+        // thread 32 completes the previous item (releasing its successors) while thread 0
+        // claims the next one; a claim that waits for those successors ends when thread 32
+        // has released them
+        __shared__ int s_st;
+        int prev_task = -1, prev_item = 0, prev_ok = 0;
+        unsigned long long prev_start = 0ull;
+        while (true) {
+            if (threadIdx.x == 0) {
+                int tk = 0, it = 0;
+                s_cmd = pop_item(p, &tk, &it);
+                s_task = tk;
+                s_item = it;
+            } else if (threadIdx.x == 32 && prev_task >= 0) {
+                finish_item(p, prev_task, prev_item, prev_start, prev_ok != 0);
+            }
+            __syncthreads();
+            const int cmd = s_cmd, task = s_task, item = s_item;
+            if (cmd != kCmdWork) break;
+            const unsigned long long t_start = p.trace ? global_ns() : 0ull;
+            DevTask t;
+            load_task(p, task, &t);
+            const int st = dispatch<VEC, T, SPLIT, ADJ, SOLVE>(p, t, item, smem, nullptr, kT64 ? &s64 : nullptr);
+            if (threadIdx.x == 0) s_st = st;
+            __syncthreads();
+            prev_task = task;
+            prev_item = item;
+            prev_start = t_start;
+            prev_ok = s_st == 0;
+        }
+#else
         while (true) {
             if (threadIdx.x == 0) {
                 int tk = 0, it = 0;
@@ -598,6 +634,7 @@ __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const __grid_co
             __syncthreads();
             if (threadIdx.x == 0) finish_item(p, task, item, t_start, st == 0);
         }
+#endif
     }
 }
 

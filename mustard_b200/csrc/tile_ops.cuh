@@ -60,6 +60,18 @@ using GemmMma =
     BlockMmaT<T, kGemmTile, kGemmTile, kGemmWarpsM, kGemmWarpsN, BL, VEC, MTD_GEMM_STAGES, MTD_GEMM_BK, SPLIT>;
 template <int BL, int VEC, typename T = double, int SPLIT = 1>
 using PanelMma = BlockMmaT<T, 64, 64, kPanelWarpsM, kPanelWarpsN, BL, VEC, MTD_PANEL_STAGES, MTD_PANEL_BK, SPLIT>;
+// The TRSM strips' updates over two inverse blocks at a time (MTD_TRSM_WIDE=1): 64 x 128
+// (row strips: TRSM_RLT, TRSM_RUN) and 128 x 64 (column strips: TRSM_LLNU) output blocks,
+// one 16 x 32 warp tile per warp; half the steps, each with one engine fill and one C
+// update.  Measured on one B200 (N = 24000, tile 1536): Cholesky 153.5 -> 151.3 ms, LU
+// unchanged (297.8 / 297.6 ms).
+#ifndef MTD_TRSM_WIDE
+#define MTD_TRSM_WIDE 1
+#endif
+template <int BL, int VEC, typename T = double, int SPLIT = 1>
+using WideMma = BlockMmaT<T, 64, 128, 4, kThreads / 32 / 4, BL, VEC, MTD_PANEL_STAGES, MTD_PANEL_BK, SPLIT>;
+template <int VEC>
+using TallMma = BlockMmaT<double, 128, 64, kThreads / 32 / 2, 2, kBKContig, VEC, MTD_PANEL_STAGES, MTD_PANEL_BK>;
 
 __device__ __forceinline__ void block_fence_sync() {
     __threadfence_block();
@@ -548,6 +560,33 @@ __device__ int op_getrf(const RunArgs &p, const MatCtx &m, const DevTask &t, voi
 // left-looking over the kNB-wide diagonal blocks of the triangular block.
 // ---------------------------------------------------------------------------------
 
+// An engine's k-loop: BlockMmaT::run, or its split-phase form (run_sp) when SP; false (after
+// reporting MTD_ERR_TIMEOUT) if a wait of the latter expired.
+template <bool SP, typename E, typename T>
+__device__ __forceinline__ bool eng_run(const RunArgs &p, E &e, void *smem, const T *A, int64_t lda, const T *B,
+                                        int64_t ldb, int M, int N, int K) {
+    if constexpr (SP) {
+        if (!e.run_sp(smem, A, lda, B, ldb, M, N, K)) {
+            if (threadIdx.x == 0) report_error(p.ctl, MTD_ERR_TIMEOUT, 0);
+            return false;
+        }
+    } else {
+        e.run(smem, A, lda, B, ldb, M, N, K);
+    }
+    return true;
+}
+// The update items' k-loop (MTD_SPLIT_PHASE) and the TRSM strips' (MTD_SPLIT_PHASE_TRSM).
+template <typename E, typename T>
+__device__ __forceinline__ bool gemm_run(const RunArgs &p, E &e, void *smem, const T *A, int64_t lda, const T *B,
+                                         int64_t ldb, int M, int N, int K) {
+    return eng_run<MTD_SPLIT_PHASE != 0>(p, e, smem, A, lda, B, ldb, M, N, K);
+}
+template <typename E, typename T>
+__device__ __forceinline__ bool trsm_run(const RunArgs &p, E &e, void *smem, const T *A, int64_t lda, const T *B,
+                                         int64_t ldb, int M, int N, int K) {
+    return eng_run<MTD_SPLIT_PHASE_TRSM != 0>(p, e, smem, A, lda, B, ldb, M, N, K);
+}
+
 // X = X * L^-T   (cublasDtrsm R, L, T, NonUnit; cholesky_mustard.cu:281)
 template <typename T, int VEC, int SPLIT = 1>
 __device__ int op_trsm_rlt(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
@@ -559,18 +598,11 @@ __device__ int op_trsm_rlt(const RunArgs &p, const MatCtx &m, const DevTask &t, 
     T *X = at<T>(m, t.cr + r0, t.cc);
     const T *L = at<T>(m, t.ar, t.ac);
     const T *W = ws_lo<T>(m) + t.ar;
-    for (int jb = 0; jb < nk; jb += kNB) {
-        const int jn = min(kNB, nk - jb);
-        if (jb > 0) {
-            Mn e;
-            e.zero();
-            e.run(smem, X, lda, L + jb, lda, mm, jn, jb);
-            e.sub_from(X + int64_t(jb) * lda, lda, mm, jn);
-            block_fence_sync();
-        }
+    // X(:, jb .. jb + jn) = X(:, jb .. jb + jn) W_jb^T (W_jb: the inverse of that diagonal block)
+    auto solve_block = [&](int jb, int jn) {
         Mn e;
         e.zero();
-        e.run(smem, X + int64_t(jb) * lda, lda, W + jb, ldw, mm, jn, jn);
+        if (!trsm_run(p, e, smem, X + int64_t(jb) * lda, lda, W + jb, ldw, mm, jn, jn)) return false;
         e.store_rounded_to(X + int64_t(jb) * lda, lda, mm, jn);  // panel of L: an operand of the updates
         if constexpr (sizeof(T) == 4)
             if (p.bf16)  // BF16-update runs: the updates read the panel from its BF16 copy
@@ -580,7 +612,44 @@ __device__ int op_trsm_rlt(const RunArgs &p, const MatCtx &m, const DevTask &t, 
             if (p.lo)  // FP32-accurate runs: the three-pass updates read the panel's low part
                 e.store_lo_to(static_cast<float *>(p.lo) + (t.cr + r0) + int64_t(t.cc + jb) * p.lo_ld, p.lo_ld, mm, jn);
         block_fence_sync();
+        return true;
+    };
+#if MTD_TRSM_WIDE
+    using Mw = WideMma<kBNContig, VEC, T, SPLIT>;
+    for (int jb = 0; jb < nk; jb += 2 * kNB) {
+        const int jw = min(2 * kNB, nk - jb);
+        if (jb > 0) {  // X(:, jb .. jb + jw) -= X(:, 0 .. jb) L(jb .. jb + jw, 0 .. jb)^T
+            Mw e;
+            e.zero();
+            if (!trsm_run(p, e, smem, X, lda, L + jb, lda, mm, jw, jb)) return MTD_ERR_TIMEOUT;
+            e.sub_from(X + int64_t(jb) * lda, lda, mm, jw);
+            block_fence_sync();
+        }
+        if (!solve_block(jb, min(kNB, jw))) return MTD_ERR_TIMEOUT;
+        if (jw > kNB) {  // the second block's update by the first, then its solve
+            Mn e;
+            e.zero();
+            if (!trsm_run(p, e, smem, X + int64_t(jb) * lda, lda, L + (jb + kNB) + int64_t(jb) * lda, lda, mm,
+                          jw - kNB, kNB))
+                return MTD_ERR_TIMEOUT;
+            e.sub_from(X + int64_t(jb + kNB) * lda, lda, mm, jw - kNB);
+            block_fence_sync();
+            if (!solve_block(jb + kNB, jw - kNB)) return MTD_ERR_TIMEOUT;
+        }
     }
+#else
+    for (int jb = 0; jb < nk; jb += kNB) {
+        const int jn = min(kNB, nk - jb);
+        if (jb > 0) {
+            Mn e;
+            e.zero();
+            if (!trsm_run(p, e, smem, X, lda, L + jb, lda, mm, jn, jb)) return MTD_ERR_TIMEOUT;
+            e.sub_from(X + int64_t(jb) * lda, lda, mm, jn);
+            block_fence_sync();
+        }
+        if (!solve_block(jb, jn)) return MTD_ERR_TIMEOUT;
+    }
+#endif
     return 0;
 }
 
@@ -595,21 +664,50 @@ __device__ int op_trsm_run(const RunArgs &p, const MatCtx &m, const DevTask &t, 
     double *X = at<double>(m, t.cr + r0, t.cc);
     const double *U = at<double>(m, t.ar, t.ac);
     const double *W = ws_up<double>(m) + t.ar;
+    auto solve_block = [&](int jb, int jn) {
+        Mk e;
+        e.zero();
+        if (!trsm_run(p, e, smem, X + int64_t(jb) * lda, lda, W + jb, ldw, mm, jn, jn)) return false;
+        e.store_to(X + int64_t(jb) * lda, lda, mm, jn);
+        block_fence_sync();
+        return true;
+    };
+#if MTD_TRSM_WIDE
+    using Mw = WideMma<kBKContig, VEC>;
+    for (int jb = 0; jb < nk; jb += 2 * kNB) {
+        const int jw = min(2 * kNB, nk - jb);
+        if (jb > 0) {  // X(:, jb .. jb + jw) -= X(:, 0 .. jb) U(0 .. jb, jb .. jb + jw)
+            Mw e;
+            e.zero();
+            if (!trsm_run(p, e, smem, X, lda, U + int64_t(jb) * lda, lda, mm, jw, jb)) return MTD_ERR_TIMEOUT;
+            e.sub_from(X + int64_t(jb) * lda, lda, mm, jw);
+            block_fence_sync();
+        }
+        if (!solve_block(jb, min(kNB, jw))) return MTD_ERR_TIMEOUT;
+        if (jw > kNB) {
+            Mk e;
+            e.zero();
+            if (!trsm_run(p, e, smem, X + int64_t(jb) * lda, lda, U + jb + int64_t(jb + kNB) * lda, lda, mm,
+                          jw - kNB, kNB))
+                return MTD_ERR_TIMEOUT;
+            e.sub_from(X + int64_t(jb + kNB) * lda, lda, mm, jw - kNB);
+            block_fence_sync();
+            if (!solve_block(jb + kNB, jw - kNB)) return MTD_ERR_TIMEOUT;
+        }
+    }
+#else
     for (int jb = 0; jb < nk; jb += kNB) {
         const int jn = min(kNB, nk - jb);
         if (jb > 0) {
             Mk e;
             e.zero();
-            e.run(smem, X, lda, U + int64_t(jb) * lda, lda, mm, jn, jb);
+            if (!trsm_run(p, e, smem, X, lda, U + int64_t(jb) * lda, lda, mm, jn, jb)) return MTD_ERR_TIMEOUT;
             e.sub_from(X + int64_t(jb) * lda, lda, mm, jn);
             block_fence_sync();
         }
-        Mk e;
-        e.zero();
-        e.run(smem, X + int64_t(jb) * lda, lda, W + jb, ldw, mm, jn, jn);
-        e.store_to(X + int64_t(jb) * lda, lda, mm, jn);
-        block_fence_sync();
+        if (!solve_block(jb, jn)) return MTD_ERR_TIMEOUT;
     }
+#endif
     return 0;
 }
 
@@ -624,21 +722,49 @@ __device__ int op_trsm_llnu(const RunArgs &p, const MatCtx &m, const DevTask &t,
     double *X = at<double>(m, t.cr, t.cc + c0);
     const double *L = at<double>(m, t.ar, t.ac);
     const double *W = ws_lo<double>(m) + t.ar;
+    auto solve_block = [&](int jb, int jn) {
+        Mk e;
+        e.zero();
+        if (!trsm_run(p, e, smem, W + jb, ldw, X + jb, lda, jn, nc, jn)) return false;
+        e.store_to(X + jb, lda, jn, nc);
+        block_fence_sync();
+        return true;
+    };
+#if MTD_TRSM_WIDE
+    using Mt = TallMma<VEC>;
+    for (int jb = 0; jb < nk; jb += 2 * kNB) {
+        const int jw = min(2 * kNB, nk - jb);
+        if (jb > 0) {  // X(jb .. jb + jw, :) -= L(jb .. jb + jw, 0 .. jb) X(0 .. jb, :)
+            Mt e;
+            e.zero();
+            if (!trsm_run(p, e, smem, L + jb, lda, X, lda, jw, nc, jb)) return MTD_ERR_TIMEOUT;
+            e.sub_from(X + jb, lda, jw, nc);
+            block_fence_sync();
+        }
+        if (!solve_block(jb, min(kNB, jw))) return MTD_ERR_TIMEOUT;
+        if (jw > kNB) {
+            Mk e;
+            e.zero();
+            if (!trsm_run(p, e, smem, L + (jb + kNB) + int64_t(jb) * lda, lda, X + jb, lda, jw - kNB, nc, kNB))
+                return MTD_ERR_TIMEOUT;
+            e.sub_from(X + jb + kNB, lda, jw - kNB, nc);
+            block_fence_sync();
+            if (!solve_block(jb + kNB, jw - kNB)) return MTD_ERR_TIMEOUT;
+        }
+    }
+#else
     for (int jb = 0; jb < nk; jb += kNB) {
         const int jn = min(kNB, nk - jb);
         if (jb > 0) {
             Mk e;
             e.zero();
-            e.run(smem, L + jb, lda, X, lda, jn, nc, jb);
+            if (!trsm_run(p, e, smem, L + jb, lda, X, lda, jn, nc, jb)) return MTD_ERR_TIMEOUT;
             e.sub_from(X + jb, lda, jn, nc);
             block_fence_sync();
         }
-        Mk e;
-        e.zero();
-        e.run(smem, W + jb, ldw, X + jb, lda, jn, nc, jn);
-        e.store_to(X + jb, lda, jn, nc);
-        block_fence_sync();
+        if (!solve_block(jb, jn)) return MTD_ERR_TIMEOUT;
     }
+#endif
     return 0;
 }
 
@@ -692,7 +818,8 @@ __device__ int op_gemm_nt(const RunArgs &p, const MatCtx &m, const DevTask &t, i
                                            at<double>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn, false);
     Mg e;
     e.zero();
-    e.run(smem, at<T>(m, t.ar + r0, t.ac), m.lda, at<T>(m, t.br + c0, t.bc), m.lda, mm, nn, t.k);
+    if (!gemm_run(p, e, smem, at<T>(m, t.ar + r0, t.ac), m.lda, at<T>(m, t.br + c0, t.bc), m.lda, mm, nn, t.k))
+        return MTD_ERR_TIMEOUT;
     e.sub_from(at<T>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn);
     return 0;
 }
@@ -711,7 +838,9 @@ __device__ int op_gemm_nn(const RunArgs &p, const MatCtx &m, const DevTask &t, i
                                            at<double>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn, false);
     Mg e;
     e.zero();
-    e.run(smem, at<double>(m, t.ar + r0, t.ac), m.lda, at<double>(m, t.br, t.bc + c0), m.lda, mm, nn, t.k);
+    if (!gemm_run(p, e, smem, at<double>(m, t.ar + r0, t.ac), m.lda, at<double>(m, t.br, t.bc + c0), m.lda, mm, nn,
+                  t.k))
+        return MTD_ERR_TIMEOUT;
     e.sub_from(at<double>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn);
     return 0;
 }
@@ -732,7 +861,8 @@ __device__ int op_syrk_ln(const RunArgs &p, const MatCtx &m, const DevTask &t, i
                                            at<double>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn, pb == qb);
     Mg e;
     e.zero();
-    e.run(smem, at<T>(m, t.ar + r0, t.ac), m.lda, at<T>(m, t.ar + c0, t.ac), m.lda, mm, nn, t.k);
+    if (!gemm_run(p, e, smem, at<T>(m, t.ar + r0, t.ac), m.lda, at<T>(m, t.ar + c0, t.ac), m.lda, mm, nn, t.k))
+        return MTD_ERR_TIMEOUT;
     e.sub_from(at<T>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn, pb == qb, 0, 0);
     return 0;
 }
@@ -750,8 +880,18 @@ constexpr int kOpSmemBytes() {
                            ? PanelMma<kBNContig, 2>::SMEM_BYTES
                            : PanelMma<kBKContig, 2>::SMEM_BYTES;
     static_assert(pn <= 227 * 1024, "panel engine stages fit shared memory");
+#if MTD_TRSM_WIDE
+    constexpr int w1 = WideMma<kBNContig, 2>::SMEM_BYTES > WideMma<kBKContig, 2>::SMEM_BYTES
+                           ? WideMma<kBNContig, 2>::SMEM_BYTES
+                           : WideMma<kBKContig, 2>::SMEM_BYTES;
+    constexpr int w = w1 > TallMma<2>::SMEM_BYTES ? w1 : TallMma<2>::SMEM_BYTES;
+    static_assert(w <= 227 * 1024, "wide TRSM engine stages fit shared memory");
+#else
+    constexpr int w = 0;
+#endif
     constexpr int m12 = (g1 > g2 ? g1 : g2) > pn ? (g1 > g2 ? g1 : g2) : pn;
-    constexpr int m = m12 > g3 ? m12 : g3;
+    constexpr int m3 = m12 > g3 ? m12 : g3;
+    constexpr int m = m3 > w ? m3 : w;
     constexpr int d = diag > chol ? diag : chol;
     static_assert(t64::kSmemBytes <= (m > d ? m : d), "the FP64 TMA ring fits the engines' shared memory");
     return m > d ? m : d;
