@@ -335,22 +335,26 @@ int mtd_batch_solve_status(mtd_batch *b, int *info, double *latency_ms, double *
 /* CTA-to-task schedule of the batch's launches: the order in which the matrices' first
  * tasks enter the ready queues (MTD_BATCH_ORDER_*; the queues are FIFO, so it is the order
  * in which the 148 CTAs start the matrices), ORed with MTD_BATCH_SOLVE_LATE to queue the
- * solve tasks of mtd_batch_factor_solve behind all factor work instead of ahead of it. */
+ * solve tasks of mtd_batch_factor_solve behind all factor work instead of ahead of it, and
+ * with MTD_BATCH_SOLVE_PAIRS to give each solve task two matrices adjacent in that order
+ * (one per half of the CTA) instead of one (the whole CTA). */
 enum {
     MTD_BATCH_ORDER_INPUT = 0,
     MTD_BATCH_ORDER_LARGEST_FIRST = 1,
     MTD_BATCH_ORDER_SMALLEST_FIRST = 2,
     MTD_BATCH_SOLVE_LATE = 4,
-    MTD_BATCH_NUM_SCHEDULES = 6 /* candidates the schedule tuner times: 3 orders x 2 */
+    MTD_BATCH_SOLVE_PAIRS = 8,
+    MTD_BATCH_NUM_SCHEDULES = 12 /* candidates the schedule tuner times: 3 orders x 2 x 2 */
 };
 int mtd_batch_set_schedule(mtd_batch *b, int schedule);
 int mtd_batch_get_schedule(const mtd_batch *b);
 /* Schedule tuner: times mtd_batch_factor_solve (arguments as there) under each of the
- * MTD_BATCH_NUM_SCHEDULES schedules (candidate c = (c / 2) | (c % 2 ? MTD_BATCH_SOLVE_LATE :
- * 0)), `reps` timed launches each after one untimed, and keeps the fastest (set on the
- * batch and returned in *best).  FP64 batches factor in place, so before every launch the
- * tuner restores dF[m] from dSrc[m] (device copies, outside the timed region); dSrc may be
- * NULL for low-precision batches, whose conversion tasks rewrite dF.  ms (nullable, 6
+ * MTD_BATCH_NUM_SCHEDULES schedules (candidate c = (c % 6 / 2) | (c % 2 ?
+ * MTD_BATCH_SOLVE_LATE : 0) | (c >= 6 ? MTD_BATCH_SOLVE_PAIRS : 0)), `reps` timed launches
+ * each after one untimed, and keeps the fastest (set on the batch and returned in *best).
+ * FP64 batches factor in place, so before every launch the tuner restores dF[m] from
+ * dSrc[m] (device copies, outside the timed region); dSrc may be NULL for low-precision
+ * batches, whose conversion tasks rewrite dF.  ms (nullable, MTD_BATCH_NUM_SCHEDULES
  * entries): each candidate's best device time. */
 int mtd_batch_tune_schedule(mtd_batch *b, void *const *dF, const int64_t *ldf, const void *const *dSrc,
                             const int64_t *ldsrc, const double *const *dA, const int64_t *lda, const double *const *dB,

@@ -20,7 +20,7 @@ import os
 from . import _capi
 from ._capi import (  # noqa: F401  (re-exported constants)
     BATCH_NUM_SCHEDULES, BATCH_ORDER_INPUT, BATCH_ORDER_LARGEST_FIRST, BATCH_ORDER_SMALLEST_FIRST,
-    BATCH_SOLVE_LATE, GEN_SPD, GEN_UNIFORM_DIAG, KIND_CHOLESKY, KIND_CUSTOM, KIND_LU, OP_GEMM_NN, OP_GEMM_NT,
+    BATCH_SOLVE_LATE, BATCH_SOLVE_PAIRS, GEN_SPD, GEN_UNIFORM_DIAG, KIND_CHOLESKY, KIND_CUSTOM, KIND_LU, OP_GEMM_NN, OP_GEMM_NT,
     OP_GETRF, OP_NAMES, OP_POTRF, OP_SYRK_LN, OP_TRSM_LLNU, OP_TRSM_RLT, OP_TRSM_RUN,
     PREC_BF16, PREC_FP32, PREC_FP64, PREC_TF32, REFINE_GMRES_IR, REFINE_IR, REFINE_NONE, STATUS_NAMES, MtdError,
     lib, lib_path)
@@ -468,7 +468,8 @@ class Batch:
         _capi.check(self._lib.mtd_batch_tune_schedule(self._h, pf, lf, ps, ls, pa, la, pb, lb, px, lx, nr, method,
                                                       float(tol), int(max_iter), float(shift), int(reps),
                                                       ctypes.byref(best), ms, _stream_handle(stream)))
-        sched = [(c // 2) | (_capi.BATCH_SOLVE_LATE if c % 2 else 0) for c in range(_capi.BATCH_NUM_SCHEDULES)]
+        sched = [(c % 6 // 2) | (_capi.BATCH_SOLVE_LATE if c % 2 else 0) | (_capi.BATCH_SOLVE_PAIRS if c >= 6 else 0)
+                 for c in range(_capi.BATCH_NUM_SCHEDULES)]
         return best.value, {s: ms[c] for c, s in enumerate(sched)}
 
     def close(self):

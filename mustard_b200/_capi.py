@@ -35,7 +35,7 @@ class RunStats(ctypes.Structure):
 PREC_FP64, PREC_TF32, PREC_FP32, PREC_BF16 = 0, 1, 2, 3
 REFINE_NONE, REFINE_IR, REFINE_GMRES_IR = 0, 1, 2
 BATCH_ORDER_INPUT, BATCH_ORDER_LARGEST_FIRST, BATCH_ORDER_SMALLEST_FIRST = 0, 1, 2
-BATCH_SOLVE_LATE, BATCH_NUM_SCHEDULES = 4, 6
+BATCH_SOLVE_LATE, BATCH_SOLVE_PAIRS, BATCH_NUM_SCHEDULES = 4, 8, 12
 
 
 class SolveStats(ctypes.Structure):

@@ -17,7 +17,7 @@ normwise backward error 1e-13):
   one launch factor AND solve (+ refinement; + conversion from FP64 for fp32) as ONE
              persistent launch (mtd_batch_factor_solve), captured in a CUDA graph and
              replayed: device time, wall time-to-solution, latencies, backward errors; first
-             the schedule tuner times the six CTA-to-task schedules and keeps the fastest;
+             the schedule tuner times the twelve CTA-to-task schedules and keeps the fastest;
   defaults   the same factor launch with the library's default tiles (what tuning buys);
   torch      torch.linalg.cholesky + cholesky_solve per size group, for reference.
 One JSON line per measurement.
@@ -72,7 +72,7 @@ def one_launch(b, pname, prec, work, restore, rhs, a64, groups, base, flops_s, r
     tune_s = time.perf_counter() - t0
     names = {0: "input order", 1: "largest first", 2: "smallest first"}
     label = {s_: names[s_ & 3] + (", solves late" if s_ & mtd.BATCH_SOLVE_LATE else ", solves early")
-             for s_ in trial}
+             + (", two matrices per solve task" if s_ & mtd.BATCH_SOLVE_PAIRS else "") for s_ in trial}
     print(json.dumps(dict(base, prec=pname, step="schedule tuner", wall_s=tune_s, chosen=label[sched],
                           device_ms={label[k]: v for k, v in trial.items()})), flush=True)
     restore()

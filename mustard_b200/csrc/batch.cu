@@ -56,7 +56,7 @@ template <typename T>
 __global__ void __launch_bounds__(kBT, 2) batch_trsv_kernel(const SolveMat *mats, const T *ws, int target, Skip done) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (done()) return;
-    bsolve::trsv<T, kBT>(mats[blockIdx.x], ws, target, bsolve::Smem{smem_raw});
+    bsolve::trsv<T, kBT>(bsolve::Grp{int(threadIdx.x), 0}, mats[blockIdx.x], ws, target, bsolve::Smem{smem_raw});
 }
 
 // r = b - A_sym x and the matrix's backward error into berr[m]; the first call of a solve
@@ -65,8 +65,8 @@ __global__ void __launch_bounds__(kBT, 2) batch_residual_kernel(const SolveMat *
                                                                 int want_anorm, Skip done) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (done()) return;  // converged before the last step: x and berr[m] stand
-    const double be = bsolve::residual<kBT>(mats[blockIdx.x], anorm + blockIdx.x, want_anorm != 0,
-                                            bsolve::Smem{smem_raw});
+    const double be = bsolve::residual<kBT>(bsolve::Grp{int(threadIdx.x), 0}, mats[blockIdx.x], anorm + blockIdx.x,
+                                            want_anorm != 0, bsolve::Smem{smem_raw});
     if (threadIdx.x == 0) berr[blockIdx.x] = be;
 }
 
@@ -77,27 +77,28 @@ __global__ void __launch_bounds__(kBT) batch_scale_kernel(const SolveMat *mats, 
     if (done()) return;
     double *scale = colscale + int64_t(blockIdx.x) * kMaxRhs;
     if (to_low)
-        bsolve::scale_to_low<T, kBT>(mats[blockIdx.x], scale, red);
+        bsolve::scale_to_low<T, kBT>(bsolve::Grp{int(threadIdx.x), 0}, mats[blockIdx.x], scale, red);
     else
-        bsolve::add_scaled<T, kBT>(mats[blockIdx.x], scale);
+        bsolve::add_scaled<T, kBT>(bsolve::Grp{int(threadIdx.x), 0}, mats[blockIdx.x], scale);
 }
 
 // x += r (FP64 correction).
 __global__ void __launch_bounds__(kBT) batch_add_kernel(const SolveMat *mats, Skip done) {
-    if (!done()) bsolve::add_r<kBT>(mats[blockIdx.x]);
+    if (!done()) bsolve::add_r<kBT>(bsolve::Grp{int(threadIdx.x), 0}, mats[blockIdx.x]);
 }
 
 // X = B (columns), or X = 0.
 __global__ void __launch_bounds__(kBT) batch_copy_rhs_kernel(const SolveMat *mats, bool zero) {
-    bsolve::copy_rhs<kBT>(mats[blockIdx.x], zero);
+    bsolve::copy_rhs<kBT>(bsolve::Grp{int(threadIdx.x), 0}, mats[blockIdx.x], zero);
 }
 
 // F = lower triangle of A (+ shift on the diagonal), as float; grid (column strips, count).
 __global__ void __launch_bounds__(kBT) batch_convert_kernel(const SolveMat *mats, double shift) {
     const SolveMat &sm = mats[blockIdx.y];
     for (int c0 = blockIdx.x * kConvertCols; c0 < sm.n; c0 += gridDim.x * kConvertCols)
-        bsolve::convert<float, kBT>(sm.a, sm.lda, static_cast<float *>(const_cast<void *>(sm.f)), sm.ldf, sm.n, shift,
-                                    c0, min(sm.n, c0 + kConvertCols));
+        bsolve::convert<float, kBT>(bsolve::Grp{int(threadIdx.x), 0}, sm.a, sm.lda,
+                                    static_cast<float *>(const_cast<void *>(sm.f)), sm.ldf, sm.n, shift, c0,
+                                    min(sm.n, c0 + kConvertCols));
 }
 
 template <typename T>
@@ -235,37 +236,48 @@ std::vector<int> scheduled_roots(const mtd_batch *b) {
 // order.  Uploaded into the batch's fs tables.
 int build_fs(mtd_batch *b, bool convert) {
     release_fs(b);
-    const int count = b->count, n0 = b->n_dev;
+    const int count = b->count;
     std::vector<DevTask> t = b->h_tasks;
     std::vector<int> succ = b->h_succ, deps = b->h_deps_init, roots;
     const int solve_queue = (b->schedule & MTD_BATCH_SOLVE_LATE) ? kNumQueues - 1 : 0;
-    const int total = n0 + count * (convert ? 2 : 1);
-    t.resize(total);
-    deps.resize(total, 0);
-    for (int m = 0; m < count; ++m) {
+    const bool pairs = (b->schedule & MTD_BATCH_SOLVE_PAIRS) != 0;
+    const std::vector<int> order = schedule_order(b);
+    // solve tasks: one per matrix, or one per two matrices adjacent in the schedule order
+    std::vector<int> solve_of(count);
+    for (size_t q = 0; q < order.size(); q += pairs ? 2 : 1) {
         DevTask s{};
         s.op = kOpBatchSolve;
         s.queue = solve_queue;
         s.n_items = 1;
-        s.m = s.n = static_cast<int32_t>(b->n[m]);
-        s.mat = m;
-        s.succ_begin = 0;
-        s.succ_count = 0;
-        t[n0 + m] = s;
+        s.mat = order[q];
+        s.pad = (pairs && q + 1 < order.size()) ? order[q + 1] : -1;
+        s.m = s.n = static_cast<int32_t>(b->n[s.mat]);
+        const int idx = static_cast<int>(t.size());
+        t.push_back(s);
+        solve_of[s.mat] = idx;
+        if (s.pad >= 0) solve_of[s.pad] = idx;
+    }
+    deps.resize(t.size(), 0);
+    for (int m = 0; m < count; ++m) {
         for (int i = b->first_task[m]; i < b->first_task[m + 1]; ++i)
-            if (t[i].succ_count == 0) {  // a sink of matrix m: the solve follows it
+            if (t[i].succ_count == 0) {  // a sink of matrix m: its solve follows it
                 t[i].succ_begin = static_cast<int32_t>(succ.size());
                 t[i].succ_count = 1;
-                succ.push_back(n0 + m);
-                ++deps[n0 + m];
+                succ.push_back(solve_of[m]);
+                ++deps[solve_of[m]];
             }
     }
-    for (int m : schedule_order(b)) {
+    const int first_convert = static_cast<int>(t.size());
+    if (convert) {
+        t.resize(first_convert + count);
+        deps.resize(t.size(), 0);
+    }
+    for (int m : order) {
         if (!convert) {
             for (int r : b->roots_of[m]) roots.push_back(r);
             continue;
         }
-        const int c = n0 + count + m;
+        const int c = first_convert + m;
         DevTask d{};
         d.op = kOpBatchConvert;
         d.queue = 0;
@@ -301,7 +313,7 @@ int build_fs(mtd_batch *b, bool convert) {
         release_fs(b);
         return rc;
     }
-    b->fs_tasks = total;
+    b->fs_tasks = static_cast<int>(t.size());
     b->fs_roots = static_cast<int>(roots.size());
     for (int q = 0; q < kNumQueues; ++q) b->fs_qcap[q] = qcap[q];
     b->fs_convert = convert ? 1 : 0;
@@ -508,7 +520,8 @@ int mtd_batch_create(mtd_batch **out, int count, const int64_t *n, const int64_t
 int mtd_batch_num_tasks(const mtd_batch *b) { return b ? b->n_dev : -MTD_ERR_INVALID_ARG; }
 
 int mtd_batch_set_schedule(mtd_batch *b, int schedule) {
-    if (!b || schedule < 0 || (schedule & ~(3 | MTD_BATCH_SOLVE_LATE)) || (schedule & 3) > MTD_BATCH_ORDER_SMALLEST_FIRST)
+    if (!b || schedule < 0 || (schedule & ~(3 | MTD_BATCH_SOLVE_LATE | MTD_BATCH_SOLVE_PAIRS)) ||
+        (schedule & 3) > MTD_BATCH_ORDER_SMALLEST_FIRST)
         return MTD_ERR_INVALID_ARG;
     if (schedule == b->schedule) return MTD_OK;
     if ((b->pending || b->fs_pending) && b->last_stream && cudaStreamSynchronize(b->last_stream) != cudaSuccess)
@@ -744,7 +757,7 @@ int mtd_batch_tune_schedule(mtd_batch *b, void *const *dF, const int64_t *ldf, c
     int rc = MTD_OK, winner = b->schedule;
     double best_ms = 1e300;
     for (int c = 0; c < MTD_BATCH_NUM_SCHEDULES && !rc; ++c) {
-        const int sched = (c / 2) | (c % 2 ? MTD_BATCH_SOLVE_LATE : 0);
+        const int sched = (c % 6 / 2) | (c % 2 ? MTD_BATCH_SOLVE_LATE : 0) | (c >= 6 ? MTD_BATCH_SOLVE_PAIRS : 0);
         rc = mtd_batch_set_schedule(b, sched);
         double cand = 1e300;
         for (int rep = 0; rep <= reps && !rc; ++rep) {  // rep 0 is untimed

@@ -62,6 +62,18 @@ struct Smem {
 template <typename T>
 __device__ __forceinline__ T ldcg(const T *p) { return __ldcg(p); }
 
+// The threads that run one matrix's steps: the whole CTA (bar = 0: __syncthreads), or a
+// warp-aligned group of NT threads that meets at named barrier `bar` (two matrices per CTA).
+struct Grp {
+    int tid;  // thread index within the group
+    int bar;
+};
+template <int NT>
+__device__ __forceinline__ void gsync(const Grp &g) {
+    if (g.bar == 0) gsync<NT>(g);
+    else asm volatile("bar.sync %0, %1;" ::"r"(g.bar), "r"(NT) : "memory");
+}
+
 __device__ __forceinline__ void blk_mma(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
     mma_16x8x8(d, a, b);
 }
@@ -90,14 +102,14 @@ __device__ __forceinline__ int tile_col(int n0, int v) { return n0 + 2 * (thread
 // on the n x nrhs block Y (the target of SolveMat), in T.  Block row j subtracts L(j, k) Y(k)
 // for the rows k solved before it and applies the inverse of its diagonal block.
 template <typename T, int NT>
-__device__ void trsv(const SolveMat &sm, const T *ws, int target, Smem sh) {
+__device__ void trsv(const Grp &g, const SolveMat &sm, const T *ws, int target, Smem sh) {
     constexpr int kL = kSB * kSB / NT;       // elements of a 64 x 64 block per thread
     constexpr int kY = kMaxRhs * kSB / NT;   // elements of a vector block per thread
     static_assert(kSB * kSB % NT == 0 && kMaxRhs * kSB % NT == 0, "whole elements per thread");
     T *Lb = sh.blocks<T>();
     T *Yb = sh.vecs<T>();
     T *Acc = sh.acc<T>();
-    const int n = sm.n, nrhs = sm.nrhs, tid = threadIdx.x;
+    const int n = sm.n, nrhs = sm.nrhs, tid = g.tid;
     const T *L = static_cast<const T *>(sm.f);
     const int64_t ldl = sm.ldf;
     const T *W = ws + sm.ws_off;
@@ -167,7 +179,7 @@ __device__ void trsv(const SolveMat &sm, const T *ws, int target, Smem sh) {
                 Acc[c * kLD + r] = (r < rj && c < nrhs) ? Y[(int64_t(j) * kSB + r) + c * ldy] : T(0);
             }
             stash(0);
-            __syncthreads();
+            gsync<NT>(g);
             for (int t = 0; t <= s; ++t) {
                 if (t + 1 <= s) fetch(t + 1);  // in flight during the product below
                 const T *Lc = Lb + (t & 1) * kSB * kLD;
@@ -187,7 +199,7 @@ __device__ void trsv(const SolveMat &sm, const T *ws, int target, Smem sh) {
                     }
                 }
                 if (t + 1 <= s) stash(t + 1);  // the other buffer: last read in step t - 1
-                __syncthreads();  // Y(j) stored before later rows read it; the buffers change hands
+                gsync<NT>(g);  // Y(j) stored before later rows read it; the buffers change hands
             }
         }
     }
@@ -212,8 +224,9 @@ __device__ __forceinline__ int64_t sym_offset(int I, int J, int r, int c, int64_
 
 // Column maxima of |v| (nrhs columns, leading dimension ld) into red[which][c][warp].
 template <int NT>
-__device__ __forceinline__ void col_absmax(const double *v, int64_t ld, int n, int nrhs, double *red, int which) {
-    const int tid = threadIdx.x;
+__device__ __forceinline__ void col_absmax(const Grp &g, const double *v, int64_t ld, int n, int nrhs, double *red,
+                                           int which) {
+    const int tid = g.tid;
     for (int c = 0; c < nrhs; ++c) {
         double m = 0.0;
         for (int i = tid; i < n; i += NT) m = fmax(m, fabs(v[i + int64_t(c) * ld]));
@@ -228,13 +241,13 @@ __device__ __forceinline__ void col_absmax(const double *v, int64_t ld, int n, i
 // pass sums |A| along each row and stores ||A_sym||_inf in *anorm (thread 0); otherwise
 // *anorm is read.
 template <int NT>
-__device__ double residual(const SolveMat &sm, double *anorm, bool want_anorm, Smem sh) {
+__device__ double residual(const Grp &g, const SolveMat &sm, double *anorm, bool want_anorm, Smem sh) {
     constexpr int kA = kSB * kSB / NT;
     constexpr int kX = kMaxRhs * kSB / NT;
     double *Ab = sh.blocks<double>();
     double *Xb = sh.vecs<double>();
     double *red = sh.red();
-    const int n = sm.n, nrhs = sm.nrhs, tid = threadIdx.x;
+    const int n = sm.n, nrhs = sm.nrhs, tid = g.tid;
     const double *A = sm.a;
     const int64_t lda = sm.lda;
     const int nb = (n + kSB - 1) / kSB;
@@ -277,7 +290,7 @@ __device__ double residual(const SolveMat &sm, double *anorm, bool want_anorm, S
         double rowsum = 0.0;
         fetch(0);
         stash(0);
-        __syncthreads();
+        gsync<NT>(g);
         for (int J = 0; J < nb; ++J) {
             if (J + 1 < nb) fetch(J + 1);
             const double *Ac = Ab + (J & 1) * kSB * kLD;
@@ -287,7 +300,7 @@ __device__ double residual(const SolveMat &sm, double *anorm, bool want_anorm, S
                 for (int k = 0; k < kSB; ++k) rowsum += fabs(Ac[tid * kLD + k]);
             }
             if (J + 1 < nb) stash(J + 1);
-            __syncthreads();
+            gsync<NT>(g);
         }
         if (warp < tiles) {
 #pragma unroll
@@ -302,18 +315,18 @@ __device__ double residual(const SolveMat &sm, double *anorm, bool want_anorm, S
     if (want_anorm) {
         for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
         if ((tid & 31) == 0) red[tid >> 5] = amax;
-        __syncthreads();
+        gsync<NT>(g);
         if (tid == 0) {
             double m = 0.0;
             for (int w = 0; w < NT / 32; ++w) m = fmax(m, red[w]);
             *anorm = m;
         }
     }
-    __syncthreads();  // r written; the reduction area is free again; *anorm published
-    col_absmax<NT>(sm.r, n, n, nrhs, red, 0);
-    col_absmax<NT>(sm.x, sm.ldx, n, nrhs, red, 1);
-    col_absmax<NT>(sm.b, sm.ldb, n, nrhs, red, 2);
-    __syncthreads();
+    gsync<NT>(g);  // r written; the reduction area is free again; *anorm published
+    col_absmax<NT>(g, sm.r, n, n, nrhs, red, 0);
+    col_absmax<NT>(g, sm.x, sm.ldx, n, nrhs, red, 1);
+    col_absmax<NT>(g, sm.b, sm.ldb, n, nrhs, red, 2);
+    gsync<NT>(g);
     const double an = *anorm;
     double worst = 0.0;
     for (int c = 0; c < nrhs; ++c) {
@@ -326,68 +339,69 @@ __device__ double residual(const SolveMat &sm, double *anorm, bool want_anorm, S
         const double den = an * mx + mb;
         worst = fmax(worst, den > 0 ? mr / den : mr);
     }
-    __syncthreads();  // every thread has read the reductions
+    gsync<NT>(g);  // every thread has read the reductions
     return worst;
 }
 
 // d = r / max|r| per column, rounded to T; the column scales go to scale[c].
 template <typename T, int NT>
-__device__ void scale_to_low(const SolveMat &sm, double *scale, double *red) {
-    const int n = sm.n, tid = threadIdx.x;
+__device__ void scale_to_low(const Grp &g, const SolveMat &sm, double *scale, double *red) {
+    const int n = sm.n, tid = g.tid;
     T *d = static_cast<T *>(sm.d);
     for (int c = 0; c < sm.nrhs; ++c) {
         double m = 0.0;
         for (int i = tid; i < n; i += NT) m = fmax(m, fabs(sm.r[i + int64_t(c) * n]));
         for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-        __syncthreads();  // the previous column's reduction has been read
+        gsync<NT>(g);  // the previous column's reduction has been read
         if ((tid & 31) == 0) red[tid >> 5] = m;
-        __syncthreads();
+        gsync<NT>(g);
         double s = 0.0;
         for (int w = 0; w < NT / 32; ++w) s = fmax(s, red[w]);
         if (s == 0.0) s = 1.0;
         if (tid == 0) scale[c] = s;
         for (int i = tid; i < n; i += NT) d[i + int64_t(c) * n] = static_cast<T>(sm.r[i + int64_t(c) * n] / s);
     }
-    __syncthreads();
+    gsync<NT>(g);
 }
 
 // x += scale_c * d (the scaled low-precision correction).
 template <typename T, int NT>
-__device__ void add_scaled(const SolveMat &sm, const double *scale) {
+__device__ void add_scaled(const Grp &g, const SolveMat &sm, const double *scale) {
     const T *d = static_cast<const T *>(sm.d);
     for (int c = 0; c < sm.nrhs; ++c) {
         const double s = scale[c];
-        for (int i = threadIdx.x; i < sm.n; i += NT)
+        for (int i = g.tid; i < sm.n; i += NT)
             sm.x[i + int64_t(c) * sm.ldx] += s * static_cast<double>(d[i + int64_t(c) * sm.n]);
     }
-    __syncthreads();
+    gsync<NT>(g);
 }
 
 // x += r (FP64 correction).
 template <int NT>
-__device__ void add_r(const SolveMat &sm) {
-    for (int64_t e = threadIdx.x; e < int64_t(sm.n) * sm.nrhs; e += NT) {
+__device__ void add_r(const Grp &g, const SolveMat &sm) {
+    for (int64_t e = g.tid; e < int64_t(sm.n) * sm.nrhs; e += NT) {
         const int64_t i = e % sm.n, c = e / sm.n;
         sm.x[i + c * sm.ldx] += sm.r[i + c * sm.n];
     }
-    __syncthreads();
+    gsync<NT>(g);
 }
 
 // x = b, or x = 0.
 template <int NT>
-__device__ void copy_rhs(const SolveMat &sm, bool zero) {
-    for (int64_t e = threadIdx.x; e < int64_t(sm.n) * sm.nrhs; e += NT) {
+__device__ void copy_rhs(const Grp &g, const SolveMat &sm, bool zero) {
+    for (int64_t e = g.tid; e < int64_t(sm.n) * sm.nrhs; e += NT) {
         const int64_t i = e % sm.n, c = e / sm.n;
         sm.x[i + c * sm.ldx] = zero ? 0.0 : sm.b[i + c * sm.ldb];
     }
-    __syncthreads();
+    gsync<NT>(g);
 }
 
 // Columns [c0, c1) of F = lower triangle of A (+ shift on the diagonal), rounded to T.
 template <typename T, int NT>
-__device__ void convert(const double *A, int64_t lda, T *F, int64_t ldf, int n, double shift, int c0, int c1) {
+__device__ void convert(const Grp &g, const double *A, int64_t lda, T *F, int64_t ldf, int n, double shift, int c0,
+                        int c1) {
     for (int j = c0; j < c1; ++j)
-        for (int i = j + threadIdx.x; i < n; i += NT) {
+        for (int i = j + g.tid; i < n; i += NT) {
             double v = A[i + int64_t(j) * lda];
             if (i == j) v += shift;
             F[i + int64_t(j) * ldf] = static_cast<T>(v);
@@ -401,32 +415,32 @@ __device__ void convert(const double *A, int64_t lda, T *F, int64_t ldf, int n, 
 // per column, until the backward error is <= tol after at least one step, or max_iter steps.
 // *berr: the last backward error (-1 without A); *iters: the solves applied.
 template <typename T, int NT>
-__device__ void solve_refine(const SolveMat &sm, const T *ws, int method, double tol, int max_iter, Smem sh,
-                             double *berr, int *iters) {
+__device__ void solve_refine(const Grp &g, const SolveMat &sm, const T *ws, int method, double tol, int max_iter,
+                             Smem sh, double *berr, int *iters) {
     constexpr bool low = sizeof(T) != sizeof(double);
     double *scale = sh.scale<NT>();
     int steps = 0;
     double be = -1.0;
     if (!low) {
-        copy_rhs<NT>(sm, false);
-        trsv<T, NT>(sm, ws, kOnX, sh);
+        copy_rhs<NT>(g, sm, false);
+        trsv<T, NT>(g, sm, ws, kOnX, sh);
         steps = 1;
     } else {
-        copy_rhs<NT>(sm, true);
+        copy_rhs<NT>(g, sm, true);
     }
     if (sm.a) {
         for (int it = 0;; ++it) {
-            be = residual<NT>(sm, sh.norm<NT>(), it == 0, sh);
+            be = residual<NT>(g, sm, sh.norm<NT>(), it == 0, sh);
             if (method == MTD_REFINE_NONE) break;
             if ((it > 0 || !low) && be <= tol) break;
             if (it >= max_iter) break;
             if constexpr (low) {
-                scale_to_low<T, NT>(sm, scale, sh.red());
-                trsv<T, NT>(sm, ws, kOnD, sh);
-                add_scaled<T, NT>(sm, scale);
+                scale_to_low<T, NT>(g, sm, scale, sh.red());
+                trsv<T, NT>(g, sm, ws, kOnD, sh);
+                add_scaled<T, NT>(g, sm, scale);
             } else {
-                trsv<T, NT>(sm, ws, kOnR, sh);
-                add_r<NT>(sm);
+                trsv<T, NT>(g, sm, ws, kOnR, sh);
+                add_r<NT>(g, sm);
             }
             steps = it + 1 + (low ? 0 : 1);  // + the first FP64 solve
         }

@@ -399,8 +399,14 @@ struct BlockMmaT {
     // pipe at a CTA barrier every slice.  All threads must call.  Returns false if a wait ran
     // past ~1 s (in a correct run every copy lands and every warp arrives): the caller
     // reports a timeout.  Shared memory is free again on return.
+#if MTD_EARLY_CLAIM2
+    template <typename OnLast>
+    __device__ __forceinline__ bool run_sp(void *smem_raw, const T *A, int64_t lda, const T *B, int64_t ldb, int M,
+                                           int N, int K, OnLast on_last) {
+#else
     __device__ __forceinline__ bool run_sp(void *smem_raw, const T *A, int64_t lda, const T *B, int64_t ldb, int M,
                                            int N, int K) {
+#endif
         __shared__ alignas(8) unsigned long long full[STAGES], empty[STAGES];
         if (K <= 0) return true;
         T *As = static_cast<T *>(smem_raw);
@@ -443,6 +449,9 @@ struct BlockMmaT {
         for (int kt = 0; kt < ktiles; ++kt) {
             const int st = kt % STAGES;
             wait(&full[st], (kt / STAGES) & 1);
+#if MTD_EARLY_CLAIM2
+            if (kt == ktiles - 1 && threadIdx.x == 0) on_last();  // thread 0, before the last slice
+#endif
             compute_stage(As + st * A_STAGE, Bs + st * B_STAGE);
             __syncwarp();
             if ((threadIdx.x & 31) == 0)

@@ -101,6 +101,27 @@ __device__ __forceinline__ int claim_item(const RunArgs &p, int *task, int *item
     return kCmdNone;
 }
 
+#if MTD_EARLY_CLAIM2
+// The item an FP64 update claimed ahead (early_claim), for the persistent loop's next round.
+struct EarlyClaim {
+    int valid, task, item;
+};
+static __shared__ EarlyClaim g_early;
+
+// Thread 0 of an FP64 update item, before its last k-slice: one attempt to claim the CTA's
+// next item (kept in g_early).  Not inlined, so the claim's registers are not allocated in the
+// update's k-loop.
+static __device__ __noinline__ void early_claim(const RunArgs &p) {
+    if (g_early.valid) return;
+    int tk = 0, it = 0;
+    if (claim_item(p, &tk, &it, global_ns()) == kCmdWork) {
+        g_early.task = tk;
+        g_early.item = it;
+        g_early.valid = 1;
+    }
+}
+#endif
+
 // One thread of a CTA: claim one work item, waiting (bounded) while none is ready.
 __device__ __forceinline__ int pop_item(const RunArgs &p, int *task, int *item) {
     const unsigned long long t0 = global_ns();
@@ -238,23 +259,46 @@ __device__ __forceinline__ int op_update_tc(const RunArgs &p, const MatCtx &m, c
     return 0;
 }
 
-// The solve task of one matrix of a batched factor-and-solve launch (the sink of its DAG):
-// the matrix's whole solve with refinement on this CTA (batch_ops.cuh).  A matrix whose
-// factorisation met a bad pivot is not solved: its backward error and step count keep the
-// values the launch reset them to.
-template <typename T>
-__device__ __noinline__ int op_batch_solve(const RunArgs &p, const DevTask &t, void *smem) {
-    static_assert(bsolve::smem_bytes<kThreads>() <= size_t(kOpSmemBytes()), "solve scratch fits the kernel's");
-    if (ld_volatile(p.mat_info + t.mat) != kBatchInfoOk) return 0;
+// The solve task of a batched factor-and-solve launch (after its matrices' factorisations):
+// the whole solve with refinement of matrix t.mat on this CTA (batch_ops.cuh) or, when the
+// task pairs two matrices (t.pad >= 0), of t.mat on threads 0-255 and of t.pad on threads
+// 256-511, each half with its own named barrier and half of the shared memory.  A matrix
+// whose factorisation met a bad pivot is not solved: its backward error and step count keep
+// the values the launch reset them to.  Each group stamps its matrix's finish time.
+template <typename T, int NT>
+__device__ __forceinline__ void batch_solve_one(const RunArgs &p, int mat, bsolve::Grp g, unsigned char *smem) {
+    if (ld_volatile(p.mat_info + mat) != kBatchInfoOk) return;
     double berr = -1.0;
     int iters = 0;
-    bsolve::solve_refine<T, kThreads>(p.solve[t.mat], static_cast<const T *>(p.ws_lower), p.solve_method,
-                                      p.solve_tol, p.solve_max_iter, bsolve::Smem{static_cast<unsigned char *>(smem)},
-                                      &berr, &iters);
-    if (threadIdx.x == 0) {
-        p.solve_berr[t.mat] = berr;
-        p.solve_iters[t.mat] = iters;
+    bsolve::solve_refine<T, NT>(g, p.solve[mat], static_cast<const T *>(p.ws_lower), p.solve_method, p.solve_tol,
+                                p.solve_max_iter, bsolve::Smem{smem}, &berr, &iters);
+    if (g.tid == 0) {
+        p.solve_berr[mat] = berr;
+        p.solve_iters[mat] = iters;
+        if (p.mat_done_ns) p.mat_done_ns[mat] = global_ns();
     }
+}
+// The two forms in their own functions, each with its own register allocation (the
+// half-CTA form stages twice the elements per thread).
+template <typename T>
+__device__ __noinline__ void batch_solve_whole(const RunArgs &p, const DevTask &t, void *smem) {
+    batch_solve_one<T, kThreads>(p, t.mat, bsolve::Grp{static_cast<int>(threadIdx.x), 0},
+                                 static_cast<unsigned char *>(smem));
+}
+template <typename T>
+__device__ __noinline__ void batch_solve_halves(const RunArgs &p, const DevTask &t, void *smem) {
+    constexpr int kHalf = kThreads / 2;
+    const int half = static_cast<int>(threadIdx.x) / kHalf;
+    batch_solve_one<T, kHalf>(p, half ? t.pad : t.mat, bsolve::Grp{static_cast<int>(threadIdx.x) % kHalf, 3 + half},
+                              static_cast<unsigned char *>(smem) + half * bsolve::smem_bytes<kHalf>());
+}
+template <typename T>
+__device__ int op_batch_solve(const RunArgs &p, const DevTask &t, void *smem) {
+    static_assert(bsolve::smem_bytes<kThreads>() <= size_t(kOpSmemBytes()) &&
+                      2 * bsolve::smem_bytes<kThreads / 2>() <= size_t(kOpSmemBytes()),
+                  "solve scratch fits the kernel's");
+    if (t.pad >= 0) batch_solve_halves<T>(p, t, smem);
+    else batch_solve_whole<T>(p, t, smem);
     return 0;
 }
 
@@ -265,8 +309,8 @@ __device__ __noinline__ int op_batch_convert(const RunArgs &p, const DevTask &t,
     const SolveMat &sm = p.solve[t.mat];
     const BatchMat bm = p.mats[t.mat];
     const int c0 = item * kConvertCols;
-    bsolve::convert<T, kThreads>(sm.a, sm.lda, static_cast<T *>(bm.a), bm.lda, sm.n, p.solve_shift, c0,
-                                 min(sm.n, c0 + kConvertCols));
+    bsolve::convert<T, kThreads>(bsolve::Grp{static_cast<int>(threadIdx.x), 0}, sm.a, sm.lda, static_cast<T *>(bm.a),
+                                 bm.lda, sm.n, p.solve_shift, c0, min(sm.n, c0 + kConvertCols));
     return 0;
 }
 
@@ -617,10 +661,24 @@ __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const __grid_co
             prev_ok = s_st == 0;
         }
 #else
+#if MTD_EARLY_CLAIM2
+        if (threadIdx.x == 0) g_early.valid = 0;
+#endif
         while (true) {
             if (threadIdx.x == 0) {
                 int tk = 0, it = 0;
+#if MTD_EARLY_CLAIM2
+                if (g_early.valid) {  // claimed during the previous item
+                    s_cmd = kCmdWork;
+                    tk = g_early.task;
+                    it = g_early.item;
+                    g_early.valid = 0;
+                } else {
+                    s_cmd = pop_item(p, &tk, &it);
+                }
+#else
                 s_cmd = pop_item(p, &tk, &it);
+#endif
                 s_task = tk;
                 s_item = it;
             }

@@ -575,10 +575,28 @@ __device__ __forceinline__ bool eng_run(const RunArgs &p, E &e, void *smem, cons
     }
     return true;
 }
+// 1: in the FP64 persistent loop, thread 0 of an update item makes one attempt to claim the
+// CTA's next item before the item's last k-slice (scheduler.cuh, early_claim).
+#ifndef MTD_EARLY_CLAIM2
+#define MTD_EARLY_CLAIM2 0
+#endif
+#if MTD_EARLY_CLAIM2
+static __device__ __noinline__ void early_claim(const RunArgs &p);
+#endif
+
 // The update items' k-loop (MTD_SPLIT_PHASE) and the TRSM strips' (MTD_SPLIT_PHASE_TRSM).
 template <typename E, typename T>
 __device__ __forceinline__ bool gemm_run(const RunArgs &p, E &e, void *smem, const T *A, int64_t lda, const T *B,
                                          int64_t ldb, int M, int N, int K) {
+#if MTD_EARLY_CLAIM2
+    if constexpr (sizeof(T) == 8) {
+        if (!e.run_sp(smem, A, lda, B, ldb, M, N, K, [&]() { early_claim(p); })) {
+            if (threadIdx.x == 0) report_error(p.ctl, MTD_ERR_TIMEOUT, 0);
+            return false;
+        }
+        return true;
+    }
+#endif
     return eng_run<MTD_SPLIT_PHASE != 0>(p, e, smem, A, lda, B, ldb, M, N, K);
 }
 template <typename E, typename T>

@@ -63,6 +63,7 @@ def main():
     ap.add_argument("--tile", type=int, default=768)
     ap.add_argument("--runs", type=int, default=2)
     ap.add_argument("--prec", choices=["fp64", "tf32", "bf16", "fp32"], default="fp64")
+    ap.add_argument("--nest", type=int, default=None, help="nested sub-tile edge of the diagonal factorisations")
     ap.add_argument("--trace", action="store_true", help="per-operation item-time breakdown")
     ap.add_argument("--trace-out", default=None,
                     help="also write the records, task spans and critical path to this JSON file")
@@ -94,6 +95,8 @@ def main():
     if args.prec != "fp64":
         g.set_precision({"tf32": mtd.PREC_TF32, "bf16": mtd.PREC_BF16, "fp32": mtd.PREC_FP32}[args.prec])
         a = a.t().contiguous().float().t()
+    if args.nest is not None:
+        g.set_nest(args.nest)
     if args.trace_out:
         args.trace = True
     if args.trace:

@@ -128,7 +128,7 @@ def test_every_schedule_gives_the_same_bits(mtd):
     mats, bs = _problem(sizes, 1400)
     b = mtd.Batch(sizes, prec=mtd.PREC_FP32)
     outs = []
-    for sched in range(8):
+    for sched in range(16):
         if (sched & 3) == 3:
             continue
         b.schedule = sched
@@ -198,7 +198,7 @@ def test_schedule_tuner_keeps_a_valid_fastest_schedule(mtd):
     a64, work, bd, xd = _fresh(mats, bs)
     src = [to_dev(a) for a in mats]
     best, ms = b.tune_schedule(work, bd, xd, a64=a64, source=src, method=mtd.REFINE_NONE, reps=1)
-    assert sorted(ms) == [0, 1, 2, 4, 5, 6] and all(v > 0 for v in ms.values())
+    assert sorted(ms) == [0, 1, 2, 4, 5, 6, 8, 9, 10, 12, 13, 14] and all(v > 0 for v in ms.values())
     assert best in ms and ms[best] == min(ms.values()) and b.schedule == best
     # the tuned batch still solves correctly from a restored input
     for w, s_ in zip(work, src):
