@@ -112,6 +112,11 @@ int mtd_graph_create(mtd_graph **out, int kind, int64_t n, int64_t tile);
  * index (>= 0) or a negative mtd_status. */
 int mtd_graph_add_task(mtd_graph *g, int op, int wi, int wj, const int *reads, int nreads);
 
+/* Tile rows (and columns) at the element edges edges[0] = 0 < edges[1] < ... <
+ * edges[count - 1] = n instead of uniform `tile`-wide ones, e.g. a narrower first or last
+ * tile (the reference's tiles are uniform).  Only before any task is recorded. */
+int mtd_graph_set_tile_edges(mtd_graph *g, const int64_t *edges, int count);
+
 /* Emit the reference's whole task list for the graph's kind, in its loop order
  * (cholesky_mustard.cu:224-395 or lu_mustard.cu:345-533).  MTD_ERR_INVALID_ARG when the
  * list would exceed 2^25 tasks (the count is cubic in the tile count). */

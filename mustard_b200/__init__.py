@@ -91,6 +91,12 @@ class TaskGraph:
         _capi.check(self._lib.mtd_graph_set_trace(self._h, 1 if enable else 0))
         return self
 
+    def set_tile_edges(self, edges):
+        """Tiles at the given element edges (0 < ... < n) instead of uniform ones."""
+        arr = (ctypes.c_int64 * len(edges))(*edges)
+        _capi.check(self._lib.mtd_graph_set_tile_edges(self._h, arr, len(edges)))
+        return self
+
     def set_nest(self, nest):
         """Sub-tile edge of nested diagonal factorisations (multiple of 64; 0 = off)."""
         _capi.check(self._lib.mtd_graph_set_nest(self._h, int(nest)))

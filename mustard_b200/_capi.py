@@ -105,6 +105,7 @@ SIGNATURES = {
     "mtd_graph_set_trace": (_i, [_vp, _i]),
     "mtd_graph_set_timeout": (_i, [_vp, _d]),
     "mtd_graph_set_nest": (_i, [_vp, _i]),
+    "mtd_graph_set_tile_edges": (_i, [_vp, _pi64, _i]),
     "mtd_run": (_i, [_vp, _vp, _i64, _vp, ctypes.POINTER(_i)]),
     "mtd_run_graph": (_i, [_vp, _vp, _i64, _vp, ctypes.POINTER(_i)]),
     "mtd_graph_status": (_i, [_vp, ctypes.POINTER(_i)]),

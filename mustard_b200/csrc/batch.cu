@@ -70,6 +70,14 @@ __global__ void __launch_bounds__(kBT, 2) batch_residual_kernel(const SolveMat *
     if (threadIdx.x == 0) berr[blockIdx.x] = be;
 }
 
+// r = b and its backward error, for x = 0 (the first step of a low-precision solve).
+__global__ void __launch_bounds__(kBT) batch_residual_zero_kernel(const SolveMat *mats, double *berr) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const double be = bsolve::residual_of_zero<kBT>(bsolve::Grp{int(threadIdx.x), 0}, mats[blockIdx.x],
+                                                    bsolve::Smem{smem_raw});
+    if (threadIdx.x == 0) berr[blockIdx.x] = be;
+}
+
 // d = r / max|r| per column (rounded to T), or x += max|r| * d.
 template <typename T>
 __global__ void __launch_bounds__(kBT) batch_scale_kernel(const SolveMat *mats, double *colscale, bool to_low, Skip done) {
@@ -608,6 +616,8 @@ int mtd_batch_solve(mtd_batch *b, const double *const *dA, const int64_t *lda, v
         cudaFuncSetAttribute(batch_trsv_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem32)) !=
             cudaSuccess ||
         cudaFuncSetAttribute(batch_residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(batch_residual_zero_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) !=
             cudaSuccess)
         return MTD_ERR_CUDA;
     const double *ws64 = reinterpret_cast<const double *>(b->d_ws);
@@ -623,8 +633,12 @@ int mtd_batch_solve(mtd_batch *b, const double *const *dA, const int64_t *lda, v
     }
     if (dA) {
         for (int it = 0;; ++it) {
-            batch_residual_kernel<<<count, kBT, smem, s>>>(b->d_solve, b->d_anorm, b->d_berr, it == 0,
-                                                           Skip{(it > 1 || (it > 0 && !low)) ? b->d_berr : nullptr, tol});
+            if (low && it == 0)  // x = 0: the residual is b itself
+                batch_residual_zero_kernel<<<count, kBT, smem, s>>>(b->d_solve, b->d_berr);
+            else
+                batch_residual_kernel<<<count, kBT, smem, s>>>(b->d_solve, b->d_anorm, b->d_berr, it == (low ? 1 : 0),
+                                                               Skip{(it > 1 || (it > 0 && !low)) ? b->d_berr : nullptr,
+                                                                    tol});
             if (cudaMemcpyAsync(b->h_berr, b->d_berr, count * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
                 cudaStreamSynchronize(s) != cudaSuccess)
                 return MTD_ERR_CUDA;

@@ -343,6 +343,28 @@ __device__ double residual(const Grp &g, const SolveMat &sm, double *anorm, bool
     return worst;
 }
 
+// r = b, the residual of x = 0, and its backward error (1 for a column with b != 0, else 0:
+// with x = 0 the error measure is ||b|| / ||b||), without reading A.
+template <int NT>
+__device__ double residual_of_zero(const Grp &g, const SolveMat &sm, Smem sh) {
+    double *red = sh.red();
+    const int n = sm.n, nrhs = sm.nrhs;
+    for (int64_t e = g.tid; e < int64_t(n) * nrhs; e += NT) {
+        const int64_t i = e % n, c = e / n;
+        sm.r[i + c * n] = sm.b[i + c * sm.ldb];
+    }
+    col_absmax<NT>(g, sm.b, sm.ldb, n, nrhs, red, 2);
+    gsync<NT>(g);
+    double worst = 0.0;
+    for (int c = 0; c < nrhs; ++c) {
+        double mb = 0.0;
+        for (int w = 0; w < NT / 32; ++w) mb = fmax(mb, red[(2 * kMaxRhs + c) * (NT / 32) + w]);
+        worst = fmax(worst, mb > 0.0 ? 1.0 : 0.0);
+    }
+    gsync<NT>(g);  // every thread has read the reductions
+    return worst;
+}
+
 // d = r / max|r| per column, rounded to T; the column scales go to scale[c].
 template <typename T, int NT>
 __device__ void scale_to_low(const Grp &g, const SolveMat &sm, double *scale, double *red) {
@@ -430,7 +452,9 @@ __device__ void solve_refine(const Grp &g, const SolveMat &sm, const T *ws, int 
     }
     if (sm.a) {
         for (int it = 0;; ++it) {
-            be = residual<NT>(g, sm, sh.norm<NT>(), it == 0, sh);
+            // a low-precision solve starts from x = 0, whose residual is b itself
+            if (low && it == 0) be = residual_of_zero<NT>(g, sm, sh);
+            else be = residual<NT>(g, sm, sh.norm<NT>(), it == (low ? 1 : 0), sh);
             if (method == MTD_REFINE_NONE) break;
             if ((it > 0 || !low) && be <= tol) break;
             if (it >= max_iter) break;

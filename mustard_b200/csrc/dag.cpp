@@ -14,7 +14,31 @@ int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 Dag::Dag(int kind, int64_t n, int64_t tile)
     : kind_(kind), n_(n), tile_(tile), tiles_(static_cast<int>(ceil_div(n, tile))) {}
 
-int64_t Dag::extent(int t) const { return std::min<int64_t>(tile_, n_ - int64_t(t) * tile_); }
+int64_t Dag::origin(int t) const { return edges_.empty() ? int64_t(t) * tile_ : edges_[t]; }
+
+int64_t Dag::extent(int t) const {
+    return edges_.empty() ? std::min<int64_t>(tile_, n_ - int64_t(t) * tile_) : edges_[t + 1] - edges_[t];
+}
+
+int64_t Dag::unit() const {
+    if (edges_.empty()) return tile_;
+    int64_t u = int64_t(1) << 30;
+    for (int64_t e : edges_)
+        if (e > 0) u = std::min<int64_t>(u, e & -e);  // lowest set bit
+    return u;
+}
+
+int Dag::set_edges(const std::vector<int64_t> &edges) {
+    if (!tasks_.empty()) return MTD_ERR_STATE;
+    if (edges.size() < 2 || edges.front() != 0 || edges.back() != n_) return MTD_ERR_INVALID_ARG;
+    for (size_t i = 1; i < edges.size(); ++i)
+        if (edges[i] <= edges[i - 1]) return MTD_ERR_INVALID_ARG;
+    edges_ = edges;
+    tiles_ = static_cast<int>(edges.size()) - 1;
+    tile_ = 0;
+    for (size_t i = 1; i < edges.size(); ++i) tile_ = std::max(tile_, edges[i] - edges[i - 1]);
+    return MTD_OK;
+}
 
 bool Dag::valid_tile(const TileId &t) const {
     return t.first >= 0 && t.second >= 0 && t.first < tiles_ && t.second < tiles_;
@@ -286,13 +310,12 @@ int Dag::lower(int nest, Lowered &out) const {
     std::vector<std::vector<int>> entry(nt);
     std::vector<int> exit_of(nt, -1);
     out.host_items.assign(nt, 0);
-    const int64_t B = tile_;
     for (int t = 0; t < nt; ++t) {
         const HostTask &h = tasks_[t];
         const int q = queue_of(t);
-        const int64_t wr = h.write.first * B, wc = h.write.second * B;
+        const int64_t wr = origin(h.write.first), wc = origin(h.write.second);
         const int64_t em = extent(h.write.first), en = extent(h.write.second);
-        const int64_t ar = h.a.first * B, ac = h.a.second * B, br = h.b.first * B, bc = h.b.second * B;
+        const int64_t ar = origin(h.a.first), ac = origin(h.a.second), br = origin(h.b.first), bc = origin(h.b.second);
         const int first = static_cast<int>(dev.size());
         const bool diag = h.op == MTD_OP_POTRF || h.op == MTD_OP_GETRF;
         if (diag && nest > 0 && em > nest) {

@@ -40,7 +40,14 @@ public:
     int64_t n() const { return n_; }
     int64_t tile() const { return tile_; }
     int tiles() const { return tiles_; }
+    int64_t origin(int t) const;  // first row (or column) of tile row t
     int64_t extent(int t) const;  // rows (or columns) of tile row t
+    // The largest power of two dividing every tile edge (and n): the alignment every tile
+    // origin and extent has.  With uniform tiles, the tile edge itself.
+    int64_t unit() const;
+    // Tile rows at the given element edges (edges[0] = 0 < edges[1] < ... < edges[T] = n)
+    // instead of uniform `tile`-wide ones; only before any task is recorded.
+    int set_edges(const std::vector<int64_t> &edges);
 
     // Returns the new task index, or a negative mtd_status.
     int add_task(int op, int wi, int wj, const int *reads, int nreads);
@@ -67,6 +74,7 @@ private:
     int kind_;
     int64_t n_, tile_;
     int tiles_;
+    std::vector<int64_t> edges_;  // empty: uniform tiles
     std::vector<HostTask> tasks_;
     std::vector<std::vector<int>> deps_;
     std::map<TileId, int> last_writer_;                 // tileIndexByMap (mustard.h:177)

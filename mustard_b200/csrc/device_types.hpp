@@ -31,6 +31,14 @@ constexpr int kBatchInfoOk = 0x7f7f7f7f;  // per-matrix info of a batched run be
 // and the row interchanges of one block column.
 constexpr int kOpPanelPiv = 103;
 constexpr int kOpLaswp = 104;
+// Shared memory a pivoted panel item needs besides its slab of w-wide rows: the pivot row
+// and the previous row c (w doubles each) and the per-warp reduction scratch.
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+constexpr int64_t panel_piv_extra_bytes(int w) {
+    return int64_t(2 * w) * 8 + int64_t(kThreads / 32) * (8 + 4) + 64;
+}
 
 // Cholesky adjoint operations (device tasks of the reverse sweep; see adjoint_ops.cuh).
 constexpr int kOpAdjTrsm = 20;    // C(m x n) := C * L^-1, L = n x n lower at (ar, ac) of the factor

@@ -34,13 +34,9 @@ using namespace mtd;
 
 namespace {
 
-constexpr int kThreadsHost = kThreads;
 constexpr int kGemmEdge = 128;   // output block of one GEMM work item
 constexpr int kTrsmCols = 64;    // columns of one TRSM work item
 constexpr int kSwapColsHost = 64;
-
-// Bytes a panel item needs besides its slab (the pivot row, the previous row c, reductions).
-int64_t panel_extra(int w) { return int64_t(2 * w) * 8 + int64_t(kThreadsHost / 32) * 12 + 64; }
 
 template <typename T>
 int dalloc(T **p, size_t count) {
@@ -120,7 +116,7 @@ namespace mtd {
 // fit the kernel's shared memory, never fewer rows than w (item 0 holds the diagonal tile);
 // 0 if more than `grid` items would be needed.
 int lupiv_panel_shape(int64_t m, int w, int smem_bytes, int grid, int *R_out) {
-    const int64_t rmax = (smem_bytes - panel_extra(w)) / (int64_t(w) * 8);
+    const int64_t rmax = (smem_bytes - panel_piv_extra_bytes(w)) / (int64_t(w) * 8);
     if (rmax < std::min<int64_t>(m, w)) return 0;
     int64_t P = ceil_div(m, std::min(m, rmax));
     int64_t R = std::max(ceil_div(m, P), std::min<int64_t>(m, w));

@@ -23,19 +23,11 @@ namespace piv {
 constexpr int kSwapCols = 64;    // columns of one row-interchange work item
 constexpr int kSwapChunk = 128;  // pivots gathered at a time (a panel's worth)
 
-// Shared memory of a panel item: the slab [w][R] (column-major, R rows), the pivot row and
-// the previous row c ([w] each), and the reduction scratch.
-__host__ __device__ constexpr size_t panel_extra_bytes(int w) {
-    return size_t(2 * w) * sizeof(double) + size_t(kThreads / 32) * (sizeof(double) + sizeof(int)) + 64;
-}
-__host__ __device__ constexpr size_t panel_smem_bytes(int w, int R) {
-    return size_t(w) * R * sizeof(double) + panel_extra_bytes(w);
-}
-// The inverse blocks of L_kk are formed after the slab is written back, in its space.
-constexpr size_t kInverseScratch = size_t(2) * kNB * kDiagLd * sizeof(double);
-// Exchange slots of one panel: per column parity, per item, (|a|, row, the row's w values);
-// then per parity the panel's row c before the interchange.
-__host__ __device__ constexpr size_t slot_doubles(int P, int w) { return size_t(2) * P * (w + 2) + size_t(2) * w; }
+// Shared memory of a panel item: the slab [w][R] (column-major, R rows), then the pivot row,
+// the previous row c and the reduction scratch (panel_piv_extra_bytes).  After the slab is
+// written back, item 0 forms the inverse blocks of L_kk in that space (two kNB x kDiagLd
+// blocks, always within the kernel's shared memory).
+static_assert(size_t(2) * kNB * kDiagLd * sizeof(double) <= size_t(kOpSmemBytes()), "inverse scratch fits");
 
 // Largest |value| with the smallest row on ties (LAPACK's idamax takes the first maximum).
 __device__ __forceinline__ void better(double &v, int &r, double v2, int r2) {

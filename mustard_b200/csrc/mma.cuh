@@ -400,6 +400,10 @@ struct BlockMmaT {
     // past ~1 s (in a correct run every copy lands and every warp arrives): the caller
     // reports a timeout.  Shared memory is free again on return.
 #if MTD_EARLY_CLAIM2
+    __device__ __forceinline__ bool run_sp(void *smem_raw, const T *A, int64_t lda, const T *B, int64_t ldb, int M,
+                                           int N, int K) {
+        return run_sp(smem_raw, A, lda, B, ldb, M, N, K, [] {});
+    }
     template <typename OnLast>
     __device__ __forceinline__ bool run_sp(void *smem_raw, const T *A, int64_t lda, const T *B, int64_t ldb, int M,
                                            int N, int K, OnLast on_last) {

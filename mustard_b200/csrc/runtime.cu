@@ -127,7 +127,7 @@ size_t elem_size(const mtd_graph *g) { return g->prec == MTD_PREC_FP64 ? sizeof(
 // whole 16-byte chunks of elements.
 bool use_vec2(const mtd_graph *g, const void *dA, int64_t lda) {
     const int64_t epc = 16 / static_cast<int64_t>(elem_size(g));
-    return (reinterpret_cast<uintptr_t>(dA) % 16 == 0) && (lda % epc == 0) && (g->dag.tile() % epc == 0) &&
+    return (reinterpret_cast<uintptr_t>(dA) % 16 == 0) && (lda % epc == 0) && (g->dag.unit() % epc == 0) &&
            (g->dag.n() % epc == 0);
 }
 
@@ -365,6 +365,12 @@ int mtd_graph_set_nest(mtd_graph *g, int nest) {
     return MTD_OK;
 }
 
+int mtd_graph_set_tile_edges(mtd_graph *g, const int64_t *edges, int count) {
+    if (!g || !edges || count < 2) return MTD_ERR_INVALID_ARG;
+    if (g->finalized) return MTD_ERR_STATE;
+    return g->dag.set_edges(std::vector<int64_t>(edges, edges + count));
+}
+
 int mtd_graph_set_timeout(mtd_graph *g, double seconds) {
     if (!g || !(seconds > 0.0) || seconds > 3600.0) return MTD_ERR_INVALID_ARG;
     g->timeout_s = seconds;
@@ -432,7 +438,7 @@ int mtd_graph_finalize(mtd_graph *g) {
     // FP32-accurate runs whose updates can take the three-pass tcgen05 path: the panels' low
     // parts (the TMA boxes start on 32-row atoms, so n, the tile and the nested sub-tile are
     // multiples of 32)
-    if (g->prec == MTD_PREC_FP32 && g->dag.n() % 32 == 0 && g->dag.tile() % 32 == 0 && g->nest % 32 == 0) {
+    if (g->prec == MTD_PREC_FP32 && g->dag.n() % 32 == 0 && g->dag.unit() % 32 == 0 && g->nest % 32 == 0) {
         g->lo_ld = (g->dag.n() + 63) & ~int64_t(63);
         rc = rc ? rc : dev_alloc(&g->d_lo, size_t(g->lo_ld) * size_t(g->dag.n()));
     }
@@ -644,10 +650,10 @@ static int run_persistent(mtd_graph *g, void *dA, int64_t lda, void *stream, int
     // 32-row atom (tile and nested sub-tile edges multiples of 32); updates whose depth is
     // not a whole number of 64-column stages use the cp.async path
     const bool tf32_items = g->prec == MTD_PREC_TF32 || g->prec == MTD_PREC_BF16;
-    if (tf32_items && vec2 && g->dag.tile() % 32 == 0 && g->nest % 32 == 0) mtd::encode_tmap(a, dA, g->dag.n(), lda);
+    if (tf32_items && vec2 && g->dag.unit() % 32 == 0 && g->nest % 32 == 0) mtd::encode_tmap(a, dA, g->dag.n(), lda);
     // BF16 updates read the BF16 copy by TMA when every item's rows start on a 64-row atom;
     // the others keep the TF32 path on the FP32 matrix
-    if (g->prec == MTD_PREC_BF16 && vec2 && g->dag.tile() % 64 == 0 && g->nest % 64 == 0)
+    if (g->prec == MTD_PREC_BF16 && vec2 && g->dag.unit() % 64 == 0 && g->nest % 64 == 0)
         mtd::encode_tmap_bf16(a, g->d_bf16, g->dag.n(), g->bf16_ld);
     // FP32-accurate runs: the three-pass tcgen05 updates read the matrix and its low parts by
     // TMA (boxes of 32-deep slices); the TRSM items write the low parts only then
@@ -661,7 +667,7 @@ static int run_persistent(mtd_graph *g, void *dA, int64_t lda, void *stream, int
     }
     // FP64 GEMM / SYRK items read their operands by TMA when every operand block starts on a
     // 16-row atom (tile and nested sub-tile edges multiples of 16)
-    if (g->prec == MTD_PREC_FP64 && vec2 && g->dag.tile() % 16 == 0 && g->nest % 16 == 0 && g->use_tma64)
+    if (g->prec == MTD_PREC_FP64 && vec2 && g->dag.unit() % 16 == 0 && g->nest % 16 == 0 && g->use_tma64)
         mtd::encode_tmap64(a, dA, g->dag.n(), lda);
     const int grid = g->num_sms;
     g->last_grid = grid;

@@ -10,6 +10,10 @@
     python -m mustard_b200.profile_cases lupiv --n 8192 --tile 128
         LU with partial pivoting (mtd_lupiv) of a U[-1, 1) matrix (no diagonal boost, so most
         rows are interchanged)
+    python -m mustard_b200.profile_cases batch --n 512 --prec fp64
+        the batched factor-and-solve launch (mtd_batch_factor_solve) of `--n` matrices with
+        sizes and right-hand sides drawn as config 3 draws them (batch_bench.make_batch),
+        library default tiles; fp32: conversion + split-TF32 factor + FP64 refinement
     python -m mustard_b200.profile_cases gemm --n 8192 --tile 1024 --prec tf32
         the same cases on a float32 matrix with TF32 tensor-core products (tcgen05 GEMM /
         SYRK items fed by TMA; Cholesky and the GEMM-only step only); --prec bf16 (BF16
@@ -58,12 +62,14 @@ def op_breakdown(g):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["gemm", "chol", "lu", "lupiv"])
+    ap.add_argument("case", choices=["gemm", "chol", "lu", "lupiv", "batch"])
     ap.add_argument("--n", type=int, default=6144)
     ap.add_argument("--tile", type=int, default=768)
     ap.add_argument("--runs", type=int, default=2)
     ap.add_argument("--prec", choices=["fp64", "tf32", "bf16", "fp32"], default="fp64")
     ap.add_argument("--nest", type=int, default=None, help="nested sub-tile edge of the diagonal factorisations")
+    ap.add_argument("--first", type=int, default=0, help="a narrower first tile of this edge")
+    ap.add_argument("--last", type=int, default=0, help="the end of the matrix in tiles of at most this edge")
     ap.add_argument("--trace", action="store_true", help="per-operation item-time breakdown")
     ap.add_argument("--trace-out", default=None,
                     help="also write the records, task spans and critical path to this JSON file")
@@ -74,14 +80,23 @@ def main():
     t = (n + b - 1) // b
     if args.case == "lupiv":
         return run_pivoted(n, b, args.runs)
+    if args.case == "batch":
+        return run_batch(n, args.prec, args.runs)
     a = torch.empty((n, n), dtype=torch.float64, device="cuda").t()
+    edges = tile_edges(n, b, args.first, args.last) if (args.first or args.last) else None
     if args.case == "lu":
         mtd.generate(a, mtd.GEN_UNIFORM_DIAG, seed=3)
-        g = mtd.TaskGraph(mtd.KIND_LU, n, b).build_tiled()
+        g = mtd.TaskGraph(mtd.KIND_LU, n, b)
+        if edges:
+            g.set_tile_edges(edges)
+        g.build_tiled()
         flops = 2.0 * n ** 3 / 3
     elif args.case == "chol":
         mtd.generate(a, mtd.GEN_SPD, seed=3)
-        g = mtd.TaskGraph(mtd.KIND_CHOLESKY, n, b).build_tiled()
+        g = mtd.TaskGraph(mtd.KIND_CHOLESKY, n, b)
+        if edges:
+            g.set_tile_edges(edges)
+        g.build_tiled()
         flops = n ** 3 / 3.0
     else:
         mtd.generate(a, mtd.GEN_SPD, seed=3)
@@ -129,6 +144,55 @@ def main():
                                 else trace_analysis.summary(g, recs))["critical_path"]
     print(json.dumps(rec))
     g.close()
+
+
+def tile_edges(n, b, first, last):
+    """0, first, then b-wide tiles while at least `last` elements (or one b tile) remain, the
+    rest in near-equal tiles of at most `last` (multiples of 64)."""
+    edges = [0]
+    if first:
+        edges.append(first)
+    tail = last or b
+    while n - edges[-1] > b + tail:
+        edges.append(edges[-1] + b)
+    rest = n - edges[-1]
+    pieces = max(1, -(-rest // tail))
+    for i in range(1, pieces):
+        edges.append(edges[-1] + ((rest // pieces) // 64) * 64)
+    edges.append(n)
+    return edges
+
+
+def run_batch(count, prec, runs):
+    from mustard_b200 import batch_bench
+    if prec not in ("fp64", "fp32"):
+        raise SystemExit("batch: --prec fp64 or fp32")
+    sizes, nrhs, groups, rhs = batch_bench.make_batch(count, 7)
+    a64 = batch_bench.views(groups, count)
+    p, dt = batch_bench.PRECS[prec]
+    work_groups = {k: (idx, a.to(dt).clone()) for k, (idx, a) in groups.items()}
+    work = batch_bench.views(work_groups, count)
+    xs = [torch.zeros_like(r) for r in rhs]
+    b = mtd.Batch(sizes, prec=p)
+    kw = dict(method=mtd.REFINE_NONE) if prec == "fp64" else dict(method=mtd.REFINE_IR, tol=1e-13, max_iter=30)
+    s = torch.cuda.current_stream()
+    ms = 0.0
+    for _ in range(runs):
+        for k, (idx, w) in work_groups.items():
+            w.copy_(groups[k][1].to(dt))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        b.factor_solve(work, rhs, xs, a64=a64, stream=s, **kw)
+        e1.record(s)
+        rc, info, lat, berr, its, st = b.solve_status()
+        if rc:
+            raise mtd.MtdError(rc)
+        ms = e0.elapsed_time(e1)
+    flops = sum(k ** 3 / 3.0 for k in sizes)
+    print(json.dumps({"case": "batch", "prec": prec, "count": count, "tasks": b.num_tasks, "ms": ms,
+                      "tflops": flops / (ms * 1e-3) / 1e12, "max_backward_error": st["max_backward_error"],
+                      "converged": st["converged_count"]}))
+    b.close()
 
 
 def run_pivoted(n, b, runs):

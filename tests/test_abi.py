@@ -62,6 +62,33 @@ def test_build_tiled_matches_oracle_dependencies(mtd, kind, n, b):
     g.close()
 
 
+@pytest.mark.parametrize("kind", ["chol", "lu"])
+def test_tile_edges_give_the_reference_order_over_uneven_tiles(mtd, kind):
+    # custom tile edges (a narrower first and last tile): the same task list and dependencies
+    # as the reference's order over that many tiles; bad edge lists are refused, and so are
+    # edges set after tasks exist
+    k = mtd.KIND_CHOLESKY if kind == "chol" else mtd.KIND_LU
+    edges = [0, 512, 2048, 3584, 4096, 4600]
+    g = mtd.TaskGraph(k, 4600, 1536).set_tile_edges(edges).build_tiled()
+    t = len(edges) - 1
+    tasks = tiled.cholesky_tasks(t) if kind == "chol" else tiled.lu_tasks(t)
+    want = tiled.subgraph_dependencies(tasks)
+    assert g.num_tasks == len(tasks)
+    for i in range(len(tasks)):
+        assert g.deps(i) == want[i], i
+    with pytest.raises(mtd.MtdError):
+        g.set_tile_edges(edges)  # tasks already recorded
+    g.close()
+    for bad in ([0, 4600], [0, 700, 700, 4600], [1, 4600], [0, 2000, 4000], [0, 3000, 2000, 4600]):
+        h = mtd.TaskGraph(k, 4600, 1536)
+        if bad == [0, 4600]:
+            h.set_tile_edges(bad)  # one tile is allowed
+        else:
+            with pytest.raises(mtd.MtdError):
+                h.set_tile_edges(bad)
+        h.close()
+
+
 def test_creator_mirror_records_reference_calls(mtd):
     # The reference driver's capture sequence for Cholesky T=3 (cholesky_mustard.cu:224-395).
     c = mtd.TiledGraphCreator(mtd.KIND_CUSTOM, 90, 30)

@@ -217,6 +217,25 @@ def test_nested_diagonal_factorisation(mtd, kind, nest):
     g.close()
 
 
+@pytest.mark.parametrize("kind", ["chol", "lu"])
+def test_uneven_tile_edges(mtd, kind):
+    # a narrower first and last tile (mtd_graph_set_tile_edges), nested diagonal
+    # factorisations inside the wide ones: the factors match LAPACK's as with uniform tiles
+    n = 3000
+    edges = [0, 256, 1024, 1792, 2560, 2816, 3000]
+    a = gen.spd_input(n, 21) if kind == "chol" else gen.lu_input(n, 21)
+    g = mtd.TaskGraph(mtd.KIND_CHOLESKY if kind == "chol" else mtd.KIND_LU, n, 768)
+    g.set_tile_edges(edges).build_tiled().finalize()
+    d = to_dev(a)
+    assert g.run(d) == 0
+    out = from_dev(d)
+    if kind == "chol":
+        assert rel_diff(np.tril(out), np.tril(tiled.cholesky_lapack(a))) <= TOL
+    else:
+        assert rel_diff(out, tiled.lu_nopiv_lapack(a)) <= TOL
+    g.close()
+
+
 def test_nest_edge_must_be_multiple_of_64(mtd):
     g = mtd.TaskGraph(mtd.KIND_CHOLESKY, 600, 300).build_tiled()
     with pytest.raises(mtd.MtdError):
