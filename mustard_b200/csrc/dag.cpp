@@ -181,9 +181,9 @@ int items_of(const DevTask &t) {
     }
     case MTD_OP_TRSM_RLT:
     case MTD_OP_TRSM_RUN:
-        return static_cast<int>(ceil_div(t.m, kPanelRows));
+        return static_cast<int>(ceil_div(t.m, kTrsmRows));
     case MTD_OP_TRSM_LLNU:
-        return static_cast<int>(ceil_div(t.n, kPanelRows));
+        return static_cast<int>(ceil_div(t.n, kTrsmRows));
     default:  // diagonal factorisations, and a join's one no-op item
         return 1;
     }

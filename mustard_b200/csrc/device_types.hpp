@@ -14,7 +14,14 @@ constexpr int kNumQueues = 3;
 #endif
 constexpr int kThreads = MTD_THREADS;  // threads per persistent CTA
 constexpr int kGemmTile = 128;  // output sub-tile edge of one GEMM / SYRK work item
-constexpr int kPanelRows = 64;  // rows (or columns) of one TRSM work item
+constexpr int kPanelRows = 64;  // rows of one TRSM work item of the adjoint
+// Rows (or columns) of one TRSM strip of the tiled factorisations: 64, or 128 (fewer, larger
+// items whose updates run on the 128 x 128 update engine).
+#ifndef MTD_TRSM_ROWS
+#define MTD_TRSM_ROWS 64
+#endif
+constexpr int kTrsmRows = MTD_TRSM_ROWS;
+static_assert(kTrsmRows == 64 || kTrsmRows == 128, "TRSM strips are 64 or 128 rows");
 constexpr int kNB = 64;         // diagonal block edge inside POTRF / GETRF (and inverse blocks)
 constexpr int kNestTile = 128;  // default sub-tile edge of a nested diagonal factorisation
 

@@ -15,6 +15,8 @@
 // solver.  The LU operations are FP64 only.
 #pragma once
 
+#include <type_traits>
+
 #include "device_types.hpp"
 #include "mma.cuh"
 #include "tma64.cuh"
@@ -70,8 +72,19 @@ using PanelMma = BlockMmaT<T, 64, 64, kPanelWarpsM, kPanelWarpsN, BL, VEC, MTD_P
 #endif
 template <int BL, int VEC, typename T = double, int SPLIT = 1>
 using WideMma = BlockMmaT<T, 64, 128, 4, kThreads / 32 / 4, BL, VEC, MTD_PANEL_STAGES, MTD_PANEL_BK, SPLIT>;
+template <int VEC, int BL = kBKContig, typename T = double, int SPLIT = 1>
+using TallMma = BlockMmaT<T, 128, 64, kThreads / 32 / 2, 2, BL, VEC, MTD_PANEL_STAGES, MTD_PANEL_BK, SPLIT>;
+// The engines of one TRSM strip: its solve steps (kTrsmRows x 64 blocks: row strips; 64 x
+// kTrsmRows: column strips) and its updates over two inverse blocks (kTrsmRows x 128 and
+// 128 x kTrsmRows).  128-row strips run their updates on the 128 x 128 update engine.
+template <int BL, int VEC, typename T = double, int SPLIT = 1>
+using StripStep = std::conditional_t<kTrsmRows == 128, TallMma<VEC, BL, T, SPLIT>, PanelMma<BL, VEC, T, SPLIT>>;
+template <int BL, int VEC, typename T = double, int SPLIT = 1>
+using StripUpdate = std::conditional_t<kTrsmRows == 128, GemmMma<BL, VEC, T, SPLIT>, WideMma<BL, VEC, T, SPLIT>>;
 template <int VEC>
-using TallMma = BlockMmaT<double, 128, 64, kThreads / 32 / 2, 2, kBKContig, VEC, MTD_PANEL_STAGES, MTD_PANEL_BK>;
+using ColStripStep = std::conditional_t<kTrsmRows == 128, WideMma<kBKContig, VEC>, PanelMma<kBKContig, VEC>>;
+template <int VEC>
+using ColStripUpdate = std::conditional_t<kTrsmRows == 128, GemmMma<kBKContig, VEC>, TallMma<VEC>>;
 
 __device__ __forceinline__ void block_fence_sync() {
     __threadfence_block();
@@ -556,7 +569,7 @@ __device__ int op_getrf(const RunArgs &p, const MatCtx &m, const DevTask &t, voi
 }
 
 // ---------------------------------------------------------------------------------
-// TRSM work items: kPanelRows-row (or -column) strips of the block being solved,
+// TRSM work items: kTrsmRows-row (or -column) strips of the block being solved,
 // left-looking over the kNB-wide diagonal blocks of the triangular block.
 // ---------------------------------------------------------------------------------
 
@@ -608,9 +621,9 @@ __device__ __forceinline__ bool trsm_run(const RunArgs &p, E &e, void *smem, con
 // X = X * L^-T   (cublasDtrsm R, L, T, NonUnit; cholesky_mustard.cu:281)
 template <typename T, int VEC, int SPLIT = 1>
 __device__ int op_trsm_rlt(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
-    using Mn = PanelMma<kBNContig, VEC, T, SPLIT>;
-    const int r0 = item * kPanelRows;
-    const int mm = min(kPanelRows, t.m - r0);
+    using Mn = StripStep<kBNContig, VEC, T, SPLIT>;
+    const int r0 = item * kTrsmRows;
+    const int mm = min(kTrsmRows, t.m - r0);
     const int nk = t.n;
     const int64_t lda = m.lda, ldw = m.wsld;
     T *X = at<T>(m, t.cr + r0, t.cc);
@@ -633,7 +646,7 @@ __device__ int op_trsm_rlt(const RunArgs &p, const MatCtx &m, const DevTask &t, 
         return true;
     };
 #if MTD_TRSM_WIDE
-    using Mw = WideMma<kBNContig, VEC, T, SPLIT>;
+    using Mw = StripUpdate<kBNContig, VEC, T, SPLIT>;
     for (int jb = 0; jb < nk; jb += 2 * kNB) {
         const int jw = min(2 * kNB, nk - jb);
         if (jb > 0) {  // X(:, jb .. jb + jw) -= X(:, 0 .. jb) L(jb .. jb + jw, 0 .. jb)^T
@@ -674,9 +687,9 @@ __device__ int op_trsm_rlt(const RunArgs &p, const MatCtx &m, const DevTask &t, 
 // X = X * U^-1   (cublasDtrsm R, U, N, NonUnit; lu_mustard.cu:459)
 template <int VEC>
 __device__ int op_trsm_run(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
-    using Mk = PanelMma<kBKContig, VEC>;
-    const int r0 = item * kPanelRows;
-    const int mm = min(kPanelRows, t.m - r0);
+    using Mk = StripStep<kBKContig, VEC>;
+    const int r0 = item * kTrsmRows;
+    const int mm = min(kTrsmRows, t.m - r0);
     const int nk = t.n;
     const int64_t lda = m.lda, ldw = m.wsld;
     double *X = at<double>(m, t.cr + r0, t.cc);
@@ -691,7 +704,7 @@ __device__ int op_trsm_run(const RunArgs &p, const MatCtx &m, const DevTask &t, 
         return true;
     };
 #if MTD_TRSM_WIDE
-    using Mw = WideMma<kBKContig, VEC>;
+    using Mw = StripUpdate<kBKContig, VEC>;
     for (int jb = 0; jb < nk; jb += 2 * kNB) {
         const int jw = min(2 * kNB, nk - jb);
         if (jb > 0) {  // X(:, jb .. jb + jw) -= X(:, 0 .. jb) U(0 .. jb, jb .. jb + jw)
@@ -732,9 +745,9 @@ __device__ int op_trsm_run(const RunArgs &p, const MatCtx &m, const DevTask &t, 
 // X = L^-1 * X, unit diagonal   (cublasDtrsm L, L, N, Unit; lu_mustard.cu:413)
 template <int VEC>
 __device__ int op_trsm_llnu(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
-    using Mk = PanelMma<kBKContig, VEC>;
-    const int c0 = item * kPanelRows;
-    const int nc = min(kPanelRows, t.n - c0);
+    using Mk = ColStripStep<VEC>;
+    const int c0 = item * kTrsmRows;
+    const int nc = min(kTrsmRows, t.n - c0);
     const int nk = t.m;
     const int64_t lda = m.lda, ldw = m.wsld;
     double *X = at<double>(m, t.cr, t.cc + c0);
@@ -749,7 +762,7 @@ __device__ int op_trsm_llnu(const RunArgs &p, const MatCtx &m, const DevTask &t,
         return true;
     };
 #if MTD_TRSM_WIDE
-    using Mt = TallMma<VEC>;
+    using Mt = ColStripUpdate<VEC>;
     for (int jb = 0; jb < nk; jb += 2 * kNB) {
         const int jw = min(2 * kNB, nk - jb);
         if (jb > 0) {  // X(jb .. jb + jw, :) -= L(jb .. jb + jw, 0 .. jb) X(0 .. jb, :)
@@ -902,7 +915,8 @@ constexpr int kOpSmemBytes() {
     constexpr int w1 = WideMma<kBNContig, 2>::SMEM_BYTES > WideMma<kBKContig, 2>::SMEM_BYTES
                            ? WideMma<kBNContig, 2>::SMEM_BYTES
                            : WideMma<kBKContig, 2>::SMEM_BYTES;
-    constexpr int w = w1 > TallMma<2>::SMEM_BYTES ? w1 : TallMma<2>::SMEM_BYTES;
+    constexpr int w2 = w1 > TallMma<2>::SMEM_BYTES ? w1 : TallMma<2>::SMEM_BYTES;
+    constexpr int w = w2 > TallMma<2, kBNContig>::SMEM_BYTES ? w2 : TallMma<2, kBNContig>::SMEM_BYTES;
     static_assert(w <= 227 * 1024, "wide TRSM engine stages fit shared memory");
 #else
     constexpr int w = 0;

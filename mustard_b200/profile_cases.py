@@ -56,8 +56,20 @@ def op_breakdown(g):
         d.sort()
         ops[name] = {"items": len(d), "median_us": d[len(d) // 2], "sum_ms": sum(d) * 1e-3,
                      "share": sum(d) / total}
+    # gaps between consecutive items of one CTA: completing one item and claiming the next
+    # (or waiting for work)
+    by_sm = {}
+    for s, e, sm, _task, _item in tr:
+        by_sm.setdefault(sm, []).append((s, e))
+    gaps = []
+    for v in by_sm.values():
+        v.sort()
+        gaps += [(b[0] - a[1]) * 1e-3 for a, b in zip(v, v[1:])]
+    gaps.sort()
+    gap = {"count": len(gaps), "median_us": gaps[len(gaps) // 2] if gaps else 0.0,
+           "p90_us": gaps[(9 * len(gaps)) // 10] if gaps else 0.0, "sum_ms": sum(gaps) * 1e-3}
     from mustard_b200 import trace_analysis
-    return {"span_ms": (t1 - t0) * 1e-6, "busy": trace_analysis.busy_fraction(tr), "ops": ops}
+    return {"span_ms": (t1 - t0) * 1e-6, "busy": trace_analysis.busy_fraction(tr), "ops": ops, "gaps": gap}
 
 
 def main():
