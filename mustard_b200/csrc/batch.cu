@@ -396,6 +396,7 @@ int stage_factor(mtd_batch *b, void *const *dA, const int64_t *lda, cudaStream_t
 // The run arguments every batched launch shares (the task tables are the caller's).
 RunArgs batch_args(const mtd_batch *b) {
     RunArgs a{};
+    a.opset = kOpsCholesky;  // every matrix's graph is a tiled Cholesky (+ its solve tasks)
     a.qctl = b->d_qctl;
     a.ctl = b->d_ctl;
     a.ws_lower = b->d_ws;

@@ -15,9 +15,9 @@ namespace mtd {
 
 namespace {
 
-template <int VEC, typename T, int SPLIT>
+template <int VEC, typename T, int SPLIT, int OPS = kOpsAll>
 bool allow_smem(int bytes) {
-    return cudaFuncSetAttribute(persistent_kernel<VEC, T, SPLIT, false, false, true>,
+    return cudaFuncSetAttribute(persistent_kernel<VEC, T, SPLIT, false, false, true, OPS>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
 }
 
@@ -31,6 +31,7 @@ int solve_smem_setup(int device) {
     if (!done[device].load(std::memory_order_relaxed)) {
         const int bytes = kOpSmemBytes();
         const bool ok = allow_smem<2, double, 1>(bytes) && allow_smem<1, double, 1>(bytes) &&
+                        allow_smem<2, double, 1, kOpsCholesky>(bytes) && allow_smem<2, double, 1, kOpsLu>(bytes) &&
                         allow_smem<2, float, 1>(bytes) && allow_smem<1, float, 1>(bytes) &&
                         allow_smem<2, float, 3>(bytes) && allow_smem<1, float, 3>(bytes);
         if (!ok) return MTD_ERR_CUDA;
@@ -58,7 +59,13 @@ int launch_run_solve(const RunArgs &a, const int *deps_init, const int *roots, i
     seed_kernel<<<1, kSeedThreads, 0, s>>>(a, roots, n_roots);
     const int bytes = kOpSmemBytes();
     if (prec == MTD_PREC_FP64) {
-        if (vec2) persistent_kernel<2, double, 1, false, false, true><<<grid, kThreads, bytes, s>>>(a);
+        // the batched factor-and-solve (Cholesky) and the pivoted LU run instances compiled with
+        // their own operations only
+        if (vec2 && a.opset == kOpsCholesky)
+            persistent_kernel<2, double, 1, false, false, true, kOpsCholesky><<<grid, kThreads, bytes, s>>>(a);
+        else if (vec2 && a.opset == kOpsLu)
+            persistent_kernel<2, double, 1, false, false, true, kOpsLu><<<grid, kThreads, bytes, s>>>(a);
+        else if (vec2) persistent_kernel<2, double, 1, false, false, true><<<grid, kThreads, bytes, s>>>(a);
         else persistent_kernel<1, double, 1, false, false, true><<<grid, kThreads, bytes, s>>>(a);
     } else if (prec == MTD_PREC_FP32) {
         if (vec2) persistent_kernel<2, float, 3, false, false, true><<<grid, kThreads, bytes, s>>>(a);

@@ -131,6 +131,11 @@ struct alignas(128) RunCtl {
 };
 
 // Everything the persistent kernel needs for one run (passed by value).
+// Operation families a run's tasks use; FP64 runs whose tasks are all Cholesky (POTRF, TRSM_RLT,
+// SYRK, GEMM_NT) or all LU (GETRF, TRSM_LLNU, TRSM_RUN, GEMM_NN) operations launch a kernel
+// instance compiled with that family's operations only.
+enum : int { kOpsAll = 0, kOpsCholesky = 1, kOpsLu = 2 };
+
 struct RunArgs {
     void *a;               // matrix, column-major (double, or float for the low-precision factor)
     int64_t lda;
@@ -203,6 +208,7 @@ struct RunArgs {
     unsigned int *panel_bar;
     int n_panel_bar;
     double *panel_slots;
+    int opset;             // kOpsAll / kOpsCholesky / kOpsLu: the kernel instance the host launches
 };
 
 }  // namespace mtd

@@ -311,6 +311,7 @@ int mtd_lupiv_run(mtd_lupiv *h, double *dA, int64_t lda, int *d_ipiv, void *stre
     a.panel_bar = h->d_bar;
     a.n_panel_bar = h->T;
     a.panel_slots = h->d_slots;
+    a.opset = kOpsLu;  // panel, interchange, TRSM_LLNU and GEMM_NN tasks
     const bool vec2 = reinterpret_cast<uintptr_t>(dA) % 16 == 0 && lda % 2 == 0 && h->n % 2 == 0 && h->tile % 2 == 0;
     const int rc = launch_run_solve(a, h->d_deps_init, h->d_roots, h->n_roots, h->total_items, MTD_PREC_FP64, vec2,
                                     h->sms, s);

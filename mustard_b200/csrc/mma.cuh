@@ -51,6 +51,11 @@ namespace mtd {
 #ifndef MTD_SPLIT_PHASE_TRSM
 #define MTD_SPLIT_PHASE_TRSM 0
 #endif
+// 1: BlockMmaT::run_sp_update keeps the C pointer, its leading dimension and the lower flag
+// in shared memory during the k-loop.
+#ifndef MTD_STAGE_C_PARK
+#define MTD_STAGE_C_PARK 0
+#endif
 
 enum { kBNContig = 0, kBKContig = 1 };
 
@@ -408,8 +413,11 @@ struct BlockMmaT {
     __device__ __forceinline__ bool run_sp(void *smem_raw, const T *A, int64_t lda, const T *B, int64_t ldb, int M,
                                            int N, int K, OnLast on_last) {
 #else
+    // end_sync false: no CTA barrier at the end, so each warp goes on to its own epilogue as
+    // soon as its last slice is read; the caller then must pass a CTA barrier before shared
+    // memory or these barriers are used again.
     __device__ __forceinline__ bool run_sp(void *smem_raw, const T *A, int64_t lda, const T *B, int64_t ldb, int M,
-                                           int N, int K) {
+                                           int N, int K, bool end_sync = true) {
 #endif
         __shared__ alignas(8) unsigned long long full[STAGES], empty[STAGES];
         if (K <= 0) return true;
@@ -467,7 +475,167 @@ struct BlockMmaT {
             }
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
+#if MTD_EARLY_CLAIM2
         __syncthreads();
+#else
+        if (end_sync) __syncthreads();
+#endif
+        return ok;
+    }
+
+    // C block staging of run_sp_update: four chunks of BN / 4 columns, each [column][row] with
+    // the A stage's padded row stride, in the A and B stages of the two slices before the last.
+    static constexpr int kCCols = BN / 4;
+    static constexpr int kCLd = BM + SmemPad<T>::a;
+    static constexpr int kCPiecesPerCol = BM / EPC;                   // 16-byte copies per column
+    static constexpr int kCColsPerPass = kThreads / kCPiecesPerCol;  // columns one pass of the CTA copies
+    static constexpr bool kStageC = sizeof(T) == 8 && STAGES == 3 && AL == kAMContig && BN % 4 == 0 &&
+                                    kCCols * kCLd <= A_STAGE && kCCols * kCLd <= B_STAGE &&
+                                    kThreads % kCPiecesPerCol == 0 && kCCols % kCColsPerPass == 0 &&
+                                    (kCLd * int(sizeof(T))) % 16 == 0;
+
+    // C(r, c) -= A(M x K) * B(K x N) for r < M, c < N (with lower_only, only where r >= c): the
+    // update items' k-loop and C update in one.  The split-phase k-loop of run_sp, except that
+    // before computing the last slice every thread copies its share of the C block (cp.async)
+    // into the stages the two slices before it used (once every warp has read them), so the
+    // read half of the read-modify-write overlaps that slice's compute instead of following it;
+    // each warp then subtracts its accumulators from the staged C and stores the result.  Needs
+    // at least three slices, 16-byte aligned C columns and M a multiple of the copy width, else
+    // it runs run_sp and sub_from.  Ends without a CTA barrier: the caller passes one before
+    // shared memory or the barriers are used again.  Returns false if a wait ran past ~1 s.
+    __device__ __forceinline__ bool run_sp_update(void *smem_raw, const T *A, int64_t lda, const T *B, int64_t ldb,
+                                                  int M, int N, int K, T *C, int64_t ldc, bool lower_only) {
+        const int ktiles = (K + BK - 1) / BK;
+        if constexpr (kStageC) {
+            if (ktiles >= 3 && VEC == 2 && M % EPC == 0 && ldc % EPC == 0 &&
+                (reinterpret_cast<uintptr_t>(C) & 15) == 0)
+                return run_sp_staged_c(smem_raw, A, lda, B, ldb, M, N, K, C, ldc, lower_only);
+        }
+#if MTD_EARLY_CLAIM2
+        if (!run_sp(smem_raw, A, lda, B, ldb, M, N, K)) return false;
+#else
+        if (!run_sp(smem_raw, A, lda, B, ldb, M, N, K, false)) return false;
+#endif
+        sub_from(C, ldc, M, N, lower_only, 0, 0);
+        return true;
+    }
+
+    __device__ __forceinline__ bool run_sp_staged_c(void *smem_raw, const T *A, int64_t lda, const T *B, int64_t ldb,
+                                                    int M, int N, int K, T *C, int64_t ldc, bool lower_only) {
+        __shared__ alignas(8) unsigned long long full[STAGES], empty[STAGES], cfull;
+#if MTD_STAGE_C_PARK
+        // C, ldc and lower wait in shared memory during the k-loop, out of its registers
+        __shared__ T *park_c;
+        __shared__ int64_t park_ldc;
+        __shared__ int park_lower;
+        if (threadIdx.x == 0) {
+            park_c = C;
+            park_ldc = ldc;
+            park_lower = lower_only ? 1 : 0;
+        }
+#endif
+        T *As = static_cast<T *>(smem_raw);
+        T *Bs = As + STAGES * A_STAGE;
+        const int ktiles = (K + BK - 1) / BK;  // >= 3
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int s = 0; s < STAGES; ++s) {
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&full[s])), "r"(kThreads));
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&empty[s])), "r"(kThreads / 32));
+            }
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&cfull)), "r"(kThreads));
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        const unsigned long long deadline = global_ns() + 1000000000ull;
+        bool ok = true;
+        auto wait = [&](unsigned long long *bar, uint32_t parity) {
+            for (unsigned it = 0; ok; ++it) {
+                uint32_t done;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                    "selp.u32 %0, 1, 0, p;\n\t}"
+                    : "=r"(done)
+                    : "r"(smem_u32(bar)), "r"(parity)
+                    : "memory");
+                if (done) return;
+                if ((it & 63) == 63 && global_ns() > deadline) ok = false;
+            }
+        };
+        auto fill = [&](int slice) {
+            const int st = slice % STAGES;
+            load_a(As + st * A_STAGE, A, lda, M, K, slice * BK);
+            load_b(Bs + st * B_STAGE, B, ldb, N, K, slice * BK);
+            asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(&full[st])) : "memory");
+        };
+        // C chunk q: the A (q = 0, 1) or B (q = 2, 3) stage of slice ktiles - 2 (q even) or
+        // ktiles - 3 (q odd)
+        auto chunk = [&](int q) {
+            const int s = (ktiles - 2 - (q & 1)) % STAGES;
+            return q < 2 ? As + s * A_STAGE : Bs + s * B_STAGE;
+        };
+#pragma unroll
+        for (int s = 0; s < STAGES - 1; ++s) fill(s);
+        for (int kt = 0; kt < ktiles; ++kt) {
+            const int st = kt % STAGES;
+            wait(&full[st], (kt / STAGES) & 1);
+            if (kt == ktiles - 1) {
+#if MTD_STAGE_C_PARK
+                C = *static_cast<T *volatile *>(&park_c);
+                ldc = *static_cast<volatile int64_t *>(&park_ldc);
+#endif
+                // every warp has read slices kt - 1 and kt - 2: their stages take the C block
+                wait(&empty[(kt - 1) % STAGES], ((kt - 1) / STAGES) & 1);
+                wait(&empty[(kt - 2) % STAGES], ((kt - 2) / STAGES) & 1);
+                const int r = EPC * (threadIdx.x % kCPiecesPerCol);
+                const int c_in = threadIdx.x / kCPiecesPerCol;
+#pragma unroll
+                for (int u = 0; u < BN / kCColsPerPass; ++u) {
+                    constexpr int kPassesPerChunk = kCCols / kCColsPerPass;
+                    const int c = u * kCColsPerPass + c_in;
+                    const bool in = r < M && c < N;
+                    cp_async16(chunk(u / kPassesPerChunk) + (c - (u / kPassesPerChunk) * kCCols) * kCLd + r,
+                               in ? C + r + int64_t(c) * ldc : C, in);
+                }
+                asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(&cfull)) : "memory");
+            }
+            compute_stage(As + st * A_STAGE, Bs + st * B_STAGE);
+            __syncwarp();
+            if ((threadIdx.x & 31) == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[st])) : "memory");
+            const int nk = kt + STAGES - 1;
+            if (nk < ktiles) {
+                if (kt >= 1) wait(&empty[nk % STAGES], ((kt - 1) / STAGES) & 1);  // slice kt - 1 read by all
+                fill(nk);
+            }
+        }
+        wait(&cfull, 0);
+#if MTD_STAGE_C_PARK
+        lower_only = *static_cast<volatile int *>(&park_lower) != 0;
+#endif
+        if (ok) {
+            const int lane = threadIdx.x & 31;
+            const int warp = threadIdx.x >> 5;
+            const int wm0 = (warp / WARPS_N) * WM;
+            const int wn0 = (warp % WARPS_N) * WN;
+            const int g = lane >> 2;
+            const int t = lane & 3;
+#pragma unroll
+            for (int i = 0; i < FM; ++i)
+#pragma unroll
+                for (int j = 0; j < FN; ++j)
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) {
+                        const int r = wm0 + i * 16 + g + ((v & 2) ? 8 : 0);
+                        const int c = wn0 + j * 8 + 2 * t + (v & 1);
+                        if (r < M && c < N && (!lower_only || r >= c)) {
+                            const int q = c / kCCols;
+                            C[r + int64_t(c) * ldc] = chunk(q)[(c - q * kCCols) * kCLd + r] - acc[i][j][v];
+                        }
+                    }
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
         return ok;
     }
 

@@ -42,6 +42,7 @@ struct mtd_graph {
     // on the cp.async engine, which measured faster on B200 (the TMA engine's swizzled
     // fragment addressing costs more issue slots than the copies it saves)
     bool use_tma64 = false;
+    int opset = kOpsAll;  // operation family of the lowered tasks (the FP64 kernel instance)
     int prec = MTD_PREC_FP64;  // element type of the matrix runs factor
     unsigned short *d_bf16 = nullptr;  // MTD_PREC_BF16: BF16 copy of the panels (bf16_ld x n)
     int64_t bf16_ld = 0;
@@ -110,6 +111,13 @@ int smem_setup(int device) {
             cudaFuncSetAttribute(persistent_kernel<VEC, double, 1, false, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
             return MTD_ERR_CUDA;
+        if constexpr (VEC == 2) {
+            if (cudaFuncSetAttribute(persistent_kernel<2, double, 1, false, false, false, kOpsCholesky>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess ||
+                cudaFuncSetAttribute(persistent_kernel<2, double, 1, false, false, false, kOpsLu>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
+                return MTD_ERR_CUDA;
+        }
         done[device].store(true, std::memory_order_release);
     }
     return MTD_OK;
@@ -120,6 +128,20 @@ int smem_setup(int device) {
 // size.  Every entry point that lays out a workspace uses this one rule.
 int64_t ws_ld_for(int64_t n) { return (n + 3) & ~int64_t(3); }
 int64_t ws_ld(const mtd_graph *g) { return ws_ld_for(g->dag.n()); }
+
+// The operation family of a lowered task list (joins belong to every family).
+int opset_of(const std::vector<DevTask> &tasks) {
+    bool chol = true, lu = true;
+    for (const auto &t : tasks) {
+        if (t.op == kOpJoin) continue;
+        const bool c = t.op == MTD_OP_POTRF || t.op == MTD_OP_TRSM_RLT || t.op == MTD_OP_SYRK_LN || t.op == MTD_OP_GEMM_NT;
+        const bool l = t.op == MTD_OP_GETRF || t.op == MTD_OP_TRSM_LLNU || t.op == MTD_OP_TRSM_RUN || t.op == MTD_OP_GEMM_NN;
+        chol = chol && c;
+        lu = lu && l;
+    }
+    return chol ? kOpsCholesky : lu ? kOpsLu : kOpsAll;
+}
+
 
 size_t elem_size(const mtd_graph *g) { return g->prec == MTD_PREC_FP64 ? sizeof(double) : sizeof(float); }
 
@@ -401,6 +423,7 @@ int mtd_graph_finalize(mtd_graph *g) {
     }
     if (roots.empty()) return MTD_ERR_BAD_DAG;
     g->n_dev = nt;
+    g->opset = opset_of(tasks);
     const size_t ws = size_t(ws_ld(g)) * kNB * elem_size(g);  // bytes
     g->total_items = 0;
     for (int q = 0; q < kNumQueues; ++q) {
@@ -625,6 +648,10 @@ int launch_run(const RunArgs &a, const int *deps_init, const int *roots, int n_r
         return cudaGetLastError() == cudaSuccess ? MTD_OK : MTD_ERR_CUDA;
     }
     if (fp64 && vec2 && a.tma64) persistent_kernel<2, double, 1, false, true><<<grid, kThreads, bytes, s>>>(a);
+    else if (fp64 && vec2 && a.opset == kOpsCholesky)
+        persistent_kernel<2, double, 1, false, false, false, kOpsCholesky><<<grid, kThreads, bytes, s>>>(a);
+    else if (fp64 && vec2 && a.opset == kOpsLu)
+        persistent_kernel<2, double, 1, false, false, false, kOpsLu><<<grid, kThreads, bytes, s>>>(a);
     else if (fp64 && vec2) persistent_kernel<2, double><<<grid, kThreads, bytes, s>>>(a);
     else if (fp64) persistent_kernel<1, double><<<grid, kThreads, bytes, s>>>(a);
     else if (x3 && vec2) persistent_kernel<2, float, 3><<<grid, kThreads, bytes, s>>>(a);
@@ -671,6 +698,7 @@ static int run_persistent(mtd_graph *g, void *dA, int64_t lda, void *stream, int
         mtd::encode_tmap64(a, dA, g->dag.n(), lda);
     const int grid = g->num_sms;
     g->last_grid = grid;
+    a.opset = g->opset;
     const int rc = launch_run(a, g->d_deps_init, g->d_roots, g->n_roots, g->total_items, g->prec, vec2, grid, s,
                               false);
     if (rc) return rc;
@@ -943,7 +971,12 @@ extern "C" int mtd_factor_noalloc(int kind, double *dA, int64_t n, int64_t lda, 
         static_cast<int>(std::min<long long>(1024, (std::max<long long>(items, nt) + kThreads - 1) / kThreads));
     reset_kernel<<<std::max(reset_blocks, 1), kThreads, 0, s>>>(a, d_deps_init);
     seed_kernel<<<1, kSeedThreads, 0, s>>>(a, d_roots, static_cast<int>(roots.size()));
-    if (vec2) persistent_kernel<2, double><<<sms, kThreads, kOpSmemBytes(), s>>>(a);
+    const int opset = opset_of(low.tasks);
+    if (vec2 && opset == kOpsCholesky)
+        persistent_kernel<2, double, 1, false, false, false, kOpsCholesky><<<sms, kThreads, kOpSmemBytes(), s>>>(a);
+    else if (vec2 && opset == kOpsLu)
+        persistent_kernel<2, double, 1, false, false, false, kOpsLu><<<sms, kThreads, kOpSmemBytes(), s>>>(a);
+    else if (vec2) persistent_kernel<2, double><<<sms, kThreads, kOpSmemBytes(), s>>>(a);
     else persistent_kernel<1, double><<<sms, kThreads, kOpSmemBytes(), s>>>(a);
     if (cudaGetLastError() != cudaSuccess) return MTD_ERR_CUDA;
     RunCtl c;

@@ -317,13 +317,15 @@ __device__ __noinline__ int op_batch_convert(const RunArgs &p, const DevTask &t,
 // SOLVE: the instances of the batched factor-and-solve launch and of the pivoted LU, which
 // also run their own tasks (solve, conversion; pivoted panel, row interchanges); the other
 // instances carry none of that code.
-template <int VEC, typename T, int SPLIT = 1, bool ADJ = false, bool SOLVE = false>
+template <int VEC, typename T, int SPLIT = 1, bool ADJ = false, bool SOLVE = false, int OPS = kOpsAll>
 __device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int item, void *smem,
                                         tc::State *tcs = nullptr, t64::State *s64 = nullptr) {
     if constexpr (SOLVE) {
-        if (t.op == kOpBatchSolve) return op_batch_solve<T>(p, t, smem);
-        if (t.op == kOpBatchConvert) return op_batch_convert<T>(p, t, item);
-        if constexpr (sizeof(T) == 8) {
+        if constexpr (OPS != kOpsLu) {
+            if (t.op == kOpBatchSolve) return op_batch_solve<T>(p, t, smem);
+            if (t.op == kOpBatchConvert) return op_batch_convert<T>(p, t, item);
+        }
+        if constexpr (sizeof(T) == 8 && OPS != kOpsCholesky) {
             if (t.op == kOpPanelPiv) return op_panel_piv(p, mat_ctx<T>(p, t), t, item, smem);
             if (t.op == kOpLaswp) return op_laswp(p, mat_ctx<T>(p, t), t, item, smem);
         }
@@ -336,16 +338,23 @@ __device__ __forceinline__ int dispatch(const RunArgs &p, const DevTask &t, int 
     if constexpr (uses_tcgen05<VEC, T, SPLIT, ADJ>() && SPLIT == 1)
         if (t.op == MTD_OP_GEMM_NT || t.op == MTD_OP_SYRK_LN) return op_update_tc(p, m, t, item, smem, tcs);
     if constexpr (sizeof(T) == 8) {
-        switch (t.op) {
-        case MTD_OP_POTRF: return op_potrf<T, VEC>(p, m, t, smem);
-        case MTD_OP_TRSM_RLT: return op_trsm_rlt<T, VEC>(p, m, t, item, smem);
-        case MTD_OP_SYRK_LN: return op_syrk_ln<T, VEC>(p, m, t, item, smem, s64);
-        case MTD_OP_GEMM_NT: return op_gemm_nt<T, VEC>(p, m, t, item, smem, s64);
-        case MTD_OP_GETRF: return op_getrf<VEC>(p, m, t, smem);
-        case MTD_OP_TRSM_LLNU: return op_trsm_llnu<VEC>(p, m, t, item, smem);
-        case MTD_OP_TRSM_RUN: return op_trsm_run<VEC>(p, m, t, item, smem);
-        case MTD_OP_GEMM_NN: return op_gemm_nn<VEC>(p, m, t, item, smem, s64);
-        default: break;
+        if constexpr (OPS != kOpsLu) {
+            switch (t.op) {
+            case MTD_OP_POTRF: return op_potrf<T, VEC>(p, m, t, smem);
+            case MTD_OP_TRSM_RLT: return op_trsm_rlt<T, VEC>(p, m, t, item, smem);
+            case MTD_OP_SYRK_LN: return op_syrk_ln<T, VEC>(p, m, t, item, smem, s64);
+            case MTD_OP_GEMM_NT: return op_gemm_nt<T, VEC>(p, m, t, item, smem, s64);
+            default: break;
+            }
+        }
+        if constexpr (OPS != kOpsCholesky) {
+            switch (t.op) {
+            case MTD_OP_GETRF: return op_getrf<VEC>(p, m, t, smem);
+            case MTD_OP_TRSM_LLNU: return op_trsm_llnu<VEC>(p, m, t, item, smem);
+            case MTD_OP_TRSM_RUN: return op_trsm_run<VEC>(p, m, t, item, smem);
+            case MTD_OP_GEMM_NN: return op_gemm_nn<VEC>(p, m, t, item, smem, s64);
+            default: break;
+            }
         }
     } else {
         switch (t.op) {
@@ -605,7 +614,9 @@ __device__ __forceinline__ void persistent_loop_ws(const RunArgs &p, double *sme
 // T64: the instance whose FP64 GEMM / SYRK items may read their operands by TMA (tma64.cuh,
 // runs that carry the tensor maps); the other instances carry none of that code.
 // SOLVE: the batched factor-and-solve launch's instances (see dispatch).
-template <int VEC, typename T, int SPLIT = 1, bool ADJ = false, bool T64 = false, bool SOLVE = false>
+// OPS: the operation family the instance carries (kOpsAll: every operation).
+template <int VEC, typename T, int SPLIT = 1, bool ADJ = false, bool T64 = false, bool SOLVE = false,
+          int OPS = kOpsAll>
 __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const __grid_constant__ RunArgs p) {
     extern __shared__ __align__(128) double smem[];
     constexpr bool kTc = uses_tcgen05<VEC, T, SPLIT, ADJ>();
@@ -652,7 +663,7 @@ __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const __grid_co
             const unsigned long long t_start = p.trace ? global_ns() : 0ull;
             DevTask t;
             load_task(p, task, &t);
-            const int st = dispatch<VEC, T, SPLIT, ADJ, SOLVE>(p, t, item, smem, nullptr, kT64 ? &s64 : nullptr);
+            const int st = dispatch<VEC, T, SPLIT, ADJ, SOLVE, OPS>(p, t, item, smem, nullptr, kT64 ? &s64 : nullptr);
             if (threadIdx.x == 0) s_st = st;
             __syncthreads();
             prev_task = task;
@@ -688,7 +699,7 @@ __global__ void __launch_bounds__(kThreads, 1) persistent_kernel(const __grid_co
             const unsigned long long t_start = p.trace ? global_ns() : 0ull;
             DevTask t;
             load_task(p, task, &t);
-            const int st = dispatch<VEC, T, SPLIT, ADJ, SOLVE>(p, t, item, smem, nullptr, kT64 ? &s64 : nullptr);
+            const int st = dispatch<VEC, T, SPLIT, ADJ, SOLVE, OPS>(p, t, item, smem, nullptr, kT64 ? &s64 : nullptr);
             __syncthreads();
             if (threadIdx.x == 0) finish_item(p, task, item, t_start, st == 0);
         }

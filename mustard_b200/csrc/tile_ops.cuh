@@ -577,9 +577,14 @@ __device__ int op_getrf(const RunArgs &p, const MatCtx &m, const DevTask &t, voi
 // reporting MTD_ERR_TIMEOUT) if a wait of the latter expired.
 template <bool SP, typename E, typename T>
 __device__ __forceinline__ bool eng_run(const RunArgs &p, E &e, void *smem, const T *A, int64_t lda, const T *B,
-                                        int64_t ldb, int M, int N, int K) {
+                                        int64_t ldb, int M, int N, int K, bool end_sync = true) {
     if constexpr (SP) {
-        if (!e.run_sp(smem, A, lda, B, ldb, M, N, K)) {
+#if MTD_EARLY_CLAIM2
+        const bool ran = e.run_sp(smem, A, lda, B, ldb, M, N, K);
+#else
+        const bool ran = e.run_sp(smem, A, lda, B, ldb, M, N, K, end_sync);
+#endif
+        if (!ran) {
             if (threadIdx.x == 0) report_error(p.ctl, MTD_ERR_TIMEOUT, 0);
             return false;
         }
@@ -597,7 +602,32 @@ __device__ __forceinline__ bool eng_run(const RunArgs &p, E &e, void *smem, cons
 static __device__ __noinline__ void early_claim(const RunArgs &p);
 #endif
 
-// The update items' k-loop (MTD_SPLIT_PHASE) and the TRSM strips' (MTD_SPLIT_PHASE_TRSM).
+// 0: the update items' split-phase k-loop ends without a CTA barrier; each warp subtracts its
+// accumulators from C as soon as it has read its last slice, and the persistent loop's barrier
+// after the item is the first one every warp meets.  Measured on one B200 (ms, tile 1536, one
+// call, base / this / base): LU N = 24000 298.2 / 296.5 / 297.8, Cholesky 152.0 / 151.5 /
+// 151.9, GEMM-only N = 12288 4.83 / 4.81.
+#ifndef MTD_UPDATE_END_SYNC
+#define MTD_UPDATE_END_SYNC 0
+#endif
+// 1: FP64 update items copy their C block into shared memory during the last k-slice
+// (BlockMmaT::run_sp_update) instead of reading it after the k-loop.  A traced GEMM-only run
+// (N = 12288, tile 1536; probe timestamps after the k-loop and after the C update) put 8.8 us
+// of a 228 us item in the C read-modify-write after the k-loop.  Measured with the kernel
+// instances per operation family (ms, N = 24000, tile 1536, one call): Cholesky 152.7 ->
+// 150.3 (GEMM_NT item 224.4 -> 222.0 us), GEMM-only N = 12288 4.81 -> 4.74; for the LU's
+// GEMM_NN items the staged update measured slower (item 221.3 -> 223.0 us, LU 296.0 ->
+// 297.5 ms), so they keep the plain C update (MTD_STAGE_C_NN=0).
+#ifndef MTD_STAGE_C
+#define MTD_STAGE_C 1
+#endif
+#ifndef MTD_STAGE_C_NN
+#define MTD_STAGE_C_NN 0
+#endif
+
+// The update items' k-loop (MTD_SPLIT_PHASE) and the TRSM strips' (MTD_SPLIT_PHASE_TRSM).  The
+// update items return straight to the persistent loop after their C update, which passes a CTA
+// barrier before the next item touches shared memory.
 template <typename E, typename T>
 __device__ __forceinline__ bool gemm_run(const RunArgs &p, E &e, void *smem, const T *A, int64_t lda, const T *B,
                                          int64_t ldb, int M, int N, int K) {
@@ -610,8 +640,28 @@ __device__ __forceinline__ bool gemm_run(const RunArgs &p, E &e, void *smem, con
         return true;
     }
 #endif
-    return eng_run<MTD_SPLIT_PHASE != 0>(p, e, smem, A, lda, B, ldb, M, N, K);
+    return eng_run<MTD_SPLIT_PHASE != 0>(p, e, smem, A, lda, B, ldb, M, N, K, MTD_UPDATE_END_SYNC != 0);
 }
+// An update item's k-loop and C update: C -= A B (operand layouts as the engine's), lower
+// triangle only when lower.  The split-phase engine stages C in shared memory during the last
+// k-slice (BlockMmaT::run_sp_update); false (after reporting MTD_ERR_TIMEOUT) if a wait expired.
+template <bool STAGED = true, typename E, typename T>
+__device__ __forceinline__ bool update_run(const RunArgs &p, E &e, void *smem, const T *A, int64_t lda, const T *B,
+                                           int64_t ldb, int M, int N, int K, T *C, int64_t ldc, bool lower) {
+#if MTD_SPLIT_PHASE && !MTD_EARLY_CLAIM2 && MTD_STAGE_C
+    if constexpr (STAGED) {
+        if (!e.run_sp_update(smem, A, lda, B, ldb, M, N, K, C, ldc, lower)) {
+            if (threadIdx.x == 0) report_error(p.ctl, MTD_ERR_TIMEOUT, 0);
+            return false;
+        }
+        return true;
+    }
+#endif
+    if (!gemm_run(p, e, smem, A, lda, B, ldb, M, N, K)) return false;
+    e.sub_from(C, ldc, M, N, lower, 0, 0);
+    return true;
+}
+
 template <typename E, typename T>
 __device__ __forceinline__ bool trsm_run(const RunArgs &p, E &e, void *smem, const T *A, int64_t lda, const T *B,
                                          int64_t ldb, int M, int N, int K) {
@@ -849,9 +899,9 @@ __device__ int op_gemm_nt(const RunArgs &p, const MatCtx &m, const DevTask &t, i
                                            at<double>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn, false);
     Mg e;
     e.zero();
-    if (!gemm_run(p, e, smem, at<T>(m, t.ar + r0, t.ac), m.lda, at<T>(m, t.br + c0, t.bc), m.lda, mm, nn, t.k))
+    if (!update_run(p, e, smem, at<T>(m, t.ar + r0, t.ac), m.lda, at<T>(m, t.br + c0, t.bc), m.lda, mm, nn, t.k,
+                    at<T>(m, t.cr + r0, t.cc + c0), m.lda, false))
         return MTD_ERR_TIMEOUT;
-    e.sub_from(at<T>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn);
     return 0;
 }
 
@@ -869,10 +919,10 @@ __device__ int op_gemm_nn(const RunArgs &p, const MatCtx &m, const DevTask &t, i
                                            at<double>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn, false);
     Mg e;
     e.zero();
-    if (!gemm_run(p, e, smem, at<double>(m, t.ar + r0, t.ac), m.lda, at<double>(m, t.br, t.bc + c0), m.lda, mm, nn,
-                  t.k))
+    if (!update_run<MTD_STAGE_C_NN != 0>(p, e, smem, at<double>(m, t.ar + r0, t.ac), m.lda,
+                                         at<double>(m, t.br, t.bc + c0), m.lda, mm, nn, t.k,
+                                         at<double>(m, t.cr + r0, t.cc + c0), m.lda, false))
         return MTD_ERR_TIMEOUT;
-    e.sub_from(at<double>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn);
     return 0;
 }
 
@@ -892,9 +942,9 @@ __device__ int op_syrk_ln(const RunArgs &p, const MatCtx &m, const DevTask &t, i
                                            at<double>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn, pb == qb);
     Mg e;
     e.zero();
-    if (!gemm_run(p, e, smem, at<T>(m, t.ar + r0, t.ac), m.lda, at<T>(m, t.ar + c0, t.ac), m.lda, mm, nn, t.k))
+    if (!update_run(p, e, smem, at<T>(m, t.ar + r0, t.ac), m.lda, at<T>(m, t.ar + c0, t.ac), m.lda, mm, nn, t.k,
+                    at<T>(m, t.cr + r0, t.cc + c0), m.lda, pb == qb))
         return MTD_ERR_TIMEOUT;
-    e.sub_from(at<T>(m, t.cr + r0, t.cc + c0), m.lda, mm, nn, pb == qb, 0, 0);
     return 0;
 }
 
