@@ -319,7 +319,7 @@ def run_reference(args, rank, world):
 # The ncu capture behind roofline.traffic (profiles/dram_traffic_bench_n24000_t1536.md):
 # DRAM read + write bytes of one step's two launches, and the hash of the FP64 kernel
 # sources it measured.
-TRAFFIC_CAPTURE = {"sources_sha16": "b86497b519d2a1c0", "bytes": 75478524672 + 33292412928 + 36982104576 + 16762892544}
+TRAFFIC_CAPTURE = {"sources_sha16": "8995394af24d932b", "bytes": 76591494144 + 29405362176 + 38803758592 + 15811395072}
 
 METRIC = "FP64-accurate LU/Cholesky TFLOP/s, N=24000, 1 B200: mixed+IR vs plain FP64"
 
@@ -528,7 +528,7 @@ def main():
                            if traffic else f"none for kernel sources {sources_sha}"),
         "traffic_unit": "bytes per step (LU launch + Cholesky launch)",
         "traffic_bytes_per_flop": traffic / flops_step if traffic else None,
-        "kernel": "mtd::persistent_kernel<2> (scheduler + all FP64 tile operations)",
+        "kernel": "mtd::persistent_kernel<2, double, 1, 0, 0, 0, OPS> (scheduler + the FP64 tile operations of one family: OPS 2 = LU, 1 = Cholesky)",
         "peak_source": "measured: register-only mma.sync.m16n8k8.f64 probe on this GPU",
         "frac_of_datasheet_37": achieved / DATASHEET_FP64_TFLOPS,
         "lu_tflops": flops_lu(n) / (t_lu / args.steps * 1e-3) / 1e12 if args.only != "chol" else None,

@@ -69,7 +69,8 @@ def op_breakdown(g):
     gap = {"count": len(gaps), "median_us": gaps[len(gaps) // 2] if gaps else 0.0,
            "p90_us": gaps[(9 * len(gaps)) // 10] if gaps else 0.0, "sum_ms": sum(gaps) * 1e-3}
     from mustard_b200 import trace_analysis
-    return {"span_ms": (t1 - t0) * 1e-6, "busy": trace_analysis.busy_fraction(tr), "ops": ops, "gaps": gap}
+    return {"span_ms": (t1 - t0) * 1e-6, "busy": trace_analysis.busy_fraction(tr),
+            "busy_by_twentieth": [round(v, 3) for v in trace_analysis.busy_profile(tr, 20)], "ops": ops, "gaps": gap}
 
 
 def main():

@@ -57,6 +57,40 @@ def busy_fraction(records):
     return busy / (len(per_sm) * (t1 - t0))
 
 
+def busy_profile(records, bins=20):
+    """The busy fraction per time bin: the run's span cut into ``bins`` equal parts, and for
+    each the SM-time inside items (overlapping items of one SM counted once) over the SMs seen
+    x the bin's length.  Shows where the idle time sits (start-up, tail, in between)."""
+    if not records or bins < 1:
+        return []
+    t0 = min(r[0] for r in records)
+    t1 = max(r[1] for r in records)
+    width = (t1 - t0) / bins
+    if width <= 0:
+        return [1.0] * bins
+    per_sm = {}
+    for s, e, sm, _, _ in records:
+        per_sm.setdefault(sm, []).append((s, e))
+    busy = [0.0] * bins
+    for iv in per_sm.values():
+        iv.sort()
+        merged = []
+        for s, e in iv:
+            if merged and s <= merged[-1][1]:
+                merged[-1][1] = max(merged[-1][1], e)
+            else:
+                merged.append([s, e])
+        for s, e in merged:
+            b0 = min(bins - 1, int((s - t0) / width))
+            b1 = min(bins - 1, int((e - t0) / width))
+            for b in range(b0, b1 + 1):
+                lo = max(s, t0 + b * width)
+                hi = min(e, t0 + (b + 1) * width)
+                if hi > lo:
+                    busy[b] += hi - lo
+    return [v / (len(per_sm) * width) for v in busy]
+
+
 def critical_path(graph, spans):
     """Tasks on the critical path, first to last: dicts with task, op, start, end, wait (ns)."""
     if not spans:

@@ -63,3 +63,12 @@ def test_op_breakdown_of_a_traced_run():
     assert ops["POTRF"]["items"] == 2 and ops["TRSM_RLT"]["items"] == 3 and ops["GEMM_NT"]["items"] == 2
     assert abs(sum(o["share"] for o in ops.values()) - 1.0) < 1e-12
     assert abs(ops["TRSM_RLT"]["sum_ms"] - (90 + 190 + 145) * 1e-6) < 1e-15
+
+
+def test_busy_profile_bins_the_idle_time():
+    # two SMs over [0, 100): SM 0 busy all the time, SM 1 only in [0, 50) (two overlapping items)
+    recs = [(0, 100, 0, 1, 0), (0, 30, 1, 2, 0), (20, 50, 1, 2, 1)]
+    prof = trace_analysis.busy_profile(recs, bins=4)
+    assert prof == [1.0, 1.0, 0.5, 0.5]
+    assert abs(sum(prof) / 4 - trace_analysis.busy_fraction(recs)) < 1e-12
+    assert trace_analysis.busy_profile([], bins=4) == []
