@@ -695,6 +695,39 @@ struct BlockMmaT {
         }
     }
 
+    // S[idx(r, c)] = C(r, c) - acc(r, c) for r < M, c < N and 0 elsewhere in the BM x BN block;
+    // S in shared memory at the offsets idx gives.  The loads of one fragment row are issued
+    // together, as in sub_from.
+    template <typename Idx>
+    __device__ __forceinline__ void sub_to_smem(const T *C, int64_t ldc, int M, int N, T *S, Idx &&idx) const {
+        const int lane = threadIdx.x & 31;
+        const int warp = threadIdx.x >> 5;
+        const int wm0 = (warp / WARPS_N) * WM;
+        const int wn0 = (warp % WARPS_N) * WN;
+        const int g = lane >> 2;
+        const int t = lane & 3;
+#pragma unroll
+        for (int i = 0; i < FM; ++i) {
+            T cv[FN][4];
+#pragma unroll
+            for (int j = 0; j < FN; ++j)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int r = wm0 + i * 16 + g + ((v & 2) ? 8 : 0);
+                    const int c = wn0 + j * 8 + 2 * t + (v & 1);
+                    cv[j][v] = (r < M && c < N) ? ld_cg(C + r + int64_t(c) * ldc) : T(0);
+                }
+#pragma unroll
+            for (int j = 0; j < FN; ++j)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int r = wm0 + i * 16 + g + ((v & 2) ? 8 : 0);
+                    const int c = wn0 + j * 8 + 2 * t + (v & 1);
+                    S[idx(r, c)] = (r < M && c < N) ? cv[j][v] - acc[i][j][v] : T(0);
+                }
+        }
+    }
+
     // C(r, c) = acc(r, c).
     __device__ __forceinline__ void store_to(T *C, int64_t ldc, int M, int N) const {
         for_each(M, N, [&](int r, int c, T v) { C[r + int64_t(c) * ldc] = v; });

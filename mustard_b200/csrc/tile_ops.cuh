@@ -174,8 +174,10 @@ __device__ __forceinline__ void lower_inverse(int jn, TL tl, E *X) {
 //     arithmetic of LAPACK's dpotf2 (l(r, j) = d(r, j) * (1 / sqrt(d(j, j))), then the
 //     rank-1 update; the reciprocal square root is CUDA's rsqrt, within 1 ulp), and then
 //     its inverse (lane c forms column c by forward substitution);
-//   - the whole CTA computes the panel below it, P = A_panel X^T, and the trailing update
-//     A -= P P^T (lower), each followed by one barrier.
+//   - the whole CTA computes the panel below it, P = A_panel X^T, then the trailing update
+//     A -= P P^T (lower) of the next panel's columns; warp 0 then factors the next panel's
+//     diagonal block while the other warps update the columns right of it (the serial
+//     factorisation off the critical chain of barriers).
 // The kNB x kNB inverses are composed from the panel inverses by doubling:
 // inv([La 0; L21 Lb]) = [Xa 0; -Xb (L21 Xa) Xb].
 // (The first design synchronised the CTA three times per column and formed the inverse
@@ -301,16 +303,47 @@ __device__ __noinline__ int chol_small(const RunArgs &p, const MatCtx &m, T *Ad,
     }
     if (tid == 0) *flag = -1;
     __syncthreads();
+    auto panel_inverse = [&](int q) { return XI + (q / kNB) * kNB * kInvLd + (q % kNB) * (1 + kInvLd); };
+    // trailing-update block: A(r, c) -= sum_l P(r, l) P(c, l) for the 4 x 4 block at (r0, c0),
+    // r >= c, P = the panel at columns p0 .. p0 + pw
+    auto update_block = [&](int p0, int pw, int r0, int c0) {
+        T acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[i][q] = T(0);
+#pragma unroll 2
+        for (int l = 0; l < PW; ++l) {
+            if (l >= pw) break;
+            T x[4], y[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                x[i] = S[min(r0 + i, kSmallChol - 1) + (p0 + l) * kSmallLd];
+                y[i] = S[min(c0 + i, kSmallChol - 1) + (p0 + l) * kSmallLd];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[i][q] += x[i] * y[q];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = r0 + i, c = c0 + q;
+                if (r < n && c < n && r >= c) S[r + c * kSmallLd] -= acc[i][q];
+            }
+    };
+    // the first panel's diagonal block
+    if (tid < 32) {
+        const int bad = warp_chol<T, PW>(S, 0, min(PW, n), rdiag, panel_inverse(0));
+        if (tid == 0 && bad >= 0) *flag = bad;
+    }
+    __syncthreads();
+    if (*flag >= 0) return diag_failure(p, m, MTD_ERR_NOT_POSITIVE_DEFINITE, info_base + *flag + 1);
     for (int p0 = 0; p0 < n; p0 += PW) {
         const int pw = min(PW, n - p0);
-        T *X = XI + (p0 / kNB) * kNB * kInvLd + (p0 % kNB) * (1 + kInvLd);  // panel inverse, kInvLd
-        if (tid < 32) {
-            const int bad = warp_chol<T, PW>(S, p0, pw, rdiag + p0, X);
-            if (tid == 0 && bad >= 0) *flag = p0 + bad;
-        }
-        __syncthreads();
-        const int bad = *flag;  // every thread reads the same flag
-        if (bad >= 0) return diag_failure(p, m, MTD_ERR_NOT_POSITIVE_DEFINITE, info_base + bad + 1);
+        T *X = panel_inverse(p0);  // factored and inverted (warp 0) before this iteration
         const int q0 = p0 + pw, nr = n - q0;
         if (nr <= 0) break;
         // panel below: P(r, c) = sum_{l <= c} A(r, p0 + l) X(c, l), rows q0 .., four columns a unit
@@ -346,43 +379,30 @@ __device__ __noinline__ int chol_small(const RunArgs &p, const MatCtx &m, T *Ad,
             }
             __syncthreads();
         }
-        // trailing update: A(r, c) -= sum_l P(r, l) P(c, l), r >= c >= q0, in 4 x 4 blocks
-        {
-            const int nb4 = (nr + 3) >> 2, blocks = nb4 * (nb4 + 1) / 2;
-            if (tid < blocks) {
-                int br = int((sqrtf(8.0f * float(tid) + 1.0f) - 1.0f) * 0.5f);
-                while ((br + 1) * (br + 2) / 2 <= tid) ++br;
-                while (br * (br + 1) / 2 > tid) --br;
-                const int r0 = q0 + 4 * br, c0 = q0 + 4 * (tid - br * (br + 1) / 2);
-                T acc[4][4];
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) acc[i][q] = T(0);
-#pragma unroll 2
-                for (int l = 0; l < PW; ++l) {
-                    if (l >= pw) break;
-                    T x[4], y[4];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        x[i] = S[min(r0 + i, kSmallChol - 1) + (p0 + l) * kSmallLd];
-                        y[i] = S[min(c0 + i, kSmallChol - 1) + (p0 + l) * kSmallLd];
-                    }
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) acc[i][q] += x[i] * y[q];
-                }
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int r = r0 + i, c = c0 + q;
-                        if (r < n && c < n && r >= c) S[r + c * kSmallLd] -= acc[i][q];
-                    }
-            }
-            __syncthreads();
+        // trailing update A(r, c) -= sum_l P(r, l) P(c, l), r >= c >= q0, in 4 x 4 blocks: the
+        // next panel's columns first (all threads); then warp 0 factors and inverts the next
+        // panel's diagonal block while warps 1 .. update the columns right of it
+        const int pwn = min(PW, nr), ca = (pwn + 3) >> 2, nb4 = (nr + 3) >> 2;
+        for (int b = tid; b < ca * nb4; b += kThreads) {
+            const int cb = b / nb4, rb = b % nb4;
+            if (rb >= cb) update_block(p0, pw, q0 + 4 * rb, q0 + 4 * cb);
         }
+        __syncthreads();
+        if (tid < 32) {
+            const int bad = warp_chol<T, PW>(S, q0, pwn, rdiag + q0, panel_inverse(q0));
+            if (tid == 0 && bad >= 0) *flag = q0 + bad;
+        } else {
+            const int nbr = nb4 - ca, blocks = nbr * (nbr + 1) / 2;
+            for (int b = tid - 32; b < blocks; b += kThreads - 32) {
+                int br = int((sqrtf(8.0f * float(b) + 1.0f) - 1.0f) * 0.5f);
+                while ((br + 1) * (br + 2) / 2 <= b) ++br;
+                while (br * (br + 1) / 2 > b) --br;
+                update_block(p0, pw, q0 + 4 * (ca + br), q0 + 4 * (ca + b - br * (br + 1) / 2));
+            }
+        }
+        __syncthreads();
+        const int bad = *flag;  // every thread reads the same flag
+        if (bad >= 0) return diag_failure(p, m, MTD_ERR_NOT_POSITIVE_DEFINITE, info_base + bad + 1);
     }
     // L to the matrix
     for (int e = tid; e < n * kSmallChol; e += kThreads) {
@@ -668,9 +688,289 @@ __device__ __forceinline__ bool trsm_run(const RunArgs &p, E &e, void *smem, con
     return eng_run<MTD_SPLIT_PHASE_TRSM != 0>(p, e, smem, A, lda, B, ldb, M, N, K);
 }
 
+// 1: the FP64 TRSM strips run each two-block step's solve products from shared memory (the
+// step's 64 x 128 block and the step's three 64 x 64 operand blocks staged there once)
+// instead of as three engine runs through global memory.
+// Measured on one B200 (one call each; traced item medians, N = 24000, tile 1536):
+// Cholesky TRSM_RLT items 842 -> 833 us, Cholesky 149.8 -> 149.0 ms.  The LU's strips
+// (MTD_TRSM_FUSED_LU, off): TRSM_LLNU / TRSM_RUN items 848 / 843 -> 822 / 822 us, but its
+// GEMM_NN items in the same kernel instance went 221.2 -> 223.9 us and the LU 295.4 -> 296.5 ms.
+#ifndef MTD_TRSM_FUSED
+#define MTD_TRSM_FUSED 1
+#endif
+#ifndef MTD_TRSM_FUSED_LU
+#define MTD_TRSM_FUSED_LU 0
+#endif
+
+// Leading dimension of the fused TRSM steps' shared-memory blocks: the 64 x 64 engine's padded
+// rows, so its compute_stage reads them as staged slices.
+constexpr int kStepLd = 64 + SmemPad<double>::a;
+
+// dst[k * kStepLd + n] = src[n + k * lds] for n < rows, k < cols, zero elsewhere in 64 x 64
+// (16-byte cp.async copies; rows even, src columns 16-byte aligned).  Completes at the
+// caller's cp_async_wait.
+__device__ __forceinline__ void stage_block64(double *dst, const double *src, int64_t lds, int rows, int cols) {
+    static_assert((64 * 32) % kThreads == 0, "whole passes of the CTA");
+#pragma unroll
+    for (int u = 0; u < 64 * 32 / kThreads; ++u) {
+        const int pc = threadIdx.x + u * kThreads;
+        const int k = pc / 32, n = 2 * (pc % 32);
+        const bool ok = k < cols && n < rows;
+        cp_async16(dst + k * kStepLd + n, ok ? src + n + int64_t(k) * lds : src, ok);
+    }
+}
+
+// X = X * L^-T for one 64-row strip, FP64 with 16-byte operands (op_trsm_rlt below): per step
+// of two inverse blocks (jb .. jb + 128), the wide update from global memory, then
+//   Y  = X(:, jb .. jb + 128) - update          (shared memory, SY)
+//   X1 = Y1 W1^T;  Y2 -= X1 L21^T;  X2 = Y2 W2^T  (64 x 64 products from shared memory)
+// with W1, L21, W2 staged by cp.async while Y is formed; X1 and X2 go to global memory.  The
+// same products in the same order as the engine-run steps, so the same results.
+template <int VEC>
+__device__ int trsm_rlt_fused(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
+    using Mw = WideMma<kBNContig, VEC>;
+    using Ms = PanelMma<kBNContig, VEC>;
+    const int r0 = item * kTrsmRows;
+    const int mm = min(kTrsmRows, t.m - r0);
+    const int nk = t.n;
+    const int64_t lda = m.lda, ldw = m.wsld;
+    double *X = at<double>(m, t.cr + r0, t.cc);
+    const double *L = at<double>(m, t.ar, t.ac);
+    const double *W = ws_lo<double>(m) + t.ar;
+    double *SY = static_cast<double *>(smem);  // 128 columns
+    double *SW1 = SY + 128 * kStepLd;
+    double *SL21 = SW1 + 64 * kStepLd;
+    double *SW2 = SL21 + 64 * kStepLd;
+    for (int jb = 0; jb < nk; jb += 2 * kNB) {
+        const int jw = min(2 * kNB, nk - jb);
+        const int j1 = min(kNB, jw), j2 = jw - j1;
+        {
+            Mw e;
+            e.zero();
+            // X(:, jb .. jb + jw) -= X(:, 0 .. jb) L(jb .. jb + jw, 0 .. jb)^T; the run ends at a
+            // CTA barrier, so its ring is free below
+            if (jb > 0 && !trsm_run(p, e, smem, X, lda, L + jb, lda, mm, jw, jb)) return MTD_ERR_TIMEOUT;
+            stage_block64(SW1, W + jb, ldw, j1, j1);
+            if (j2 > 0) {
+                stage_block64(SL21, L + (jb + kNB) + int64_t(jb) * lda, lda, j2, j1);
+                stage_block64(SW2, W + jb + kNB, ldw, j2, j2);
+            }
+            cp_async_commit();
+            e.sub_to_smem(X + int64_t(jb) * lda, lda, mm, jw, SY, [](int r, int c) { return r + c * kStepLd; });
+        }
+        cp_async_wait<0>();
+        __syncthreads();
+        {  // X1 = Y1 W1^T
+            Ms e;
+            e.zero();
+            e.compute_stage(SY, SW1);
+            e.compute_stage(SY + 32 * kStepLd, SW1 + 32 * kStepLd);
+            __syncthreads();  // every warp has read Y1
+            e.for_each(kNB, kNB, [&](int r, int c, double v) {
+                SY[r + c * kStepLd] = v;
+                if (r < mm && c < j1) X[r + int64_t(jb + c) * lda] = v;
+            });
+        }
+        __syncthreads();
+        if (j2 > 0) {
+            {  // Y2 -= X1 L21^T (each thread updates its own elements of SY's second half)
+                Ms e;
+                e.zero();
+                e.compute_stage(SY, SL21);
+                e.compute_stage(SY + 32 * kStepLd, SL21 + 32 * kStepLd);
+                e.for_each(kNB, kNB, [&](int r, int c, double v) { SY[r + (kNB + c) * kStepLd] -= v; });
+            }
+            __syncthreads();
+            {  // X2 = Y2 W2^T
+                Ms e;
+                e.zero();
+                e.compute_stage(SY + kNB * kStepLd, SW2);
+                e.compute_stage(SY + (kNB + 32) * kStepLd, SW2 + 32 * kStepLd);
+                e.for_each(kNB, kNB, [&](int r, int c, double v) {
+                    if (r < mm && c < j2) X[r + int64_t(jb + kNB + c) * lda] = v;
+                });
+            }
+        }
+        block_fence_sync();
+    }
+    return 0;
+}
+
+// A k-contiguous 64 x 64 operand block as the 64 x 64 engine stages it: two 32-deep slices of
+// kStepSliceB elements, dst[s * kStepSliceB + n * kStepLdK + kk] = src[(32 s + kk) + n * lds]
+// for k = 32 s + kk < krows, n < cols, zero elsewhere (16-byte cp.async copies; krows even,
+// src columns 16-byte aligned).  Completes at the caller's cp_async_wait.
+constexpr int kStepLdK = 32 + SmemPad<double>::bk;
+constexpr int kStepSliceB = 64 * kStepLdK;
+__device__ __forceinline__ void stage_block64_k(double *dst, const double *src, int64_t lds, int krows, int cols) {
+    static_assert((64 * 32) % kThreads == 0, "whole passes of the CTA");
+#pragma unroll
+    for (int u = 0; u < 64 * 32 / kThreads; ++u) {
+        const int pc = threadIdx.x + u * kThreads;
+        const int n = pc / 32, k = 2 * (pc % 32);  // k in 0 .. 63
+        const bool ok = n < cols && k < krows;
+        cp_async16(dst + (k / 32) * kStepSliceB + n * kStepLdK + (k % 32), ok ? src + k + int64_t(n) * lds : src, ok);
+    }
+}
+
+// X = X * U^-1 for one 64-row strip, FP64 with 16-byte operands (op_trsm_run below): the fused
+// steps of trsm_rlt_fused with U's blocks (k-contiguous B operands): X1 = Y1 W1,
+// Y2 -= X1 U12, X2 = Y2 W2 (W = the inverses of U's diagonal blocks).
+template <int VEC>
+__device__ int trsm_run_fused(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
+    using Mw = WideMma<kBKContig, VEC>;
+    using Ms = PanelMma<kBKContig, VEC>;
+    static_assert(Ms::LDB == kStepLdK && Ms::B_STAGE == kStepSliceB && Ms::LDA == kStepLd, "staged layouts");
+    const int r0 = item * kTrsmRows;
+    const int mm = min(kTrsmRows, t.m - r0);
+    const int nk = t.n;
+    const int64_t lda = m.lda, ldw = m.wsld;
+    double *X = at<double>(m, t.cr + r0, t.cc);
+    const double *U = at<double>(m, t.ar, t.ac);
+    const double *W = ws_up<double>(m) + t.ar;
+    double *SY = static_cast<double *>(smem);  // 128 columns
+    double *SW1 = SY + 2 * kNB * kStepLd;
+    double *SU12 = SW1 + 2 * kStepSliceB;
+    double *SW2 = SU12 + 2 * kStepSliceB;
+    for (int jb = 0; jb < nk; jb += 2 * kNB) {
+        const int jw = min(2 * kNB, nk - jb);
+        const int j1 = min(kNB, jw), j2 = jw - j1;
+        {
+            Mw e;
+            e.zero();
+            // X(:, jb .. jb + jw) -= X(:, 0 .. jb) U(0 .. jb, jb .. jb + jw)
+            if (jb > 0 && !trsm_run(p, e, smem, X, lda, U + int64_t(jb) * lda, lda, mm, jw, jb)) return MTD_ERR_TIMEOUT;
+            stage_block64_k(SW1, W + jb, ldw, j1, j1);
+            if (j2 > 0) {
+                stage_block64_k(SU12, U + jb + int64_t(jb + kNB) * lda, lda, j1, j2);
+                stage_block64_k(SW2, W + jb + kNB, ldw, j2, j2);
+            }
+            cp_async_commit();
+            e.sub_to_smem(X + int64_t(jb) * lda, lda, mm, jw, SY, [](int r, int c) { return r + c * kStepLd; });
+        }
+        cp_async_wait<0>();
+        __syncthreads();
+        {  // X1 = Y1 W1
+            Ms e;
+            e.zero();
+            e.compute_stage(SY, SW1);
+            e.compute_stage(SY + 32 * kStepLd, SW1 + kStepSliceB);
+            __syncthreads();  // every warp has read Y1
+            e.for_each(kNB, kNB, [&](int r, int c, double v) {
+                SY[r + c * kStepLd] = v;
+                if (r < mm && c < j1) X[r + int64_t(jb + c) * lda] = v;
+            });
+        }
+        __syncthreads();
+        if (j2 > 0) {
+            {  // Y2 -= X1 U12
+                Ms e;
+                e.zero();
+                e.compute_stage(SY, SU12);
+                e.compute_stage(SY + 32 * kStepLd, SU12 + kStepSliceB);
+                e.for_each(kNB, kNB, [&](int r, int c, double v) { SY[r + (kNB + c) * kStepLd] -= v; });
+            }
+            __syncthreads();
+            {  // X2 = Y2 W2
+                Ms e;
+                e.zero();
+                e.compute_stage(SY + kNB * kStepLd, SW2);
+                e.compute_stage(SY + (kNB + 32) * kStepLd, SW2 + kStepSliceB);
+                e.for_each(kNB, kNB, [&](int r, int c, double v) {
+                    if (r < mm && c < j2) X[r + int64_t(jb + kNB + c) * lda] = v;
+                });
+            }
+        }
+        block_fence_sync();
+    }
+    return 0;
+}
+
+// X = L^-1 X, unit diagonal, for one 64-column strip, FP64 with 16-byte operands
+// (op_trsm_llnu below): per step of two inverse blocks (rows jb .. jb + 128), the tall update
+// from global memory, then Y = X(jb .. jb + 128, :) - update in shared memory as the 64 x 64
+// engine's k-contiguous B slices (four 32-row slices), X1 = W1 Y1, Y2 -= L21 X1, X2 = W2 Y2
+// with W1, L21, W2 staged as m-contiguous A blocks.
+template <int VEC>
+__device__ int trsm_llnu_fused(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
+    using Mt = TallMma<VEC>;
+    using Ms = PanelMma<kBKContig, VEC>;
+    static_assert(Ms::LDB == kStepLdK && Ms::B_STAGE == kStepSliceB && Ms::LDA == kStepLd, "staged layouts");
+    const int c0 = item * kTrsmRows;
+    const int nc = min(kTrsmRows, t.n - c0);
+    const int nk = t.m;
+    const int64_t lda = m.lda, ldw = m.wsld;
+    double *X = at<double>(m, t.cr, t.cc + c0);
+    const double *L = at<double>(m, t.ar, t.ac);
+    const double *W = ws_lo<double>(m) + t.ar;
+    double *SY = static_cast<double *>(smem);  // 128 rows: four slices
+    double *SW1 = SY + 4 * kStepSliceB;
+    double *SL21 = SW1 + kNB * kStepLd;
+    double *SW2 = SL21 + kNB * kStepLd;
+    for (int jb = 0; jb < nk; jb += 2 * kNB) {
+        const int jw = min(2 * kNB, nk - jb);
+        const int j1 = min(kNB, jw), j2 = jw - j1;
+        {
+            Mt e;
+            e.zero();
+            // X(jb .. jb + jw, :) -= L(jb .. jb + jw, 0 .. jb) X(0 .. jb, :)
+            if (jb > 0 && !trsm_run(p, e, smem, L + jb, lda, X, lda, jw, nc, jb)) return MTD_ERR_TIMEOUT;
+            stage_block64(SW1, W + jb, ldw, j1, j1);
+            if (j2 > 0) {
+                stage_block64(SL21, L + (jb + kNB) + int64_t(jb) * lda, lda, j2, j1);
+                stage_block64(SW2, W + jb + kNB, ldw, j2, j2);
+            }
+            cp_async_commit();
+            e.sub_to_smem(X + jb, lda, jw, nc, SY,
+                          [](int r, int c) { return (r / 32) * kStepSliceB + c * kStepLdK + (r % 32); });
+        }
+        cp_async_wait<0>();
+        __syncthreads();
+        {  // X1 = W1 Y1
+            Ms e;
+            e.zero();
+            e.compute_stage(SW1, SY);
+            e.compute_stage(SW1 + 32 * kStepLd, SY + kStepSliceB);
+            __syncthreads();  // every warp has read Y1
+            e.for_each(kNB, kNB, [&](int r, int c, double v) {
+                SY[(r / 32) * kStepSliceB + c * kStepLdK + (r % 32)] = v;
+                if (r < j1 && c < nc) X[jb + r + int64_t(c) * lda] = v;
+            });
+        }
+        __syncthreads();
+        if (j2 > 0) {
+            {  // Y2 -= L21 X1
+                Ms e;
+                e.zero();
+                e.compute_stage(SL21, SY);
+                e.compute_stage(SL21 + 32 * kStepLd, SY + kStepSliceB);
+                e.for_each(kNB, kNB, [&](int r, int c, double v) {
+                    SY[(2 + r / 32) * kStepSliceB + c * kStepLdK + (r % 32)] -= v;
+                });
+            }
+            __syncthreads();
+            {  // X2 = W2 Y2
+                Ms e;
+                e.zero();
+                e.compute_stage(SW2, SY + 2 * kStepSliceB);
+                e.compute_stage(SW2 + 32 * kStepLd, SY + 3 * kStepSliceB);
+                e.for_each(kNB, kNB, [&](int r, int c, double v) {
+                    if (r < j2 && c < nc) X[jb + kNB + r + int64_t(c) * lda] = v;
+                });
+            }
+        }
+        block_fence_sync();
+    }
+    return 0;
+}
+
 // X = X * L^-T   (cublasDtrsm R, L, T, NonUnit; cholesky_mustard.cu:281)
 template <typename T, int VEC, int SPLIT = 1>
 __device__ int op_trsm_rlt(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
+#if MTD_TRSM_FUSED && MTD_TRSM_WIDE
+    if constexpr (sizeof(T) == 8 && VEC == 2 && kTrsmRows == 64 && kNB == 64)
+        return trsm_rlt_fused<VEC>(p, m, t, item, smem);
+#endif
     using Mn = StripStep<kBNContig, VEC, T, SPLIT>;
     const int r0 = item * kTrsmRows;
     const int mm = min(kTrsmRows, t.m - r0);
@@ -737,6 +1037,9 @@ __device__ int op_trsm_rlt(const RunArgs &p, const MatCtx &m, const DevTask &t, 
 // X = X * U^-1   (cublasDtrsm R, U, N, NonUnit; lu_mustard.cu:459)
 template <int VEC>
 __device__ int op_trsm_run(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
+#if MTD_TRSM_FUSED_LU && MTD_TRSM_WIDE
+    if constexpr (VEC == 2 && kTrsmRows == 64 && kNB == 64) return trsm_run_fused<VEC>(p, m, t, item, smem);
+#endif
     using Mk = StripStep<kBKContig, VEC>;
     const int r0 = item * kTrsmRows;
     const int mm = min(kTrsmRows, t.m - r0);
@@ -795,6 +1098,9 @@ __device__ int op_trsm_run(const RunArgs &p, const MatCtx &m, const DevTask &t, 
 // X = L^-1 * X, unit diagonal   (cublasDtrsm L, L, N, Unit; lu_mustard.cu:413)
 template <int VEC>
 __device__ int op_trsm_llnu(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
+#if MTD_TRSM_FUSED_LU && MTD_TRSM_WIDE
+    if constexpr (VEC == 2 && kTrsmRows == 64 && kNB == 64) return trsm_llnu_fused<VEC>(p, m, t, item, smem);
+#endif
     using Mk = ColStripStep<VEC>;
     const int c0 = item * kTrsmRows;
     const int nc = min(kTrsmRows, t.n - c0);
@@ -978,5 +1284,9 @@ constexpr int kOpSmemBytes() {
     static_assert(t64::kSmemBytes <= (m > d ? m : d), "the FP64 TMA ring fits the engines' shared memory");
     return m > d ? m : d;
 }
+static_assert((2 * kNB + 3 * kNB) * kStepLd * int(sizeof(double)) <= kOpSmemBytes() &&
+                  (2 * kNB * kStepLd + 6 * kStepSliceB) * int(sizeof(double)) <= kOpSmemBytes() &&
+                  (4 * kStepSliceB + 3 * kNB * kStepLd) * int(sizeof(double)) <= kOpSmemBytes(),
+              "a fused TRSM step's blocks fit the operations' shared memory");
 
 }  // namespace mtd
