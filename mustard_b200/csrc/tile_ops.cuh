@@ -174,10 +174,8 @@ __device__ __forceinline__ void lower_inverse(int jn, TL tl, E *X) {
 //     arithmetic of LAPACK's dpotf2 (l(r, j) = d(r, j) * (1 / sqrt(d(j, j))), then the
 //     rank-1 update; the reciprocal square root is CUDA's rsqrt, within 1 ulp), and then
 //     its inverse (lane c forms column c by forward substitution);
-//   - the whole CTA computes the panel below it, P = A_panel X^T, then the trailing update
-//     A -= P P^T (lower) of the next panel's columns; warp 0 then factors the next panel's
-//     diagonal block while the other warps update the columns right of it (the serial
-//     factorisation off the critical chain of barriers).
+//   - the whole CTA computes the panel below it, P = A_panel X^T, and the trailing update
+//     A -= P P^T (lower), each followed by one barrier.
 // The kNB x kNB inverses are composed from the panel inverses by doubling:
 // inv([La 0; L21 Lb]) = [Xa 0; -Xb (L21 Xa) Xb].
 // (The first design synchronised the CTA three times per column and formed the inverse
@@ -303,47 +301,16 @@ __device__ __noinline__ int chol_small(const RunArgs &p, const MatCtx &m, T *Ad,
     }
     if (tid == 0) *flag = -1;
     __syncthreads();
-    auto panel_inverse = [&](int q) { return XI + (q / kNB) * kNB * kInvLd + (q % kNB) * (1 + kInvLd); };
-    // trailing-update block: A(r, c) -= sum_l P(r, l) P(c, l) for the 4 x 4 block at (r0, c0),
-    // r >= c, P = the panel at columns p0 .. p0 + pw
-    auto update_block = [&](int p0, int pw, int r0, int c0) {
-        T acc[4][4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc[i][q] = T(0);
-#pragma unroll 2
-        for (int l = 0; l < PW; ++l) {
-            if (l >= pw) break;
-            T x[4], y[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                x[i] = S[min(r0 + i, kSmallChol - 1) + (p0 + l) * kSmallLd];
-                y[i] = S[min(c0 + i, kSmallChol - 1) + (p0 + l) * kSmallLd];
-            }
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int q = 0; q < 4; ++q) acc[i][q] += x[i] * y[q];
-        }
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int r = r0 + i, c = c0 + q;
-                if (r < n && c < n && r >= c) S[r + c * kSmallLd] -= acc[i][q];
-            }
-    };
-    // the first panel's diagonal block
-    if (tid < 32) {
-        const int bad = warp_chol<T, PW>(S, 0, min(PW, n), rdiag, panel_inverse(0));
-        if (tid == 0 && bad >= 0) *flag = bad;
-    }
-    __syncthreads();
-    if (*flag >= 0) return diag_failure(p, m, MTD_ERR_NOT_POSITIVE_DEFINITE, info_base + *flag + 1);
     for (int p0 = 0; p0 < n; p0 += PW) {
         const int pw = min(PW, n - p0);
-        T *X = panel_inverse(p0);  // factored and inverted (warp 0) before this iteration
+        T *X = XI + (p0 / kNB) * kNB * kInvLd + (p0 % kNB) * (1 + kInvLd);  // panel inverse, kInvLd
+        if (tid < 32) {
+            const int bad = warp_chol<T, PW>(S, p0, pw, rdiag + p0, X);
+            if (tid == 0 && bad >= 0) *flag = p0 + bad;
+        }
+        __syncthreads();
+        const int bad = *flag;  // every thread reads the same flag
+        if (bad >= 0) return diag_failure(p, m, MTD_ERR_NOT_POSITIVE_DEFINITE, info_base + bad + 1);
         const int q0 = p0 + pw, nr = n - q0;
         if (nr <= 0) break;
         // panel below: P(r, c) = sum_{l <= c} A(r, p0 + l) X(c, l), rows q0 .., four columns a unit
@@ -379,30 +346,43 @@ __device__ __noinline__ int chol_small(const RunArgs &p, const MatCtx &m, T *Ad,
             }
             __syncthreads();
         }
-        // trailing update A(r, c) -= sum_l P(r, l) P(c, l), r >= c >= q0, in 4 x 4 blocks: the
-        // next panel's columns first (all threads); then warp 0 factors and inverts the next
-        // panel's diagonal block while warps 1 .. update the columns right of it
-        const int pwn = min(PW, nr), ca = (pwn + 3) >> 2, nb4 = (nr + 3) >> 2;
-        for (int b = tid; b < ca * nb4; b += kThreads) {
-            const int cb = b / nb4, rb = b % nb4;
-            if (rb >= cb) update_block(p0, pw, q0 + 4 * rb, q0 + 4 * cb);
-        }
-        __syncthreads();
-        if (tid < 32) {
-            const int bad = warp_chol<T, PW>(S, q0, pwn, rdiag + q0, panel_inverse(q0));
-            if (tid == 0 && bad >= 0) *flag = q0 + bad;
-        } else {
-            const int nbr = nb4 - ca, blocks = nbr * (nbr + 1) / 2;
-            for (int b = tid - 32; b < blocks; b += kThreads - 32) {
-                int br = int((sqrtf(8.0f * float(b) + 1.0f) - 1.0f) * 0.5f);
-                while ((br + 1) * (br + 2) / 2 <= b) ++br;
-                while (br * (br + 1) / 2 > b) --br;
-                update_block(p0, pw, q0 + 4 * (ca + br), q0 + 4 * (ca + b - br * (br + 1) / 2));
+        // trailing update: A(r, c) -= sum_l P(r, l) P(c, l), r >= c >= q0, in 4 x 4 blocks
+        {
+            const int nb4 = (nr + 3) >> 2, blocks = nb4 * (nb4 + 1) / 2;
+            if (tid < blocks) {
+                int br = int((sqrtf(8.0f * float(tid) + 1.0f) - 1.0f) * 0.5f);
+                while ((br + 1) * (br + 2) / 2 <= tid) ++br;
+                while (br * (br + 1) / 2 > tid) --br;
+                const int r0 = q0 + 4 * br, c0 = q0 + 4 * (tid - br * (br + 1) / 2);
+                T acc[4][4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc[i][q] = T(0);
+#pragma unroll 2
+                for (int l = 0; l < PW; ++l) {
+                    if (l >= pw) break;
+                    T x[4], y[4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        x[i] = S[min(r0 + i, kSmallChol - 1) + (p0 + l) * kSmallLd];
+                        y[i] = S[min(c0 + i, kSmallChol - 1) + (p0 + l) * kSmallLd];
+                    }
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) acc[i][q] += x[i] * y[q];
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int r = r0 + i, c = c0 + q;
+                        if (r < n && c < n && r >= c) S[r + c * kSmallLd] -= acc[i][q];
+                    }
             }
+            __syncthreads();
         }
-        __syncthreads();
-        const int bad = *flag;  // every thread reads the same flag
-        if (bad >= 0) return diag_failure(p, m, MTD_ERR_NOT_POSITIVE_DEFINITE, info_base + bad + 1);
     }
     // L to the matrix
     for (int e = tid; e < n * kSmallChol; e += kThreads) {
