@@ -681,6 +681,16 @@ __device__ __forceinline__ bool trsm_run(const RunArgs &p, E &e, void *smem, con
 #ifndef MTD_TRSM_FUSED_LU
 #define MTD_TRSM_FUSED_LU 0
 #endif
+// 1: the fused strips are separate (not inlined) functions with their own register
+// allocation, apart from the update items' paths.
+#ifndef MTD_TRSM_FUSED_NOINLINE
+#define MTD_TRSM_FUSED_NOINLINE 0
+#endif
+#if MTD_TRSM_FUSED_NOINLINE
+#define MTD_TRSM_FUSED_LINKAGE static __device__ __noinline__
+#else
+#define MTD_TRSM_FUSED_LINKAGE __device__
+#endif
 
 // Leading dimension of the fused TRSM steps' shared-memory blocks: the 64 x 64 engine's padded
 // rows, so its compute_stage reads them as staged slices.
@@ -707,7 +717,7 @@ __device__ __forceinline__ void stage_block64(double *dst, const double *src, in
 // with W1, L21, W2 staged by cp.async while Y is formed; X1 and X2 go to global memory.  The
 // same products in the same order as the engine-run steps, so the same results.
 template <int VEC>
-__device__ int trsm_rlt_fused(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
+MTD_TRSM_FUSED_LINKAGE int trsm_rlt_fused(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
     using Mw = WideMma<kBNContig, VEC>;
     using Ms = PanelMma<kBNContig, VEC>;
     const int r0 = item * kTrsmRows;
@@ -797,7 +807,7 @@ __device__ __forceinline__ void stage_block64_k(double *dst, const double *src, 
 // steps of trsm_rlt_fused with U's blocks (k-contiguous B operands): X1 = Y1 W1,
 // Y2 -= X1 U12, X2 = Y2 W2 (W = the inverses of U's diagonal blocks).
 template <int VEC>
-__device__ int trsm_run_fused(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
+MTD_TRSM_FUSED_LINKAGE int trsm_run_fused(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
     using Mw = WideMma<kBKContig, VEC>;
     using Ms = PanelMma<kBKContig, VEC>;
     static_assert(Ms::LDB == kStepLdK && Ms::B_STAGE == kStepSliceB && Ms::LDA == kStepLd, "staged layouts");
@@ -872,7 +882,7 @@ __device__ int trsm_run_fused(const RunArgs &p, const MatCtx &m, const DevTask &
 // engine's k-contiguous B slices (four 32-row slices), X1 = W1 Y1, Y2 -= L21 X1, X2 = W2 Y2
 // with W1, L21, W2 staged as m-contiguous A blocks.
 template <int VEC>
-__device__ int trsm_llnu_fused(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
+MTD_TRSM_FUSED_LINKAGE int trsm_llnu_fused(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
     using Mt = TallMma<VEC>;
     using Ms = PanelMma<kBKContig, VEC>;
     static_assert(Ms::LDB == kStepLdK && Ms::B_STAGE == kStepSliceB && Ms::LDA == kStepLd, "staged layouts");
