@@ -86,6 +86,17 @@ using ColStripStep = std::conditional_t<kTrsmRows == 128, WideMma<kBKContig, VEC
 template <int VEC>
 using ColStripUpdate = std::conditional_t<kTrsmRows == 128, GemmMma<kBKContig, VEC>, TallMma<VEC>>;
 
+// 1: the diagonal factorisations and the TRSM strips are separate (not inlined) functions, so
+// the update items' paths of the persistent kernel are allocated without them.
+#ifndef MTD_NOINLINE_PANEL_OPS
+#define MTD_NOINLINE_PANEL_OPS 0
+#endif
+#if MTD_NOINLINE_PANEL_OPS
+#define MTD_PANEL_OP_LINKAGE static __device__ __noinline__
+#else
+#define MTD_PANEL_OP_LINKAGE __device__
+#endif
+
 __device__ __forceinline__ void block_fence_sync() {
     __threadfence_block();
     __syncthreads();
@@ -472,7 +483,7 @@ __device__ __forceinline__ int factor_lu_diag(const RunArgs &p, const MatCtx &m,
 // POTRF: left-looking blocked Cholesky of the m x m diagonal block at (cr, cc), one CTA.
 // ---------------------------------------------------------------------------------
 template <typename T, int VEC, int SPLIT = 1>
-__device__ int op_potrf(const RunArgs &p, const MatCtx &m, const DevTask &t, void *smem) {
+MTD_PANEL_OP_LINKAGE int op_potrf(const RunArgs &p, const MatCtx &m, const DevTask &t, void *smem) {
     using Mn = PanelMma<kBNContig, VEC, T, SPLIT>;
     const int n = t.m;
     T *A = at<T>(m, t.cr, t.cc);
@@ -516,7 +527,7 @@ __device__ int op_potrf(const RunArgs &p, const MatCtx &m, const DevTask &t, voi
 // GETRF without pivoting: left-looking (Crout) blocked LU of the m x m block, one CTA.
 // ---------------------------------------------------------------------------------
 template <int VEC>
-__device__ int op_getrf(const RunArgs &p, const MatCtx &m, const DevTask &t, void *smem) {
+MTD_PANEL_OP_LINKAGE int op_getrf(const RunArgs &p, const MatCtx &m, const DevTask &t, void *smem) {
     using Mk = PanelMma<kBKContig, VEC>;
     const int n = t.m;
     double *A = at<double>(m, t.cr, t.cc);
@@ -956,7 +967,7 @@ MTD_TRSM_FUSED_LINKAGE int trsm_llnu_fused(const RunArgs &p, const MatCtx &m, co
 
 // X = X * L^-T   (cublasDtrsm R, L, T, NonUnit; cholesky_mustard.cu:281)
 template <typename T, int VEC, int SPLIT = 1>
-__device__ int op_trsm_rlt(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
+MTD_PANEL_OP_LINKAGE int op_trsm_rlt(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
 #if MTD_TRSM_FUSED && MTD_TRSM_WIDE
     if constexpr (sizeof(T) == 8 && VEC == 2 && kTrsmRows == 64 && kNB == 64)
         return trsm_rlt_fused<VEC>(p, m, t, item, smem);
@@ -1026,7 +1037,7 @@ __device__ int op_trsm_rlt(const RunArgs &p, const MatCtx &m, const DevTask &t, 
 
 // X = X * U^-1   (cublasDtrsm R, U, N, NonUnit; lu_mustard.cu:459)
 template <int VEC>
-__device__ int op_trsm_run(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
+MTD_PANEL_OP_LINKAGE int op_trsm_run(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
 #if MTD_TRSM_FUSED_LU && MTD_TRSM_WIDE
     if constexpr (VEC == 2 && kTrsmRows == 64 && kNB == 64) return trsm_run_fused<VEC>(p, m, t, item, smem);
 #endif
@@ -1087,7 +1098,7 @@ __device__ int op_trsm_run(const RunArgs &p, const MatCtx &m, const DevTask &t, 
 
 // X = L^-1 * X, unit diagonal   (cublasDtrsm L, L, N, Unit; lu_mustard.cu:413)
 template <int VEC>
-__device__ int op_trsm_llnu(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
+MTD_PANEL_OP_LINKAGE int op_trsm_llnu(const RunArgs &p, const MatCtx &m, const DevTask &t, int item, void *smem) {
 #if MTD_TRSM_FUSED_LU && MTD_TRSM_WIDE
     if constexpr (VEC == 2 && kTrsmRows == 64 && kNB == 64) return trsm_llnu_fused<VEC>(p, m, t, item, smem);
 #endif
