@@ -319,7 +319,7 @@ def run_reference(args, rank, world):
 # The ncu capture behind roofline.traffic (profiles/dram_traffic_bench_n24000_t1536.md):
 # DRAM read + write bytes of one step's two launches, and the hash of the FP64 kernel
 # sources it measured.
-TRAFFIC_CAPTURE = {"sources_sha16": "c9da22b6ea919263", "bytes": 75729731584 + 29367978240 + 39134266368 + 15665840640}
+TRAFFIC_CAPTURE = {"sources_sha16": "05cdf8236daa2661", "bytes": 74811281152 + 29310189824 + 39191000320 + 15616010240}
 
 METRIC = "FP64-accurate LU/Cholesky TFLOP/s, N=24000, 1 B200: mixed+IR vs plain FP64"
 
