@@ -269,3 +269,29 @@ def test_tma_fed_updates_match_cp_async_engine(mtd, kind, n, tile, nest, monkeyp
     if kind == "chol":
         out, ref = np.tril(out), np.tril(ref)
     assert rel_diff(out, ref) <= TOL
+
+
+def test_mixed_operation_families_in_one_custom_graph(mtd):
+    """A custom graph with Cholesky and LU operations together runs the kernel instance that
+    carries every operation (pure Cholesky or LU graphs run their family's instance): the
+    tiled Cholesky of the leading 2 x 2 tile block beside a tiled LU of the trailing one, on
+    a block-diagonal matrix, each against the oracle."""
+    n, b = 1024, 256
+    a = np.zeros((n, n), order="F")
+    a[:512, :512] = gen.spd_input(512, 21)
+    a[512:, 512:] = gen.lu_input(512, 22)
+    g = mtd.TaskGraph(mtd.KIND_CUSTOM, n, b)
+    ch = tiled.cholesky_tasks(2)
+    lu = [(op, (wi + 2, wj + 2), [(ri + 2, rj + 2) for ri, rj in reads]) for op, (wi, wj), reads in tiled.lu_tasks(2)]
+    for op, write, reads in ch + lu:
+        g.add_task(getattr(mtd, "OP_" + {"SYRK": "SYRK_LN"}.get(op, op)), write, reads)
+    g.finalize()
+    d = to_dev(a)
+    assert g.run(d) == 0
+    got = from_dev(d)
+    want = a.copy(order="F")
+    for task in ch + lu:
+        assert tiled.run_task(want, b, task) == 0
+    assert rel_diff(np.tril(got[:512, :512]), np.tril(want[:512, :512])) <= TOL
+    assert rel_diff(got[512:, 512:], want[512:, 512:]) <= TOL
+    g.close()
